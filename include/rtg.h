@@ -1,0 +1,222 @@
+/*
+ * rtg — C ABI of the B200 path-tracing hot path.
+ *
+ * Plain C types only (no CUDA or C++ types cross this boundary). Every function
+ * returns RTG_OK (0) or a negative RTG_ERR_* code; the message of the last
+ * failure on a context is available from rtg_last_error(ctx). A context owns one
+ * CUDA stream on one device and is driven by one host thread at a time.
+ *
+ * Each entry point names the reference interface it replaces
+ * (Kaushlendra-Kumar/ray-tracer, paths relative to that project).
+ */
+#ifndef RTG_H
+#define RTG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RTG_OK 0
+#define RTG_ERR_INVALID (-1)   /* bad argument or unknown id */
+#define RTG_ERR_SCENE (-2)     /* scene JSON rejected (parse or validation); message names the field */
+#define RTG_ERR_CUDA (-3)      /* CUDA runtime failure */
+#define RTG_ERR_NO_DEVICE (-4) /* no usable CUDA device */
+#define RTG_ERR_DEVICE (-5)    /* a kernel reported an error through its status word */
+#define RTG_ERR_BUSY (-6)      /* another render is running on this context */
+#define RTG_ERR_LIMIT (-7)     /* a size exceeds a documented maximum */
+
+typedef struct rtg_context rtg_context;
+typedef int32_t rtg_scene_id;
+
+/* RenderSettings (include/raytracer/core/scene_desc.hpp:20-35). threads and
+ * tile_size are accepted for compatibility and ignored on the GPU. */
+typedef struct rtg_settings {
+  int32_t width, height, spp, max_depth, rr_min_depth;
+  int32_t integrator; /* 0 path, 1 direct, 2 normals */
+  int32_t light_sampling;
+  int32_t tone_map;   /* 0 clamp, 1 reinhard, 2 aces */
+  uint64_t seed;
+  double exposure;
+  int32_t threads, tile_size;
+  int32_t use_bvh;    /* 0: brute-force intersection */
+  int32_t reserved;
+} rtg_settings;
+
+/* RenderOptions (include/raytracer/rendering/renderer.hpp:41-44). */
+typedef struct rtg_render_options {
+  int32_t progressive;  /* passes of 1, 1, 2, 4, ... samples */
+  int32_t max_pass_spp; /* cap on samples per pass (reference default 32) */
+} rtg_render_options;
+
+/* RenderProgress (include/raytracer/rendering/renderer.hpp:25-33). */
+typedef struct rtg_progress {
+  int32_t pass;
+  uint32_t spp_done;
+  int32_t spp_target;
+  int32_t finished;
+  int32_t cancelled;
+  int32_t reserved;
+  double elapsed_ms;
+  uint64_t rays; /* closest-hit + shadow rays so far */
+} rtg_progress;
+
+/* RenderStatsSnapshot (include/raytracer/rendering/renderer.hpp:35-39), plus the
+ * device counters behind the roofline figures. */
+typedef struct rtg_stats {
+  uint64_t camera_samples, rays, shadow_rays, rr_terminated, invalid_samples, passes;
+  uint64_t iterations, node_visits, prim_tests, extend_launches;
+  double elapsed_ms;
+  double extend_ms, shade_ms, shadow_ms, accumulate_ms, direct_ms; /* CUDA-event kernel time */
+} rtg_stats;
+
+/* SceneBuildInfo (include/raytracer/core/scene.hpp:24-27) and BvhBuildStats
+ * (include/raytracer/geometry/bvh.hpp:28-32). */
+typedef struct rtg_scene_info {
+  uint64_t primitives, triangles, spheres, planes, degenerate_skipped, lights;
+  uint64_t bvh_nodes, bvh_leaves, bvh_max_depth, bvh_max_leaf, device_bytes;
+  double bvh_build_ms, bvh_sah_cost;
+} rtg_scene_info;
+
+/* Called on the rendering thread after each pass, with no kernel of this render
+ * in flight: the framebuffer accessors below may be called from inside it.
+ * ProgressFn (include/raytracer/rendering/renderer.hpp:46-48). */
+typedef void (*rtg_pass_fn)(void* user, const rtg_progress* progress);
+
+/* ---- scene-level entry points (the editor / WASM FFI, apps/rt_wasm.cpp:117-128) ---- */
+
+/* "" if the scene parses and validates, else the first problem
+ * (rt_validate, apps/rt_wasm.cpp:117-126; parse_scene + validate_scene,
+ * src/io/scene_io.cpp:380-492). The returned string lives until the next call
+ * on the same thread. */
+const char* rtg_validate(const char* scene_json);
+
+/* Normalised scene JSON (scene_to_json, src/io/scene_io.cpp:321-378): the CLI's
+ * --dump-scene. Writes at most cap bytes including the terminator; returns the
+ * full length (excluding the terminator) or a negative error. */
+int64_t rtg_scene_dump(const char* scene_json, char* out, size_t cap);
+
+/* ---- host-side compile (no GPU needed) ---- */
+
+/* A compiled scene held on the host: Scene::compile (src/core/scene.cpp:31-137)
+ * including the binned-SAH BVH build (src/geometry/bvh.cpp:133-163). */
+typedef struct rtg_host_scene rtg_host_scene;
+
+/* Parse + validate + compile. On RTG_ERR_SCENE the message goes to err (cap bytes). */
+int rtg_compile(const char* scene_json, const char* base_dir, rtg_host_scene** out, char* err, size_t err_cap);
+void rtg_host_scene_free(rtg_host_scene* scene);
+
+/* Read-only view of a compiled scene in the reference's own layout and order
+ * (double precision): primitives in Scene::primitives order, planes, BVH nodes in
+ * the depth-first array of Bvh::nodes() with Bvh::prim_indices(), the light list
+ * (point lights first, then emitters), materials and the camera. Arrays stay
+ * valid until rtg_host_scene_free. Record layouts:
+ *   prims        24 doubles: kind (0 sphere, 1 triangle), material, smooth,
+ *                a(3), b(3), c(3), n0(3), n1(3), n2(3), 0, 0, 0
+ *                (sphere: a = centre, b.x = radius; triangle: v0, v1, v2)
+ *   planes        8 doubles: point(3), unit normal(3), material, 0
+ *   nodes        10 doubles: lo(3), hi(3), first, count (0 = interior), axis, 0
+ *   lights        2 uint32: kind (0 point, 1 emitter), index
+ *   point_lights  6 doubles: position(3), intensity(3)
+ *   materials    16 doubles: kind (0 lambertian, 1 metal, 2 dielectric, 3 emissive),
+ *                a(3) (albedo | metal albedo | tint | emitter colour), b(3) (checker
+ *                albedo 2), checker_scale, roughness, ior, intensity, two_sided, 0...
+ *   camera       19 doubles: origin(3), corner(3), du(3), dv(3), u(3), v(3), lens radius
+ *   background    8 doubles: kind (0 gradient, 1 solid), top(3), bottom(3), intensity */
+typedef struct rtg_scene_view {
+  uint64_t n_prims, n_planes, n_nodes, n_order, n_lights, n_point_lights, n_materials;
+  const double* prims;
+  const double* planes;
+  const double* nodes;
+  const uint32_t* order;
+  const uint32_t* lights;
+  const double* point_lights;
+  const double* materials;
+  double camera[19];
+  double background[8];
+  rtg_settings settings;
+  uint64_t degenerate_skipped, bvh_max_depth, bvh_leaves, bvh_max_leaf;
+  double bvh_sah_cost;
+} rtg_scene_view;
+int rtg_host_scene_view(const rtg_host_scene* scene, rtg_scene_view* out);
+
+/* ---- context ---- */
+int rtg_context_create(int device, rtg_context** out);
+void rtg_context_destroy(rtg_context* ctx);
+const char* rtg_last_error(const rtg_context* ctx);
+int rtg_device_count(void);
+
+/* ---- scenes (Scene::compile, src/core/scene.cpp:31-137; load_scene / parse_scene,
+ *      src/io/scene_io.cpp:480-502) ---- */
+
+/* Parse, validate, compile (host BVH build) and upload. base_dir resolves
+ * relative OBJ paths (may be NULL). */
+int rtg_scene_load_json(rtg_context* ctx, const char* scene_json, const char* base_dir, rtg_scene_id* out);
+int rtg_scene_load_file(rtg_context* ctx, const char* path, rtg_scene_id* out);
+/* Flatten a host-compiled scene to the device layout and copy it to HBM. The
+ * host scene stays owned by the caller. */
+int rtg_scene_upload(rtg_context* ctx, const rtg_host_scene* scene, rtg_scene_id* out);
+/* The scene file's own render settings. */
+int rtg_scene_settings(rtg_context* ctx, rtg_scene_id scene, rtg_settings* out);
+int rtg_scene_get_info(rtg_context* ctx, rtg_scene_id scene, rtg_scene_info* out);
+int rtg_scene_release(rtg_context* ctx, rtg_scene_id scene);
+
+/* ---- rendering (Renderer::render, src/rendering/renderer.cpp:58-105) ---- */
+
+/* Blocking progressive render. `cancel` may be set to non-zero from any thread;
+ * the render stops at the next wavefront iteration, drops the partial pass and
+ * reports cancelled. `settings` may be NULL (use the scene's); `opts` may be NULL
+ * (progressive, 32). */
+int rtg_render(rtg_context* ctx, rtg_scene_id scene, const rtg_settings* settings, const rtg_render_options* opts,
+               rtg_pass_fn on_pass, void* user, const volatile int32_t* cancel, rtg_progress* out);
+
+/* Batched render: n jobs traced by one shared wavefront per pass (no reference
+ * counterpart; each job's image equals its plain render bit for bit). */
+int rtg_render_batch(rtg_context* ctx, int32_t n, const rtg_scene_id* scenes, const rtg_settings* settings,
+                     const rtg_render_options* opts, const volatile int32_t* cancel, rtg_progress* out);
+
+/* Results of the last render (job = -1 or 0) or of job j of the last batch.
+ * Framebuffer::mean (include/raytracer/rendering/framebuffer.hpp:35-38): w*h*3 doubles. */
+int rtg_framebuffer_mean(rtg_context* ctx, int32_t job, double* rgb);
+/* Running sums: 4 doubles per pixel each (r, g, b, 0) and a sample count per pixel. */
+int rtg_framebuffer_moments(rtg_context* ctx, int32_t job, double* sum, double* sumsq, uint32_t* count);
+/* Renderer::image (src/rendering/renderer.cpp:107-110): tone-mapped sRGB8, w*h*3.
+ * tone_map < 0 uses the render's settings (normals: clamp, exposure 1). */
+int rtg_image_rgb8(rtg_context* ctx, int32_t job, int32_t tone_map, double exposure, uint8_t* rgb);
+int rtg_render_stats(rtg_context* ctx, rtg_stats* out);
+
+/* ---- ray queries (Scene::intersect / intersect_brute / occluded,
+ *      src/core/scene.cpp:176-234) ---- */
+
+/* rays: n records of 8 floats (ox, oy, oz, tmin, dx, dy, dz, tmax). Outputs per
+ * ray: t, primitive id (reference numbering; -1 on a miss; the plane index when
+ * is_plane), is_plane, barycentrics (b1, b2). Output pointers may be NULL. */
+int rtg_trace_closest(rtg_context* ctx, rtg_scene_id scene, const float* rays, uint64_t n, int32_t brute, float* t,
+                      int32_t* prim, int32_t* is_plane, float* bary);
+int rtg_trace_any(rtg_context* ctx, rtg_scene_id scene, const float* rays, uint64_t n, int32_t brute,
+                  uint8_t* occluded);
+
+/* ---- engine tuning (no reference counterpart) ---- */
+typedef struct rtg_tuning {
+  uint32_t pool_paths;       /* wavefront path slots (default 1 << 20) */
+  uint32_t block;            /* threads per block of the wavefront kernels: 64, 128, 256 */
+  uint64_t max_pass_samples; /* radiance slots per pass (default 1 << 27) */
+  int32_t extend_blocks, shade_blocks, shadow_blocks; /* 0 = occupancy-derived persistent grid */
+  int32_t time_kernels;      /* CUDA events around each kernel (rtg_stats.*_ms) */
+  int32_t count_traversal;   /* node / primitive counters (rtg_stats.node_visits, prim_tests) */
+} rtg_tuning;
+int rtg_get_tuning(rtg_context* ctx, rtg_tuning* out);
+int rtg_set_tuning(rtg_context* ctx, const rtg_tuning* in);
+
+/* ---- image output (encode_png / write_image, src/io/image_io.cpp:45-70) ---- */
+/* PNG bytes of an RGB8 image into out (cap bytes); returns the PNG size, or a
+ * negative error. Pass out = NULL to query the size. */
+int64_t rtg_encode_png(const uint8_t* rgb, int32_t width, int32_t height, uint8_t* out, size_t cap);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RTG_H */

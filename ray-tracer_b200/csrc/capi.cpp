@@ -1,0 +1,570 @@
+// C ABI (include/rtg.h) over the host engine. Exceptions never cross the
+// boundary: each entry point maps them to an RTG_ERR_* code and keeps the
+// message for rtg_last_error.
+#include "rtg.h"
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <exception>
+#include <fstream>
+#include <memory>
+#include <sstream>
+#include <string>
+
+#include "host/engine.hpp"
+#include "host/scene_io.hpp"
+
+namespace rtg {
+std::vector<std::uint8_t> encode_png(const std::uint8_t* rgb, int width, int height);
+}
+
+struct rtg_host_scene {
+  rtg::CompiledScene scene;
+  // Reference-layout arrays behind rtg_scene_view.
+  std::vector<double> prims, planes, nodes, point_lights, materials;
+  std::vector<std::uint32_t> lights;
+};
+
+struct rtg_context {
+  std::unique_ptr<rtg::Engine> engine;
+  std::string error;
+  bool busy = false;
+  // Settings of the last plain render (for rtg_image_rgb8 with tone_map < 0).
+  std::vector<rtg::RenderSettings> last_settings;
+};
+
+namespace {
+
+thread_local std::string g_validate_message;
+
+rtg::RenderSettings from_c(const rtg_settings& c) {
+  rtg::RenderSettings s;
+  s.width = c.width;
+  s.height = c.height;
+  s.spp = c.spp;
+  s.max_depth = c.max_depth;
+  s.rr_min_depth = c.rr_min_depth;
+  s.integrator = static_cast<rtg::Integrator>(c.integrator);
+  s.light_sampling = c.light_sampling != 0;
+  s.tone_map = static_cast<rtg::ToneMap>(c.tone_map);
+  s.seed = c.seed;
+  s.exposure = c.exposure;
+  s.threads = c.threads;
+  s.tile_size = c.tile_size;
+  s.use_bvh = c.use_bvh != 0;
+  return s;
+}
+
+rtg_settings to_c(const rtg::RenderSettings& s) {
+  rtg_settings c{};
+  c.width = s.width;
+  c.height = s.height;
+  c.spp = s.spp;
+  c.max_depth = s.max_depth;
+  c.rr_min_depth = s.rr_min_depth;
+  c.integrator = static_cast<int32_t>(s.integrator);
+  c.light_sampling = s.light_sampling ? 1 : 0;
+  c.tone_map = static_cast<int32_t>(s.tone_map);
+  c.seed = s.seed;
+  c.exposure = s.exposure;
+  c.threads = s.threads;
+  c.tile_size = s.tile_size;
+  c.use_bvh = s.use_bvh ? 1 : 0;
+  return c;
+}
+
+rtg_progress to_c(const rtg::RenderProgress& p) {
+  rtg_progress c{};
+  c.pass = p.pass;
+  c.spp_done = p.spp_done;
+  c.spp_target = p.spp_target;
+  c.finished = p.finished ? 1 : 0;
+  c.cancelled = p.cancelled ? 1 : 0;
+  c.elapsed_ms = p.elapsed_ms;
+  c.rays = p.rays;
+  return c;
+}
+
+// Range checks of validate_scene (src/io/scene_io.cpp:389-397) for settings
+// passed directly through the ABI.
+const char* settings_problem(const rtg_settings& c) {
+  if (c.integrator < 0 || c.integrator > 2) return "render.integrator: expected path, direct or normals";
+  if (c.tone_map < 0 || c.tone_map > 2) return "render.tone_map: expected clamp, reinhard or aces";
+  return nullptr;
+}
+
+const char* settings_problem(const rtg::RenderSettings& s) {
+  if (s.width < 1 || s.width > 8192) return "render.width: must be in [1, 8192]";
+  if (s.height < 1 || s.height > 8192) return "render.height: must be in [1, 8192]";
+  if (s.spp < 1 || s.spp > 1000000) return "render.spp: must be in [1, 1000000]";
+  if (s.max_depth < 1 || s.max_depth > 1000) return "render.max_depth: must be in [1, 1000]";
+  if (s.rr_min_depth < 0) return "render.rr_min_depth: must be >= 0";
+  if (!(s.exposure > 0) || !std::isfinite(s.exposure)) return "render.exposure: must be > 0";
+  return nullptr;
+}
+
+template <class F>
+int guarded(rtg_context* ctx, F&& body) {
+  if (!ctx) return RTG_ERR_INVALID;
+  try {
+    ctx->error.clear();
+    return body();
+  } catch (const rtg::SceneError& e) {
+    ctx->error = e.what();
+    return RTG_ERR_SCENE;
+  } catch (const rtg::CudaFailure& e) {
+    ctx->error = e.what();
+    return std::strstr(e.what(), "device error flag") ? RTG_ERR_DEVICE : RTG_ERR_CUDA;
+  } catch (const std::invalid_argument& e) {
+    ctx->error = e.what();
+    return RTG_ERR_INVALID;
+  } catch (const std::exception& e) {
+    ctx->error = e.what();
+    return RTG_ERR_SCENE;
+  }
+}
+
+struct BusyGuard {
+  rtg_context* ctx;
+  explicit BusyGuard(rtg_context* c) : ctx(c) { ctx->busy = true; }
+  ~BusyGuard() { ctx->busy = false; }
+};
+
+}  // namespace
+
+extern "C" {
+
+const char* rtg_validate(const char* scene_json) {
+  g_validate_message.clear();
+  if (!scene_json) {
+    g_validate_message = "scene: null input";
+    return g_validate_message.c_str();
+  }
+  try {
+    const rtg::SceneDesc d = rtg::parse_scene(scene_json);
+    const auto errors = rtg::validate_scene(d);
+    if (!errors.empty()) g_validate_message = errors.front();
+  } catch (const std::exception& e) {
+    g_validate_message = e.what();
+  }
+  return g_validate_message.c_str();
+}
+
+int64_t rtg_scene_dump(const char* scene_json, char* out, size_t cap) {
+  if (!scene_json) return RTG_ERR_INVALID;
+  try {
+    const std::string s = rtg::scene_to_json(rtg::parse_scene(scene_json)).serialize(2);
+    if (out && cap) {
+      const std::size_t n = std::min(cap - 1, s.size());
+      std::memcpy(out, s.data(), n);
+      out[n] = '\0';
+    }
+    return static_cast<int64_t>(s.size());
+  } catch (const std::exception&) {
+    return RTG_ERR_SCENE;
+  }
+}
+
+int rtg_compile(const char* scene_json, const char* base_dir, rtg_host_scene** out, char* err, size_t err_cap) {
+  if (!scene_json || !out) return RTG_ERR_INVALID;
+  *out = nullptr;
+  auto fail = [&](const char* msg) {
+    if (err && err_cap) {
+      const std::size_t n = std::min(err_cap - 1, std::strlen(msg));
+      std::memcpy(err, msg, n);
+      err[n] = '\0';
+    }
+  };
+  try {
+    rtg::SceneDesc d = rtg::parse_scene(scene_json);
+    if (base_dir) d.base_dir = base_dir;
+    auto hs = std::make_unique<rtg_host_scene>();
+    hs->scene = rtg::compile_scene(d);
+    const rtg::CompiledScene& s = hs->scene;
+    for (const rtg::Prim& p : s.prims) {
+      const rtg::D3 v[6] = {p.a, p.b, p.c, p.n0, p.n1, p.n2};
+      hs->prims.push_back(p.kind == rtg::Prim::kSphere ? 0.0 : 1.0);
+      hs->prims.push_back(p.material);
+      hs->prims.push_back(p.smooth ? 1.0 : 0.0);
+      for (const rtg::D3& q : v) {
+        hs->prims.push_back(q.x);
+        hs->prims.push_back(q.y);
+        hs->prims.push_back(q.z);
+      }
+      hs->prims.insert(hs->prims.end(), 3, 0.0);
+    }
+    for (const rtg::PlanePrim& pl : s.planes) {
+      const double r[8] = {pl.point.x, pl.point.y, pl.point.z, pl.normal.x, pl.normal.y, pl.normal.z, double(pl.material), 0};
+      hs->planes.insert(hs->planes.end(), r, r + 8);
+    }
+    for (const rtg::BinaryNode& n : s.bvh.nodes) {
+      const double r[10] = {n.box.lo.x, n.box.lo.y, n.box.lo.z, n.box.hi.x, n.box.hi.y, n.box.hi.z,
+                            double(n.first), double(n.count), double(n.axis), 0};
+      hs->nodes.insert(hs->nodes.end(), r, r + 10);
+    }
+    for (const rtg::LightEntry& l : s.lights) {
+      hs->lights.push_back(l.kind == rtg::LightEntry::kPoint ? 0u : 1u);
+      hs->lights.push_back(l.index);
+    }
+    for (const rtg::PointLight& pl : s.point_lights) {
+      const double r[6] = {pl.position.x, pl.position.y, pl.position.z, pl.intensity.x, pl.intensity.y, pl.intensity.z};
+      hs->point_lights.insert(hs->point_lights.end(), r, r + 6);
+    }
+    for (const rtg::Material& m : s.materials) {
+      double r[16] = {0};
+      if (const auto* l = std::get_if<rtg::Lambertian>(&m)) {
+        r[0] = 0;
+        r[1] = l->albedo.a.x; r[2] = l->albedo.a.y; r[3] = l->albedo.a.z;
+        r[4] = l->albedo.b.x; r[5] = l->albedo.b.y; r[6] = l->albedo.b.z;
+        r[7] = l->albedo.checker_scale;
+      } else if (const auto* me = std::get_if<rtg::Metal>(&m)) {
+        r[0] = 1;
+        r[1] = me->albedo.x; r[2] = me->albedo.y; r[3] = me->albedo.z;
+        r[8] = me->roughness;
+      } else if (const auto* di = std::get_if<rtg::Dielectric>(&m)) {
+        r[0] = 2;
+        r[1] = di->tint.x; r[2] = di->tint.y; r[3] = di->tint.z;
+        r[9] = di->ior;
+      } else {
+        const auto& e = std::get<rtg::Emissive>(m);
+        r[0] = 3;
+        r[1] = e.color.x; r[2] = e.color.y; r[3] = e.color.z;
+        r[10] = e.intensity;
+        r[11] = e.two_sided ? 1 : 0;
+      }
+      hs->materials.insert(hs->materials.end(), r, r + 16);
+    }
+    *out = hs.release();
+    return RTG_OK;
+  } catch (const std::exception& e) {
+    fail(e.what());
+    return RTG_ERR_SCENE;
+  }
+}
+
+void rtg_host_scene_free(rtg_host_scene* scene) { delete scene; }
+
+int rtg_host_scene_view(const rtg_host_scene* hs, rtg_scene_view* out) {
+  if (!hs || !out) return RTG_ERR_INVALID;
+  const rtg::CompiledScene& s = hs->scene;
+  *out = rtg_scene_view{};
+  out->n_prims = s.prims.size();
+  out->n_planes = s.planes.size();
+  out->n_nodes = s.bvh.nodes.size();
+  out->n_order = s.bvh.order.size();
+  out->n_lights = s.lights.size();
+  out->n_point_lights = s.point_lights.size();
+  out->n_materials = s.materials.size();
+  out->prims = hs->prims.data();
+  out->planes = hs->planes.data();
+  out->nodes = hs->nodes.data();
+  out->order = s.bvh.order.data();
+  out->lights = hs->lights.data();
+  out->point_lights = hs->point_lights.data();
+  out->materials = hs->materials.data();
+  const rtg::CameraFrame& c = s.camera;
+  const rtg::D3 cv[6] = {c.origin, c.corner, c.du, c.dv, c.u, c.v};
+  for (int k = 0; k < 6; ++k) {
+    out->camera[3 * k] = cv[k].x;
+    out->camera[3 * k + 1] = cv[k].y;
+    out->camera[3 * k + 2] = cv[k].z;
+  }
+  out->camera[18] = c.lens_radius;
+  const rtg::Background& b = s.background;
+  const double bg[8] = {b.kind == rtg::Background::Kind::Solid ? 1.0 : 0.0, b.top.x, b.top.y, b.top.z,
+                        b.bottom.x, b.bottom.y, b.bottom.z, b.intensity};
+  std::memcpy(out->background, bg, sizeof bg);
+  out->settings = to_c(s.settings);
+  out->degenerate_skipped = s.info.degenerate_skipped;
+  out->bvh_max_depth = s.info.bvh.max_depth;
+  out->bvh_leaves = s.info.bvh.leaves;
+  out->bvh_max_leaf = s.info.bvh.max_leaf;
+  out->bvh_sah_cost = s.info.bvh.sah_cost;
+  return RTG_OK;
+}
+
+int rtg_scene_upload(rtg_context* ctx, const rtg_host_scene* scene, rtg_scene_id* out) {
+  return guarded(ctx, [&]() {
+    if (!scene || !out) throw std::invalid_argument("null argument");
+    *out = ctx->engine->add_scene(scene->scene);
+    return RTG_OK;
+  });
+}
+
+int rtg_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+  return n;
+}
+
+int rtg_context_create(int device, rtg_context** out) {
+  if (!out) return RTG_ERR_INVALID;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return RTG_ERR_NO_DEVICE;
+  if (device < 0 || device >= n) return RTG_ERR_INVALID;
+  auto ctx = std::make_unique<rtg_context>();
+  try {
+    ctx->engine = std::make_unique<rtg::Engine>(device);
+  } catch (const std::exception&) {
+    return RTG_ERR_CUDA;
+  }
+  *out = ctx.release();
+  return RTG_OK;
+}
+
+void rtg_context_destroy(rtg_context* ctx) { delete ctx; }
+
+const char* rtg_last_error(const rtg_context* ctx) { return ctx ? ctx->error.c_str() : "null context"; }
+
+int rtg_scene_load_json(rtg_context* ctx, const char* scene_json, const char* base_dir, rtg_scene_id* out) {
+  return guarded(ctx, [&]() {
+    if (!scene_json || !out) throw std::invalid_argument("null argument");
+    rtg::SceneDesc d = rtg::parse_scene(scene_json);
+    if (base_dir) d.base_dir = base_dir;
+    *out = ctx->engine->add_scene(rtg::compile_scene(d));
+    return RTG_OK;
+  });
+}
+
+int rtg_scene_load_file(rtg_context* ctx, const char* path, rtg_scene_id* out) {
+  return guarded(ctx, [&]() {
+    if (!path || !out) throw std::invalid_argument("null argument");
+    const rtg::SceneDesc d = rtg::load_scene(path);
+    *out = ctx->engine->add_scene(rtg::compile_scene(d));
+    return RTG_OK;
+  });
+}
+
+int rtg_scene_settings(rtg_context* ctx, rtg_scene_id scene, rtg_settings* out) {
+  return guarded(ctx, [&]() {
+    if (!out) throw std::invalid_argument("null argument");
+    *out = to_c(ctx->engine->scene(scene).host.settings);
+    return RTG_OK;
+  });
+}
+
+int rtg_scene_get_info(rtg_context* ctx, rtg_scene_id scene, rtg_scene_info* out) {
+  return guarded(ctx, [&]() {
+    if (!out) throw std::invalid_argument("null argument");
+    const rtg::GpuScene& g = ctx->engine->scene(scene);
+    const rtg::BuildInfo& i = g.host.info;
+    *out = rtg_scene_info{};
+    out->primitives = g.host.prims.size();
+    out->triangles = i.triangles;
+    out->spheres = i.spheres;
+    out->planes = i.planes;
+    out->degenerate_skipped = i.degenerate_skipped;
+    out->lights = i.lights;
+    out->bvh_nodes = i.bvh.nodes;
+    out->bvh_leaves = i.bvh.leaves;
+    out->bvh_max_depth = i.bvh.max_depth;
+    out->bvh_max_leaf = i.bvh.max_leaf;
+    out->device_bytes = g.device_bytes;
+    out->bvh_build_ms = i.bvh.build_ms;
+    out->bvh_sah_cost = i.bvh.sah_cost;
+    return RTG_OK;
+  });
+}
+
+int rtg_scene_release(rtg_context* ctx, rtg_scene_id scene) {
+  return guarded(ctx, [&]() {
+    if (ctx->busy) return RTG_ERR_BUSY;
+    ctx->engine->release_scene(scene);
+    return RTG_OK;
+  });
+}
+
+int rtg_render(rtg_context* ctx, rtg_scene_id scene, const rtg_settings* settings, const rtg_render_options* opts,
+               rtg_pass_fn on_pass, void* user, const volatile int32_t* cancel, rtg_progress* out) {
+  return guarded(ctx, [&]() {
+    if (ctx->busy) return RTG_ERR_BUSY;
+    if (settings)
+      if (const char* bad = settings_problem(*settings)) throw rtg::SceneError(bad);
+    const rtg::RenderSettings s = settings ? from_c(*settings) : ctx->engine->scene(scene).host.settings;
+    if (const char* bad = settings_problem(s)) throw rtg::SceneError(bad);
+    rtg::RenderOptions o;
+    if (opts) {
+      o.progressive = opts->progressive != 0;
+      o.max_pass_spp = opts->max_pass_spp;
+    }
+    BusyGuard guard(ctx);
+    ctx->last_settings.assign(1, s);
+    rtg::PassCallback cb;
+    if (on_pass) cb = [&](const rtg::RenderProgress& p) {
+      const rtg_progress c = to_c(p);
+      on_pass(user, &c);
+    };
+    const rtg::RenderProgress p = ctx->engine->render(scene, s, o, cb, cancel);
+    if (out) *out = to_c(p);
+    return RTG_OK;
+  });
+}
+
+int rtg_render_batch(rtg_context* ctx, int32_t n, const rtg_scene_id* scenes, const rtg_settings* settings,
+                     const rtg_render_options* opts, const volatile int32_t* cancel, rtg_progress* out) {
+  return guarded(ctx, [&]() {
+    if (ctx->busy) return RTG_ERR_BUSY;
+    if (n <= 0 || n > 65535 || !scenes) throw std::invalid_argument("batch needs 1..65535 jobs");
+    std::vector<rtg::Engine::BatchJob> jobs;
+    for (int32_t j = 0; j < n; ++j) {
+      if (settings)
+        if (const char* bad = settings_problem(settings[j])) throw rtg::SceneError(bad);
+      const rtg::RenderSettings s = settings ? from_c(settings[j]) : ctx->engine->scene(scenes[j]).host.settings;
+      if (const char* bad = settings_problem(s)) throw rtg::SceneError(bad);
+      jobs.push_back({scenes[j], s});
+    }
+    rtg::RenderOptions o;
+    if (opts) {
+      o.progressive = opts->progressive != 0;
+      o.max_pass_spp = opts->max_pass_spp;
+    }
+    BusyGuard guard(ctx);
+    ctx->last_settings.clear();
+    for (const auto& j : jobs) ctx->last_settings.push_back(j.settings);
+    const std::vector<rtg::RenderProgress> p = ctx->engine->render_batch(jobs, o, cancel);
+    if (out)
+      for (int32_t j = 0; j < n; ++j) out[j] = to_c(p[static_cast<std::size_t>(j)]);
+    return RTG_OK;
+  });
+}
+
+int rtg_framebuffer_mean(rtg_context* ctx, int32_t job, double* rgb) {
+  return guarded(ctx, [&]() {
+    if (!rgb) throw std::invalid_argument("null argument");
+    ctx->engine->read_mean(job, rgb);
+    return RTG_OK;
+  });
+}
+
+int rtg_framebuffer_moments(rtg_context* ctx, int32_t job, double* sum, double* sumsq, uint32_t* count) {
+  return guarded(ctx, [&]() {
+    ctx->engine->read_moments(job, sum, sumsq, count);
+    return RTG_OK;
+  });
+}
+
+int rtg_image_rgb8(rtg_context* ctx, int32_t job, int32_t tone_map, double exposure, uint8_t* rgb) {
+  return guarded(ctx, [&]() {
+    if (!rgb) throw std::invalid_argument("null argument");
+    rtg::ToneMap op = rtg::ToneMap::Clamp;
+    double ex = exposure;
+    if (tone_map < 0) {
+      const std::size_t j = job < 0 ? 0 : static_cast<std::size_t>(job);
+      if (j >= ctx->last_settings.size()) throw std::invalid_argument("no render for job");
+      const rtg::RenderSettings& s = ctx->last_settings[j];
+      // Renderer::image(): the normals view is shown unmapped.
+      if (s.integrator == rtg::Integrator::Normals) {
+        op = rtg::ToneMap::Clamp;
+        ex = 1.0;
+      } else {
+        op = s.tone_map;
+        ex = s.exposure;
+      }
+    } else {
+      if (tone_map > 2) throw std::invalid_argument("tone_map must be 0, 1 or 2");
+      op = static_cast<rtg::ToneMap>(tone_map);
+    }
+    ctx->engine->read_image(job, op, ex, rgb);
+    return RTG_OK;
+  });
+}
+
+int rtg_render_stats(rtg_context* ctx, rtg_stats* out) {
+  return guarded(ctx, [&]() {
+    if (!out) throw std::invalid_argument("null argument");
+    const rtg::RenderStats& s = ctx->engine->stats();
+    *out = rtg_stats{};
+    out->camera_samples = s.camera_samples;
+    out->rays = s.rays;
+    out->shadow_rays = s.shadow_rays;
+    out->rr_terminated = s.rr_terminated;
+    out->invalid_samples = s.invalid_samples;
+    out->passes = s.passes;
+    out->iterations = s.iterations;
+    out->node_visits = s.node_visits;
+    out->prim_tests = s.prim_tests;
+    out->extend_launches = s.extend_launches;
+    out->elapsed_ms = s.elapsed_ms;
+    out->extend_ms = s.extend_ms;
+    out->shade_ms = s.shade_ms;
+    out->shadow_ms = s.shadow_ms;
+    out->accumulate_ms = s.accumulate_ms;
+    out->direct_ms = s.direct_ms;
+    return RTG_OK;
+  });
+}
+
+int rtg_trace_closest(rtg_context* ctx, rtg_scene_id scene, const float* rays, uint64_t n, int32_t brute, float* t,
+                      int32_t* prim, int32_t* is_plane, float* bary) {
+  return guarded(ctx, [&]() {
+    if (!rays && n) throw std::invalid_argument("null rays");
+    ctx->engine->trace_closest(scene, rays, n, brute != 0, t, prim, is_plane, bary);
+    return RTG_OK;
+  });
+}
+
+int rtg_trace_any(rtg_context* ctx, rtg_scene_id scene, const float* rays, uint64_t n, int32_t brute,
+                  uint8_t* occluded) {
+  return guarded(ctx, [&]() {
+    if ((!rays || !occluded) && n) throw std::invalid_argument("null argument");
+    ctx->engine->trace_any(scene, rays, n, brute != 0, occluded);
+    return RTG_OK;
+  });
+}
+
+int rtg_get_tuning(rtg_context* ctx, rtg_tuning* out) {
+  return guarded(ctx, [&]() {
+    if (!out) throw std::invalid_argument("null argument");
+    const rtg::EngineConfig& c = ctx->engine->config();
+    *out = rtg_tuning{};
+    out->pool_paths = c.pool_paths;
+    out->block = static_cast<uint32_t>(c.shape.extend_block);
+    out->max_pass_samples = c.max_pass_samples;
+    out->extend_blocks = c.shape.extend_blocks;
+    out->shade_blocks = c.shape.shade_blocks;
+    out->shadow_blocks = c.shape.shadow_blocks;
+    out->time_kernels = c.time_kernels ? 1 : 0;
+    out->count_traversal = c.count_traversal ? 1 : 0;
+    return RTG_OK;
+  });
+}
+
+int rtg_set_tuning(rtg_context* ctx, const rtg_tuning* in) {
+  return guarded(ctx, [&]() {
+    if (!in) throw std::invalid_argument("null argument");
+    if (ctx->busy) return RTG_ERR_BUSY;
+    if (in->block != 64 && in->block != 128 && in->block != 256) throw std::invalid_argument("block must be 64, 128 or 256");
+    if (in->pool_paths < 1024 || in->pool_paths > (1u << 26)) throw std::invalid_argument("pool_paths must be in [1024, 2^26]");
+    if (in->max_pass_samples < 1 || in->max_pass_samples > (1ull << 31)) throw std::invalid_argument("max_pass_samples must be in [1, 2^31]");
+    rtg::EngineConfig& c = ctx->engine->config();
+    const bool realloc = c.pool_paths != in->pool_paths;
+    c.pool_paths = in->pool_paths;
+    c.shape.extend_block = static_cast<int>(in->block);
+    c.max_pass_samples = in->max_pass_samples;
+    c.shape.extend_blocks = in->extend_blocks;
+    c.shape.shade_blocks = in->shade_blocks;
+    c.shape.shadow_blocks = in->shadow_blocks;
+    c.time_kernels = in->time_kernels != 0;
+    c.count_traversal = in->count_traversal != 0;
+    if (realloc) ctx->engine->reset_wave();
+    return RTG_OK;
+  });
+}
+
+int64_t rtg_encode_png(const uint8_t* rgb, int32_t width, int32_t height, uint8_t* out, size_t cap) {
+  try {
+    const std::vector<std::uint8_t> png = rtg::encode_png(rgb, width, height);
+    if (out) {
+      if (cap < png.size()) return RTG_ERR_LIMIT;
+      std::memcpy(out, png.data(), png.size());
+    }
+    return static_cast<int64_t>(png.size());
+  } catch (const std::exception&) {
+    return RTG_ERR_INVALID;
+  }
+}
+
+}  // extern "C"

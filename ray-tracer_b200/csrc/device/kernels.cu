@@ -1,0 +1,631 @@
+// Wavefront path tracer for sm_100a.
+//
+// One iteration of the wavefront over a pool of path slots:
+//   k_extend  — fills free slots with new camera paths (thin-lens generation,
+//               src/rendering/renderer.cpp:33-37 + include/raytracer/core/camera.hpp:54-62)
+//               and finds every live path's closest hit (Scene::intersect).
+//   k_shade   — emission, material sampling, next-event estimation and Russian
+//               roulette for each hit (src/rendering/integrator.cpp:97-139); continuing
+//               paths are stream-compacted into the other state buffer and shadow
+//               rays into the shadow queue with one atomic per warp (ballot + popc).
+//   k_shadow  — any-hit test of each shadow ray (Scene::occluded); unoccluded ones
+//               add their contribution to the sample's radiance slot.
+// Every path owns one radiance slot addressed by (pixel, sample-in-pass); all
+// adds to it happen in path order from kernels that are stream-ordered, so the
+// result does not depend on queue order, batch composition or timing. After the
+// pass, k_accumulate folds each pixel's samples into the double framebuffer in
+// sample order (Framebuffer::add, include/raytracer/rendering/framebuffer.hpp:31).
+//
+// Work distribution: persistent warps fetch 32 items at a time from a cursor in
+// WaveCounters (Aila & Laine, "Understanding the Efficiency of Ray Traversal on
+// GPUs", HPG 2009), so uneven traversal costs balance across SMs.
+#include <cfloat>
+
+#include "device/shade.cuh"
+#include "device/wave.h"
+
+namespace rtg {
+
+namespace {
+
+constexpr float kRayTMin = 1e-6f;  // include/raytracer/math/ray.hpp:45
+constexpr int kStackSmem = 16;
+constexpr unsigned kFull = 0xFFFFFFFFu;
+
+__device__ __forceinline__ std::uint64_t ld_u64(std::uint32_t lo, std::uint32_t hi) {
+  return static_cast<std::uint64_t>(lo) | (static_cast<std::uint64_t>(hi) << 32);
+}
+
+// Appends flagged lanes to a queue with one atomic per warp; returns this lane's
+// position (meaningful only where flag is set). All 32 lanes must call it.
+__device__ __forceinline__ std::uint32_t warp_append(bool flag, std::uint32_t* counter) {
+  const std::uint32_t mask = __ballot_sync(kFull, flag);
+  const int lane = threadIdx.x & 31;
+  std::uint32_t base = 0;
+  if (mask != 0) {
+    const int leader = __ffs(mask) - 1;
+    if (lane == leader) base = atomicAdd(counter, static_cast<std::uint32_t>(__popc(mask)));
+    base = __shfl_sync(kFull, base, leader);
+  }
+  return base + static_cast<std::uint32_t>(__popc(mask & ((1u << lane) - 1u)));
+}
+
+__device__ __forceinline__ void warp_add_u64(std::uint64_t v, std::uint64_t* dst) {
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(kFull, v, off);
+  if ((threadIdx.x & 31) == 0 && v) atomicAdd(reinterpret_cast<unsigned long long*>(dst), static_cast<unsigned long long>(v));
+}
+
+// Warp-wide fetch of the next 32 work items from `cursor`.
+__device__ __forceinline__ std::uint32_t warp_fetch(std::uint32_t* cursor) {
+  std::uint32_t base = 0;
+  if ((threadIdx.x & 31) == 0) base = atomicAdd(cursor, 32u);
+  return __shfl_sync(kFull, base, 0);
+}
+
+// Job owning global work index w (binary search over the pass table).
+__device__ __forceinline__ int find_job(const PassTable& pt, std::uint64_t w) {
+  int lo = 0, hi = pt.n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (pt.job_begin[mid] <= w) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+struct CameraSample {
+  float3 o, d;
+  Pcg rng;
+  std::uint32_t sample;  // radiance slot
+  std::uint32_t job;
+};
+
+// Camera ray for work index w: jitter (2 draws), then the lens (2 draws).
+__device__ __forceinline__ CameraSample camera_sample(const PassTable& pt, std::uint64_t w) {
+  const int k = find_job(pt, w);
+  CameraSample cs;
+  cs.job = pt.job_ids[k];
+  const RtgSceneDev& J = pt.jobs[cs.job];
+  const std::uint64_t local = w - pt.job_begin[k];
+  const std::uint32_t spp = J.pass_spp;
+  const std::uint64_t pixel = local / spp;
+  const std::uint32_t s = J.pass_s0 + static_cast<std::uint32_t>(local - pixel * spp);
+  const std::uint32_t px = static_cast<std::uint32_t>(pixel % static_cast<std::uint32_t>(J.width));
+  const std::uint32_t py = static_cast<std::uint32_t>(pixel / static_cast<std::uint32_t>(J.width));
+  cs.rng = Pcg::for_sample(J.seed, pixel, s);
+  const float jx = cs.rng.uniform();
+  const float jy = cs.rng.uniform();
+  const float3 target = J.cam_corner + (static_cast<float>(px) + jx) * J.cam_du + (static_cast<float>(py) + jy) * J.cam_dv;
+  cs.o = J.cam_origin;
+  if (J.lens_radius > 0.f) {
+    const float2 dk = unit_disk(cs.rng);
+    cs.o = cs.o + J.lens_radius * (dk.x * J.cam_u + dk.y * J.cam_v);
+  }
+  cs.d = unit_or(target - cs.o, f3(0.f, 0.f, 0.f));
+  cs.sample = static_cast<std::uint32_t>(J.sample_base + local);
+  return cs;
+}
+
+// ---------------------------------------------------------------------------
+template <int kBlock, bool kCount>
+__global__ void __launch_bounds__(kBlock) k_extend(WaveBuffers wb, PassTable pt, int par) {
+  __shared__ int stack[kStackSmem * kBlock];
+  WaveCounters* C = wb.cnt;
+  const std::uint32_t live = C->live[par];
+  const std::uint64_t next = C->next_work;
+  const std::uint64_t avail = C->total_work - next;
+  const std::uint32_t room = wb.capacity - live;
+  const std::uint32_t n_new = avail < room ? static_cast<std::uint32_t>(avail) : room;
+  const std::uint32_t n = live + n_new;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    C->n_extend = n;
+    C->live[par ^ 1] = 0;
+    C->n_shadow = 0;
+    C->fetch[2] = 0;
+  }
+  float4* const A = wb.st_a[par];
+  float4* const B = wb.st_b[par];
+  TraceCount tc;
+  std::uint64_t rays = 0;
+  while (true) {
+    const std::uint32_t base = warp_fetch(&C->fetch[0]);
+    if (base >= n) break;
+    const std::uint32_t i = base + (threadIdx.x & 31);
+    if (i >= n) continue;
+    float3 o, d;
+    std::uint32_t job;
+    if (i >= live) {
+      const CameraSample cs = camera_sample(pt, next + (i - live));
+      o = cs.o;
+      d = cs.d;
+      job = cs.job;
+      A[i] = make_float4(o.x, o.y, o.z, __uint_as_float(cs.sample));
+      // Camera rays count as a specular bounce (no NEE double-count guard).
+      B[i] = make_float4(d.x, d.y, d.z, __uint_as_float(kFlagSpecular | (job << kMetaSceneShift)));
+      wb.st_c[par][i] = make_float4(1.f, 1.f, 1.f, 0.f);
+      wb.st_d[par][i] = make_uint4(static_cast<std::uint32_t>(cs.rng.state), static_cast<std::uint32_t>(cs.rng.state >> 32),
+                                   static_cast<std::uint32_t>(cs.rng.inc), static_cast<std::uint32_t>(cs.rng.inc >> 32));
+      wb.radiance[cs.sample] = make_float4(0.f, 0.f, 0.f, 0.f);
+    } else {
+      const float4 a = A[i];
+      const float4 b = B[i];
+      o = f3(a);
+      d = f3(b);
+      job = __float_as_uint(b.w) >> kMetaSceneShift;
+    }
+    const RtgSceneDev& J = pt.jobs[job];
+    const RayHit h = J.use_bvh ? closest_hit<kStackSmem, kBlock, kCount>(J, o, d, kRayTMin, FLT_MAX, stack, tc)
+                               : closest_brute<kCount>(J, o, d, kRayTMin, FLT_MAX, tc);
+    wb.hits[i] = make_float4(h.t, __uint_as_float(h.word), h.b1, h.b2);
+    ++rays;
+  }
+  warp_add_u64(rays, &C->rays);
+  if (kCount) {
+    warp_add_u64(tc.nodes, &C->node_visits);
+    warp_add_u64(tc.prims, &C->prim_tests);
+  }
+}
+
+// ---------------------------------------------------------------------------
+template <int kBlock>
+__global__ void __launch_bounds__(kBlock) k_shade(WaveBuffers wb, PassTable pt, int par) {
+  WaveCounters* C = wb.cnt;
+  const std::uint32_t n = C->n_extend;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    C->next_work += n - C->live[par];
+    C->fetch[0] = 0;
+  }
+  const float4* const A = wb.st_a[par];
+  const float4* const B = wb.st_b[par];
+  const float4* const Cc = wb.st_c[par];
+  const uint4* const D = wb.st_d[par];
+  std::uint64_t rr_killed = 0;
+  while (true) {
+    const std::uint32_t base = warp_fetch(&C->fetch[1]);
+    if (base >= n) break;
+    const std::uint32_t i = base + (threadIdx.x & 31);
+    bool cont = false, shadow = false;
+    float3 o_next = f3(0.f, 0.f, 0.f), d_next = o_next, beta = o_next, sh_o = o_next, sh_d = o_next, sh_c = o_next;
+    float sh_tmax = 0.f;
+    std::uint32_t sample = 0, meta_next = 0, job = 0;
+    Pcg rng{0, 0};
+    if (i < n) {
+      const float4 a = A[i], b = B[i], c = Cc[i], hv = wb.hits[i];
+      const uint4 r = D[i];
+      const float3 o = f3(a), d = f3(b);
+      sample = __float_as_uint(a.w);
+      const std::uint32_t meta = __float_as_uint(b.w);
+      const std::uint32_t depth = meta & kMetaDepthMask;
+      const bool specular_bounce = (meta & kFlagSpecular) != 0;
+      job = meta >> kMetaSceneShift;
+      beta = f3(c);
+      rng.state = ld_u64(r.x, r.y);
+      rng.inc = ld_u64(r.z, r.w);
+      const RtgSceneDev& J = pt.jobs[job];
+      const RayHit h{hv.x, __float_as_uint(hv.y), hv.z, hv.w};
+      float4* const slot = &wb.radiance[sample];
+      if (J.integrator == 2) {
+        // Normals view: outward shading normal mapped to [0, 1]; black on a miss.
+        if (h.word != kHitMiss) {
+          const Surface s = make_surface(J, o, d, h);
+          const float3 nn = s.front ? s.n : -s.n;
+          *slot = make_float4(0.5f * (nn.x + 1.f), 0.5f * (nn.y + 1.f), 0.5f * (nn.z + 1.f), 0.f);
+        }
+      } else if (h.word == kHitMiss) {
+        const float3 bg = beta * background(J, d);
+        const float4 acc = *slot;
+        *slot = make_float4(acc.x + bg.x, acc.y + bg.y, acc.z + bg.z, 0.f);
+      } else {
+        const Surface s = make_surface(J, o, d, h);
+        const DevMaterial m = J.materials[s.material];
+        const float3 le = emitted(m, s.front);
+        // A light reached by a diffuse bounce was already counted by NEE.
+        if (!is_zero3(le) && (specular_bounce || !J.light_sampling || s.is_plane)) {
+          const float3 add = beta * le;
+          const float4 acc = *slot;
+          *slot = make_float4(acc.x + add.x, acc.y + add.y, acc.z + add.z, 0.f);
+        }
+        Scatter sr;
+        if (scatter(m, d, s, rng, sr)) {
+          if (J.light_sampling && !sr.specular && J.n_lights > 0) {
+            const std::uint32_t nl = static_cast<std::uint32_t>(J.n_lights);
+            const DevLight L = J.lights[rng.below(nl)];
+            const LightSample ls = sample_light(L, s, rng);
+            if (ls.valid) {
+              const float3 f = brdf_cos(m, s, ls.wi);
+              if (!is_zero3(f) && !is_zero3(ls.li_over_pdf)) {
+                sh_o = spawn_towards(s.p, s.gn, ls.wi);
+                const float3 target = s.p + ls.dist * ls.wi;
+                const float3 span = target - sh_o;
+                sh_tmax = fmaxf(sqrtf(dot3(span, span)) - shadow_margin(target), 0.f);
+                sh_d = ls.wi;
+                sh_c = beta * (f * ls.li_over_pdf) * static_cast<float>(nl);
+                shadow = true;
+              }
+            }
+          }
+          beta = beta * sr.weight;
+          bool alive = !is_zero3(beta);
+          if (alive && depth + 1 >= static_cast<std::uint32_t>(J.rr_min_depth)) {
+            const float q = fminf(fmaxf(max3(beta), 0.05f), 0.95f);
+            if (rng.uniform() >= q) {
+              alive = false;
+              ++rr_killed;
+            } else {
+              beta = beta * (1.f / q);
+            }
+          }
+          if (alive && depth + 1 < static_cast<std::uint32_t>(J.max_depth)) {
+            cont = true;
+            o_next = spawn_towards(s.p, s.gn, sr.dir);
+            d_next = sr.dir;
+            meta_next = (depth + 1) | (sr.specular ? kFlagSpecular : 0u) | (job << kMetaSceneShift);
+          }
+        }
+      }
+    }
+    const std::uint32_t cpos = warp_append(cont, &C->live[par ^ 1]);
+    const std::uint32_t spos = warp_append(shadow, &C->n_shadow);
+    if (cont) {
+      wb.st_a[par ^ 1][cpos] = make_float4(o_next.x, o_next.y, o_next.z, __uint_as_float(sample));
+      wb.st_b[par ^ 1][cpos] = make_float4(d_next.x, d_next.y, d_next.z, __uint_as_float(meta_next));
+      wb.st_c[par ^ 1][cpos] = make_float4(beta.x, beta.y, beta.z, 0.f);
+      wb.st_d[par ^ 1][cpos] = make_uint4(static_cast<std::uint32_t>(rng.state), static_cast<std::uint32_t>(rng.state >> 32),
+                                          static_cast<std::uint32_t>(rng.inc), static_cast<std::uint32_t>(rng.inc >> 32));
+    }
+    if (shadow) {
+      wb.sh_a[spos] = make_float4(sh_o.x, sh_o.y, sh_o.z, __uint_as_float(sample));
+      wb.sh_b[spos] = make_float4(sh_d.x, sh_d.y, sh_d.z, sh_tmax);
+      wb.sh_c[spos] = make_float4(sh_c.x, sh_c.y, sh_c.z, __uint_as_float(job));
+    }
+  }
+  warp_add_u64(rr_killed, &C->rr_terminated);
+}
+
+// ---------------------------------------------------------------------------
+template <int kBlock, bool kCount>
+__global__ void __launch_bounds__(kBlock) k_shadow(WaveBuffers wb, PassTable pt) {
+  __shared__ int stack[kStackSmem * kBlock];
+  WaveCounters* C = wb.cnt;
+  const std::uint32_t n = C->n_shadow;
+  if (blockIdx.x == 0 && threadIdx.x == 0) C->fetch[1] = 0;
+  TraceCount tc;
+  std::uint64_t rays = 0;
+  while (true) {
+    const std::uint32_t base = warp_fetch(&C->fetch[2]);
+    if (base >= n) break;
+    const std::uint32_t i = base + (threadIdx.x & 31);
+    if (i >= n) continue;
+    const float4 a = wb.sh_a[i], b = wb.sh_b[i], c = wb.sh_c[i];
+    const RtgSceneDev& J = pt.jobs[__float_as_uint(c.w)];
+    const float3 o = f3(a), d = f3(b);
+    const bool blocked = J.use_bvh ? any_hit<kStackSmem, kBlock, kCount>(J, o, d, kRayTMin, b.w, stack, tc)
+                                   : any_brute(J, o, d, kRayTMin, b.w);
+    ++rays;
+    if (!blocked) {
+      float4* const slot = &wb.radiance[__float_as_uint(a.w)];
+      const float4 acc = *slot;
+      *slot = make_float4(acc.x + c.x, acc.y + c.y, acc.z + c.z, 0.f);
+    }
+  }
+  warp_add_u64(rays, &C->shadow_rays);
+  if (kCount) {
+    warp_add_u64(tc.nodes, &C->node_visits);
+    warp_add_u64(tc.prims, &C->prim_tests);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Whitted-style direct integrator (src/rendering/integrator.cpp:141-174): every
+// light at diffuse hits, recursion through metal, and a deterministic Fresnel
+// split at dielectrics. The recursion becomes a depth-first walk with an explicit
+// stack of pending refraction branches, which keeps the reference's RNG draw order.
+constexpr int kDirectStack = 48;
+
+struct Pending {
+  float3 o, d, w;
+  int depth;
+};
+
+template <int kBlock>
+__device__ __forceinline__ float3 direct_light_all(const RtgSceneDev& J, const DevMaterial& m, const Surface& s,
+                                                   Pcg& rng, int* stack, TraceCount& tc, std::uint64_t& shadow_rays) {
+  float3 sum = f3(0.f, 0.f, 0.f);
+  for (int li = 0; li < J.n_lights; ++li) {
+    const LightSample ls = sample_light(J.lights[li], s, rng);
+    if (!ls.valid) continue;
+    const float3 f = brdf_cos(m, s, ls.wi);
+    if (is_zero3(f) || is_zero3(ls.li_over_pdf)) continue;
+    const float3 so = spawn_towards(s.p, s.gn, ls.wi);
+    const float3 target = s.p + ls.dist * ls.wi;
+    const float3 span = target - so;
+    const float tmax = fmaxf(sqrtf(dot3(span, span)) - shadow_margin(target), 0.f);
+    ++shadow_rays;
+    const bool blocked = J.use_bvh ? any_hit<kStackSmem, kBlock, false>(J, so, ls.wi, kRayTMin, tmax, stack, tc)
+                                   : any_brute(J, so, ls.wi, kRayTMin, tmax);
+    if (!blocked) sum = sum + f * ls.li_over_pdf;
+  }
+  return sum;
+}
+
+template <int kBlock>
+__global__ void __launch_bounds__(kBlock) k_direct(PassTable pt, std::uint64_t total, float4* radiance, WaveCounters* C) {
+  __shared__ int stack[kStackSmem * kBlock];
+  TraceCount tc;
+  std::uint64_t rays = 0, shadow_rays = 0;
+  const std::uint64_t stride = static_cast<std::uint64_t>(gridDim.x) * kBlock;
+  for (std::uint64_t w = static_cast<std::uint64_t>(blockIdx.x) * kBlock + threadIdx.x; w < total; w += stride) {
+    CameraSample cs = camera_sample(pt, w);
+    const RtgSceneDev& J = pt.jobs[cs.job];
+    Pending todo[kDirectStack];
+    int sp = 0;
+    Pending cur{cs.o, cs.d, f3(1.f, 1.f, 1.f), 0};
+    float3 L = f3(0.f, 0.f, 0.f);
+    bool overflow = false;
+    while (true) {
+      ++rays;
+      const RayHit h = J.use_bvh ? closest_hit<kStackSmem, kBlock, false>(J, cur.o, cur.d, kRayTMin, FLT_MAX, stack, tc)
+                                 : closest_brute<false>(J, cur.o, cur.d, kRayTMin, FLT_MAX, tc);
+      bool next = false;
+      if (h.word == kHitMiss) {
+        L = L + cur.w * background(J, cur.d);
+      } else {
+        const Surface s = make_surface(J, cur.o, cur.d, h);
+        const DevMaterial m = J.materials[s.material];
+        L = L + cur.w * emitted(m, s.front);
+        if (cur.depth < J.max_depth) {
+          const std::uint32_t kind = kind_of(m);
+          if (kind == kLambertian) {
+            L = L + cur.w * direct_light_all<kBlock>(J, m, s, cs.rng, stack, tc, shadow_rays);
+          } else if (kind == kMetal) {
+            Scatter sr;
+            if (scatter(m, cur.d, s, cs.rng, sr)) {
+              cur = Pending{spawn_towards(s.p, s.gn, sr.dir), sr.dir, cur.w * f3(m.colour_a), cur.depth + 1};
+              next = true;
+            }
+          } else if (kind == kDielectric) {
+            const float ior = m.head.z;
+            const float3 in = unit_or(cur.d, f3(0.f, 0.f, 0.f));
+            const float eta = s.front ? 1.f / ior : ior;
+            const float cos_i = fminf(-dot3(in, s.n), 1.f);
+            float3 refr;
+            const bool can = refract3(in, s.n, eta, refr);
+            const float F = can ? schlick(cos_i, eta) : 1.f;
+            const float3 tint = f3(m.colour_a);
+            if (can) {
+              if (sp < kDirectStack) {
+                const float3 td = unit_or(refr, f3(0.f, 0.f, 0.f));
+                todo[sp++] = Pending{spawn_towards(s.p, s.gn, td), td, cur.w * tint * (1.f - F), cur.depth + 1};
+              } else {
+                overflow = true;
+              }
+            }
+            const float3 rd = reflect3(in, s.n);
+            cur = Pending{spawn_towards(s.p, s.gn, rd), rd, cur.w * tint * F, cur.depth + 1};
+            next = true;
+          }
+        }
+      }
+      if (next) continue;
+      if (sp == 0) break;
+      cur = todo[--sp];
+    }
+    if (overflow) atomicExch(&C->error, 2u);
+    radiance[cs.sample] = make_float4(L.x, L.y, L.z, 0.f);
+  }
+  warp_add_u64(rays, &C->rays);
+  warp_add_u64(shadow_rays, &C->shadow_rays);
+}
+
+// ---------------------------------------------------------------------------
+__global__ void k_accumulate(const RtgSceneDev* __restrict__ job, const float4* __restrict__ radiance) {
+  const RtgSceneDev& J = *job;
+  const std::uint64_t pixels = static_cast<std::uint64_t>(J.width) * static_cast<std::uint64_t>(J.height);
+  const std::uint64_t p = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  std::uint64_t bad = 0;
+  if (p < pixels) {
+    const std::uint32_t k = J.pass_spp;
+    const float4* src = radiance + J.sample_base + p * k;
+    double s0 = J.fb_sum[4 * p], s1 = J.fb_sum[4 * p + 1], s2 = J.fb_sum[4 * p + 2];
+    double q0 = J.fb_sumsq[4 * p], q1 = J.fb_sumsq[4 * p + 1], q2 = J.fb_sumsq[4 * p + 2];
+    for (std::uint32_t j = 0; j < k; ++j) {
+      const float4 v = src[j];
+      double r = v.x, g = v.y, b = v.z;
+      // A non-finite or negative sample would poison the pixel: record it as black.
+      if (!isfinite(r) || !isfinite(g) || !isfinite(b) || r < 0 || g < 0 || b < 0) {
+        r = g = b = 0;
+        ++bad;
+      }
+      s0 += r; s1 += g; s2 += b;
+      q0 += r * r; q1 += g * g; q2 += b * b;
+    }
+    J.fb_sum[4 * p] = s0; J.fb_sum[4 * p + 1] = s1; J.fb_sum[4 * p + 2] = s2;
+    J.fb_sumsq[4 * p] = q0; J.fb_sumsq[4 * p + 1] = q1; J.fb_sumsq[4 * p + 2] = q2;
+    J.fb_count[p] += k;
+  }
+  warp_add_u64(bad, J.stats);
+}
+
+// Tone map (src/rendering/tonemap.cpp:15-53) in double: exposure, operator, exact
+// sRGB transfer function, round half away from zero to 8 bits.
+__device__ __forceinline__ double aces_curve(double x) {
+  const double a = 2.51, b = 0.03, c = 2.43, d = 0.59, e = 0.14;
+  const double v = (x * (a * x + b)) / (x * (c * x + d) + e);
+  return v < 0 ? 0 : (v > 1 ? 1 : v);
+}
+__device__ __forceinline__ std::uint8_t srgb8(double v) {
+  v = v < 0 ? 0 : (v > 1 ? 1 : v);
+  double s = v <= 0.0031308 ? 12.92 * v : 1.055 * pow(v, 1.0 / 2.4) - 0.055;
+  s = s < 0 ? 0 : (s > 1 ? 1 : s);
+  return static_cast<std::uint8_t>(llround(s * 255.0));
+}
+
+__global__ void k_resolve(const RtgSceneDev* __restrict__ job, int op, double exposure, std::uint8_t* rgb8, double* mean_out) {
+  const RtgSceneDev& J = *job;
+  const std::uint64_t pixels = static_cast<std::uint64_t>(J.width) * static_cast<std::uint64_t>(J.height);
+  const std::uint64_t p = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (p >= pixels) return;
+  const std::uint32_t n = J.fb_count[p];
+  double c[3] = {0, 0, 0};
+  if (n) {
+    const double inv = 1.0 / static_cast<double>(n);
+    for (int k = 0; k < 3; ++k) c[k] = J.fb_sum[4 * p + k] * inv;
+  }
+  if (mean_out)
+    for (int k = 0; k < 3; ++k) mean_out[3 * p + k] = c[k];
+  if (!rgb8) return;
+  double t[3];
+  bool finite = true;
+  for (int k = 0; k < 3; ++k) {
+    t[k] = c[k] * exposure;
+    finite = finite && isfinite(t[k]);
+  }
+  for (int k = 0; k < 3; ++k) {
+    double v = finite ? t[k] : 0.0;
+    if (op == 0) v = v < 0 ? 0 : (v > 1 ? 1 : v);
+    else if (op == 1) v = v / (1 + v);
+    else v = aces_curve(v);
+    rgb8[3 * p + k] = srgb8(v);
+  }
+}
+
+// ---------------------------------------------------------------------------
+template <int kBlock>
+__global__ void __launch_bounds__(kBlock) k_ray_closest(const RtgSceneDev* __restrict__ job, const float4* __restrict__ rays,
+                                                        std::uint32_t n, float4* out, int brute) {
+  __shared__ int stack[kStackSmem * kBlock];
+  const std::uint32_t i = blockIdx.x * kBlock + threadIdx.x;
+  if (i >= n) return;
+  const float4 a = rays[2 * i], b = rays[2 * i + 1];
+  TraceCount tc;
+  const RayHit h = brute ? closest_brute<false>(*job, f3(a), f3(b), a.w, b.w, tc)
+                         : closest_hit<kStackSmem, kBlock, false>(*job, f3(a), f3(b), a.w, b.w, stack, tc);
+  out[i] = make_float4(h.t, __uint_as_float(h.word), h.b1, h.b2);
+}
+
+template <int kBlock>
+__global__ void __launch_bounds__(kBlock) k_ray_any(const RtgSceneDev* __restrict__ job, const float4* __restrict__ rays,
+                                                    std::uint32_t n, std::uint32_t* out, int brute) {
+  __shared__ int stack[kStackSmem * kBlock];
+  const std::uint32_t i = blockIdx.x * kBlock + threadIdx.x;
+  if (i >= n) return;
+  const float4 a = rays[2 * i], b = rays[2 * i + 1];
+  TraceCount tc;
+  const bool hit = brute ? any_brute(*job, f3(a), f3(b), a.w, b.w)
+                         : any_hit<kStackSmem, kBlock, false>(*job, f3(a), f3(b), a.w, b.w, stack, tc);
+  out[i] = hit ? 1u : 0u;
+}
+
+// Blocks per SM the persistent kernels are launched with (occupancy-derived, cached).
+template <class K>
+int persistent_blocks(K kernel, int block) {
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0);
+  if (per_sm < 1) per_sm = 1;
+  return sms * per_sm;
+}
+
+struct BlockCounts {
+  int extend = 0, extend_counting = 0, shade = 0, shadow = 0, shadow_counting = 0;
+};
+
+template <int kBlock>
+const BlockCounts& block_counts() {
+  static BlockCounts bc = [] {
+    BlockCounts b;
+    b.extend = persistent_blocks(k_extend<kBlock, false>, kBlock);
+    b.extend_counting = persistent_blocks(k_extend<kBlock, true>, kBlock);
+    b.shade = persistent_blocks(k_shade<kBlock>, kBlock);
+    b.shadow = persistent_blocks(k_shadow<kBlock, false>, kBlock);
+    b.shadow_counting = persistent_blocks(k_shadow<kBlock, true>, kBlock);
+    return b;
+  }();
+  return bc;
+}
+
+template <int kBlock>
+cudaError_t stage_impl(Stage stage, const WaveBuffers& wb, const PassTable& pt, int par, const LaunchShape& shape,
+                       bool count, cudaStream_t stream) {
+  const BlockCounts& bc = block_counts<kBlock>();
+  switch (stage) {
+    case Stage::Extend: {
+      const int blocks = shape.extend_blocks ? shape.extend_blocks : (count ? bc.extend_counting : bc.extend);
+      if (count) k_extend<kBlock, true><<<blocks, kBlock, 0, stream>>>(wb, pt, par);
+      else k_extend<kBlock, false><<<blocks, kBlock, 0, stream>>>(wb, pt, par);
+      break;
+    }
+    case Stage::Shade: {
+      const int blocks = shape.shade_blocks ? shape.shade_blocks : bc.shade;
+      k_shade<kBlock><<<blocks, kBlock, 0, stream>>>(wb, pt, par);
+      break;
+    }
+    case Stage::Shadow: {
+      const int blocks = shape.shadow_blocks ? shape.shadow_blocks : (count ? bc.shadow_counting : bc.shadow);
+      if (count) k_shadow<kBlock, true><<<blocks, kBlock, 0, stream>>>(wb, pt);
+      else k_shadow<kBlock, false><<<blocks, kBlock, 0, stream>>>(wb, pt);
+      break;
+    }
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_stage(Stage stage, const WaveBuffers& wb, const PassTable& pt, int parity, const LaunchShape& shape,
+                         bool count_traversal, cudaStream_t stream) {
+  switch (shape.extend_block) {
+    case 64: return stage_impl<64>(stage, wb, pt, parity, shape, count_traversal, stream);
+    case 256: return stage_impl<256>(stage, wb, pt, parity, shape, count_traversal, stream);
+    default: return stage_impl<128>(stage, wb, pt, parity, shape, count_traversal, stream);
+  }
+}
+
+cudaError_t launch_iteration(const WaveBuffers& wb, const PassTable& pt, int parity, const LaunchShape& shape,
+                             bool count_traversal, cudaStream_t stream) {
+  for (Stage st : {Stage::Extend, Stage::Shade, Stage::Shadow}) {
+    const cudaError_t e = launch_stage(st, wb, pt, parity, shape, count_traversal, stream);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t launch_accumulate(const RtgSceneDev* job_dev, const RtgSceneDev& job_host, const float4* radiance,
+                              cudaStream_t stream) {
+  const std::uint64_t pixels = static_cast<std::uint64_t>(job_host.width) * job_host.height;
+  const unsigned blocks = static_cast<unsigned>((pixels + 255) / 256);
+  k_accumulate<<<blocks, 256, 0, stream>>>(job_dev, radiance);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_direct(const PassTable& pt, std::uint64_t total_work, float4* radiance, WaveCounters* cnt,
+                          cudaStream_t stream) {
+  static int blocks = 0;
+  if (!blocks) blocks = persistent_blocks(k_direct<128>, 128);
+  k_direct<128><<<blocks, 128, 0, stream>>>(pt, total_work, radiance, cnt);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_resolve(const RtgSceneDev* job_dev, std::uint64_t pixels, int tone_map, double exposure,
+                               std::uint8_t* rgb8, double* mean_out, cudaStream_t stream) {
+  const unsigned blocks = static_cast<unsigned>((pixels + 255) / 256);
+  k_resolve<<<blocks, 256, 0, stream>>>(job_dev, tone_map, exposure, rgb8, mean_out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ray_closest(const RtgSceneDev* job_dev, const float4* rays, std::uint32_t n, float4* out, int brute,
+                               cudaStream_t stream) {
+  if (n == 0) return cudaSuccess;
+  k_ray_closest<128><<<(n + 127) / 128, 128, 0, stream>>>(job_dev, rays, n, out, brute);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ray_any(const RtgSceneDev* job_dev, const float4* rays, std::uint32_t n, std::uint32_t* out, int brute,
+                           cudaStream_t stream) {
+  if (n == 0) return cudaSuccess;
+  k_ray_any<128><<<(n + 127) / 128, 128, 0, stream>>>(job_dev, rays, n, out, brute);
+  return cudaGetLastError();
+}
+
+}  // namespace rtg

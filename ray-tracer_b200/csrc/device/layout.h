@@ -1,0 +1,136 @@
+#pragma once
+// Device-resident scene and wavefront layouts (fp32), shared by the host
+// flattener and the sm_100a kernels. Every array is a run of 16-byte aligned
+// float4/uint4 records so a warp's loads coalesce into full sectors and each
+// record is one vectorised load.
+//
+// Geometry pools can hold many scenes back to back (batched and served modes):
+// node links and primitive slots are absolute indices into the pools, so a scene
+// is just a root node plus per-scene tables in RtgSceneDev.
+#include <cstdint>
+
+#if defined(__CUDACC__)
+#include <cuda_runtime.h>
+#else
+#include <vector_functions.h>
+#include <vector_types.h>
+#endif
+
+namespace rtg {
+
+// Two-child BVH node: both children's boxes are stored in the parent so one
+// 64-byte fetch tests two boxes. Child link >= 0: interior node index; < 0: leaf
+// whose primitives are the slots ~link, ~link + 1, ... up to the first slot that
+// carries kLastInLeaf.
+struct alignas(16) DevNode {
+  float4 xy0;   // child 0: lo.x, hi.x, lo.y, hi.y
+  float4 xy1;   // child 1: lo.x, hi.x, lo.y, hi.y
+  float4 zz;    // child 0: lo.z, hi.z; child 1: lo.z, hi.z
+  int4 link;    // x: child 0 link, y: child 1 link, z: split axis << 16, w: unused
+};
+
+// Primitive slot (leaf order): three float4.
+//  triangle: p0 = (v0, id), p1 = (e1 = v1 - v0, 0), p2 = (e2 = v2 - v0, 0)
+//  sphere:   p0 = (centre, id | kSphereBit), p1 = (radius, radius^2, 0, 0), p2 = 0
+// `id` is the scene-local primitive id (the reference's hit id), stored as bits.
+constexpr std::uint32_t kSphereBit = 0x80000000u;
+constexpr std::uint32_t kLastInLeaf = 0x40000000u;  // set on the last primitive slot of a leaf
+constexpr std::uint32_t kIdMask = 0x3FFFFFFFu;
+
+// Hit word written by the closest-hit kernel (float4.y as bits):
+constexpr std::uint32_t kHitMiss = 0xFFFFFFFFu;
+constexpr std::uint32_t kHitPlaneBit = 0x40000000u;  // low bits = plane index within the scene
+// Otherwise the word is the primitive slot (absolute, < 2^30).
+
+enum DevMaterialKind : std::uint32_t { kLambertian = 0, kMetal = 1, kDielectric = 2, kEmissive = 3 };
+
+struct alignas(16) DevMaterial {
+  float4 head;      // x: kind (bits), y: checker scale, z: roughness | ior, w: two-sided (0/1)
+  float4 colour_a;  // lambertian albedo a | metal albedo | dielectric tint | emissive colour
+  float4 colour_b;  // lambertian albedo b (checker)
+  float4 emit;      // emitted radiance colour * intensity (0 unless emissive)
+};
+
+enum DevLightKind : std::uint32_t { kLightPoint = 0, kLightSphere = 1, kLightTriangle = 2 };
+
+struct alignas(16) DevLight {
+  float4 q0;  // point: (position, kind); sphere: (centre, kind); triangle: (v0, kind)
+  float4 q1;  // point: (intensity, 0);   sphere: (r, r^2, area, two_sided); triangle: (v1, area)
+  float4 q2;  // sphere: (emission, 0);   triangle: (v2, two_sided)
+  float4 q3;  // triangle: (unit normal, 0)
+  float4 q4;  // triangle: (emission, 0)
+};
+
+struct alignas(16) DevPlane {
+  float4 point;   // xyz, w = material index (bits)
+  float4 normal;  // unit xyz
+};
+
+// One scene as the kernels see it. Pointers are device addresses.
+struct alignas(16) RtgSceneDev {
+  const DevNode* nodes;
+  const float4* prims;        // 3 per slot
+  const std::uint32_t* slot_material;  // per slot: material index | smooth flag << 31
+  const float4* slot_normals; // 3 per slot (n0, n1, n2); only read for smooth triangles
+  const DevPlane* planes;
+  const DevMaterial* materials;
+  const DevLight* lights;
+  std::int32_t root;          // >= 0: node; < 0: ~slot of a root leaf; INT32_MIN: no bounded primitives
+  std::int32_t n_planes;
+  std::int32_t n_lights;
+  std::int32_t slot_begin;    // this scene's slots are [slot_begin, slot_end)
+  std::int32_t slot_end;
+  // camera
+  float3 cam_origin, cam_corner, cam_du, cam_dv, cam_u, cam_v;
+  float lens_radius;
+  // settings
+  std::int32_t width, height, max_depth, rr_min_depth;
+  std::int32_t integrator;    // 0 path, 1 direct, 2 normals
+  std::int32_t light_sampling;
+  std::int32_t use_bvh;
+  std::uint32_t pad0;
+  std::uint64_t seed;
+  // background
+  float3 bg_top, bg_bottom;
+  float bg_intensity;
+  std::int32_t bg_solid;
+  // pass bookkeeping for this scene inside a (possibly batched) pass
+  std::uint64_t work_begin;   // first global work index of this scene in the pass
+  std::uint64_t work_count;   // pixels * pass_spp
+  std::uint32_t pass_s0;      // first sample index of the pass
+  std::uint32_t pass_spp;     // samples per pixel in this pass
+  std::uint64_t sample_base;  // offset of this scene's radiance slots in the sample buffer
+  // framebuffer of the render this descriptor belongs to (per pixel)
+  double* fb_sum;             // 4 doubles per pixel: running sum r, g, b, (unused)
+  double* fb_sumsq;           // 4 doubles per pixel: running sum of squares
+  std::uint32_t* fb_count;    // samples accumulated per pixel
+  std::uint64_t* stats;       // [0] invalid samples
+};
+
+// Path-state stream record, four float4 (SoA): one element per live path.
+//  a = (origin, sample id bits)         b = (direction, meta bits)
+//  c = (throughput, unused)             d = PCG32 state (lo, hi) and increment (lo, hi)
+// meta: depth (bits 0-11) | flags (bits 12-15) | scene (bits 16-31)
+constexpr std::uint32_t kFlagSpecular = 1u << 12;
+constexpr std::uint32_t kMetaDepthMask = 0xFFFu;
+constexpr int kMetaSceneShift = 16;
+
+// Wavefront counters in device memory.
+struct alignas(16) WaveCounters {
+  std::uint32_t live[2];      // live paths at the start of an iteration (parity)
+  std::uint32_t n_extend;     // paths traced this iteration (live + new)
+  std::uint32_t n_shadow;     // shadow rays queued this iteration
+  std::uint32_t fetch[4];     // persistent-kernel work-fetch cursors
+  std::uint64_t next_work;    // next unclaimed work index in the pass
+  std::uint64_t total_work;   // work items in the pass
+  std::uint64_t rays;         // closest-hit rays traced
+  std::uint64_t shadow_rays;
+  std::uint64_t rr_terminated;
+  std::uint64_t invalid_samples;
+  std::uint64_t node_visits;  // filled only by the counting kernel variants
+  std::uint64_t prim_tests;
+  std::uint32_t error;        // non-zero: a bounds check failed (index recorded in error_info)
+  std::uint32_t error_info;
+};
+
+}  // namespace rtg

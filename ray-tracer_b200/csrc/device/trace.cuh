@@ -1,0 +1,312 @@
+#pragma once
+// Ray queries against one scene's BVH + planes, in fp32.
+//
+// Semantics follow the reference's Scene::intersect / intersect_brute / occluded
+// (src/core/scene.cpp:152-234) and Bvh::closest / Bvh::any
+// (include/raytracer/geometry/bvh.hpp:75-132): planes are tested linearly first and
+// shrink t_max; the BVH is walked depth first, nearer child first by the sign of
+// the ray direction on the parent's split axis; a primitive is accepted only if
+// t_min < t < t_max (strict), so among equal distances the first tested wins.
+//
+// Traversal stack: the top kStackSmem entries of each thread's stack live in
+// shared memory (laid out [entry][thread] so a warp's pushes hit 32 distinct
+// banks); deeper entries spill to a small local array. The reference caps BVH
+// depth at 60, so 64 entries always suffice.
+#include "device/dmath.cuh"
+
+namespace rtg {
+
+constexpr int kStackDepth = 64;
+
+struct RayHit {
+  float t;
+  std::uint32_t word;  // slot, kHitPlaneBit | plane, or kHitMiss
+  float b1, b2;
+};
+
+struct TraceCount {
+  std::uint32_t nodes = 0, prims = 0;
+};
+
+// Precomputed per-ray slab-test terms: t = box * inv - o * inv.
+struct SlabRay {
+  float3 inv, ooi;
+  int neg[3];
+  __device__ __forceinline__ SlabRay(float3 o, float3 d) {
+    // A zero direction component becomes a tiny one so 0 * inf never appears;
+    // the slab on that axis then spans everything or nothing, as it should.
+    auto safe = [](float c) { return fabsf(c) < 1e-20f ? copysignf(1e-20f, c) : c; };
+    inv = f3(1.f / safe(d.x), 1.f / safe(d.y), 1.f / safe(d.z));
+    ooi = f3(o.x * inv.x, o.y * inv.y, o.z * inv.z);
+    neg[0] = d.x < 0.f;
+    neg[1] = d.y < 0.f;
+    neg[2] = d.z < 0.f;
+  }
+};
+
+// Both children's slab tests from one node; returns entry distances.
+__device__ __forceinline__ void node_boxes(const DevNode* __restrict__ node, const SlabRay& r, float tmin, float tmax,
+                                           bool& hit0, bool& hit1, int4& link) {
+  const float4 a = __ldg(&node->xy0);
+  const float4 b = __ldg(&node->xy1);
+  const float4 c = __ldg(&node->zz);
+  link = __ldg(&node->link);
+  const float ax0 = fmaf(a.x, r.inv.x, -r.ooi.x), ax1 = fmaf(a.y, r.inv.x, -r.ooi.x);
+  const float ay0 = fmaf(a.z, r.inv.y, -r.ooi.y), ay1 = fmaf(a.w, r.inv.y, -r.ooi.y);
+  const float az0 = fmaf(c.x, r.inv.z, -r.ooi.z), az1 = fmaf(c.y, r.inv.z, -r.ooi.z);
+  const float bx0 = fmaf(b.x, r.inv.x, -r.ooi.x), bx1 = fmaf(b.y, r.inv.x, -r.ooi.x);
+  const float by0 = fmaf(b.z, r.inv.y, -r.ooi.y), by1 = fmaf(b.w, r.inv.y, -r.ooi.y);
+  const float bz0 = fmaf(c.z, r.inv.z, -r.ooi.z), bz1 = fmaf(c.w, r.inv.z, -r.ooi.z);
+  const float a_in = fmaxf(fmaxf(fminf(ax0, ax1), fminf(ay0, ay1)), fmaxf(fminf(az0, az1), tmin));
+  const float a_out = fminf(fminf(fmaxf(ax0, ax1), fmaxf(ay0, ay1)), fminf(fmaxf(az0, az1), tmax));
+  const float b_in = fmaxf(fmaxf(fminf(bx0, bx1), fminf(by0, by1)), fmaxf(fminf(bz0, bz1), tmin));
+  const float b_out = fminf(fminf(fmaxf(bx0, bx1), fmaxf(by0, by1)), fminf(fmaxf(bz0, bz1), tmax));
+  hit0 = a_in <= a_out;
+  hit1 = b_in <= b_out;
+}
+
+// Möller-Trumbore, two-sided (include/raytracer/geometry/shapes.hpp:110-127).
+__device__ __forceinline__ bool tri_test(float3 o, float3 d, float3 v0, float3 e1, float3 e2, float tmin, float tmax,
+                                         float& t, float& b1, float& b2) {
+  const float3 pv = cross3(d, e2);
+  const float det = dot3(e1, pv);
+  if (fabsf(det) < 1e-14f) return false;
+  const float inv_det = 1.f / det;
+  const float3 tv = o - v0;
+  const float u = dot3(tv, pv) * inv_det;
+  if (u < 0.f || u > 1.f) return false;
+  const float3 qv = cross3(tv, e1);
+  const float v = dot3(d, qv) * inv_det;
+  if (v < 0.f || u + v > 1.f) return false;
+  const float tt = dot3(e2, qv) * inv_det;
+  if (!(tmin < tt && tt < tmax)) return false;
+  t = tt;
+  b1 = u;
+  b2 = v;
+  return true;
+}
+
+// Ray-sphere with the Haines et al. precision fixes ("Precision Improvements for
+// Ray/Sphere Intersection", Ray Tracing Gems ch. 7), as the reference's
+// Sphere::hit_t (include/raytracer/geometry/shapes.hpp:25-46).
+__device__ __forceinline__ bool sphere_test(float3 o, float3 d, float3 c, float radius, float tmin, float tmax,
+                                            float& t) {
+  const float3 oc = c - o;
+  const float a = dot3(d, d);
+  if (a == 0.f) return false;
+  const float h = dot3(d, oc);
+  const float cc = dot3(oc, oc) - radius * radius;
+  const float3 perp = oc - (h / a) * d;
+  const float disc = a * (radius * radius - dot3(perp, perp));
+  if (disc < 0.f) return false;
+  const float q = h + copysignf(sqrtf(disc), h);
+  float t0 = cc / q, t1 = q / a;
+  if (q == 0.f) t0 = t1 = h / a;
+  if (t0 > t1) { const float s = t0; t0 = t1; t1 = s; }
+  float tt = t0;
+  if (!(tmin < tt && tt < tmax)) {
+    tt = t1;
+    if (!(tmin < tt && tt < tmax)) return false;
+  }
+  t = tt;
+  return true;
+}
+
+__device__ __forceinline__ bool plane_test(const DevPlane& pl, float3 o, float3 d, float tmin, float tmax, float& t) {
+  const float3 n = f3(pl.normal);
+  const float denom = dot3(n, d);
+  if (fabsf(denom) < 1e-12f) return false;
+  const float tt = dot3(f3(pl.point) - o, n) / denom;
+  if (!(tmin < tt && tt < tmax)) return false;
+  t = tt;
+  return true;
+}
+
+// Tests one primitive slot; updates the best hit when closer.
+__device__ __forceinline__ std::uint32_t prim_slot_test(const float4* __restrict__ prims, int slot, float3 o, float3 d,
+                                                        float tmin, RayHit& best) {
+  const float4 p0 = __ldg(&prims[3 * slot]);
+  const float4 p1 = __ldg(&prims[3 * slot + 1]);
+  const std::uint32_t id = __float_as_uint(p0.w);
+  float t, b1 = 0.f, b2 = 0.f;
+  bool hit;
+  if (id & kSphereBit) {
+    hit = sphere_test(o, d, f3(p0), p1.x, tmin, best.t, t);
+  } else {
+    const float4 p2 = __ldg(&prims[3 * slot + 2]);
+    hit = tri_test(o, d, f3(p0), f3(p1), f3(p2), tmin, best.t, t, b1, b2);
+  }
+  if (hit) {
+    best.t = t;
+    best.word = static_cast<std::uint32_t>(slot);
+    best.b1 = b1;
+    best.b2 = b2;
+  }
+  return id;
+}
+
+template <int kStackSmem, int kBlock>
+struct TraversalStack {
+  int* smem;  // this thread's column: entry k at smem[k * kBlock]
+  int spill[kStackDepth - kStackSmem];
+  int sp = 0;
+  __device__ __forceinline__ explicit TraversalStack(int* base) : smem(base + threadIdx.x) {}
+  __device__ __forceinline__ void push(int v) {
+    if (sp < kStackSmem) smem[sp * kBlock] = v;
+    else spill[sp - kStackSmem] = v;
+    ++sp;
+  }
+  __device__ __forceinline__ bool pop(int& v) {
+    if (sp == 0) return false;
+    --sp;
+    v = sp < kStackSmem ? smem[sp * kBlock] : spill[sp - kStackSmem];
+    return true;
+  }
+};
+
+// Closest hit over planes then BVH. `stack_base` is the block's shared stack area.
+template <int kStackSmem, int kBlock, bool kCount>
+__device__ __forceinline__ RayHit closest_hit(const RtgSceneDev& sc, float3 o, float3 d, float tmin, float tmax,
+                                              int* stack_base, TraceCount& cnt) {
+  RayHit best{tmax, kHitMiss, 0.f, 0.f};
+  for (int i = 0; i < sc.n_planes; ++i) {
+    float t;
+    if (plane_test(sc.planes[i], o, d, tmin, best.t, t)) {
+      best.t = t;
+      best.word = kHitPlaneBit | static_cast<std::uint32_t>(i);
+    }
+  }
+  if (sc.root == INT32_MIN) return best;  // no bounded primitives
+  const SlabRay sr(o, d);
+  TraversalStack<kStackSmem, kBlock> st(stack_base);
+  int cur = sc.root;
+  while (true) {
+    if (cur >= 0) {
+      if (kCount) cnt.nodes++;
+      bool h0, h1;
+      int4 link;
+      node_boxes(sc.nodes + cur, sr, tmin, best.t, h0, h1, link);
+      if (h0 && h1) {
+        const int axis = (link.z >> 16) & 3;
+        const bool right_first = sr.neg[axis];
+        st.push(right_first ? link.x : link.y);
+        cur = right_first ? link.y : link.x;
+        continue;
+      }
+      if (h0) { cur = link.x; continue; }
+      if (h1) { cur = link.y; continue; }
+    } else {
+      int slot = ~cur;
+      while (true) {
+        if (kCount) cnt.prims++;
+        const std::uint32_t id = prim_slot_test(sc.prims, slot, o, d, tmin, best);
+        if (id & kLastInLeaf) break;
+        ++slot;
+      }
+    }
+    if (!st.pop(cur)) break;
+  }
+  return best;
+}
+
+// Any hit in (tmin, tmax): planes, then BVH with early exit.
+template <int kStackSmem, int kBlock, bool kCount>
+__device__ __forceinline__ bool any_hit(const RtgSceneDev& sc, float3 o, float3 d, float tmin, float tmax,
+                                        int* stack_base, TraceCount& cnt) {
+  for (int i = 0; i < sc.n_planes; ++i) {
+    float t;
+    if (plane_test(sc.planes[i], o, d, tmin, tmax, t)) return true;
+  }
+  if (sc.root == INT32_MIN) return false;
+  const SlabRay sr(o, d);
+  TraversalStack<kStackSmem, kBlock> st(stack_base);
+  int cur = sc.root;
+  RayHit probe{tmax, kHitMiss, 0.f, 0.f};
+  while (true) {
+    if (cur >= 0) {
+      if (kCount) cnt.nodes++;
+      bool h0, h1;
+      int4 link;
+      node_boxes(sc.nodes + cur, sr, tmin, tmax, h0, h1, link);
+      if (h0 && h1) {
+        st.push(link.y);
+        cur = link.x;
+        continue;
+      }
+      if (h0) { cur = link.x; continue; }
+      if (h1) { cur = link.y; continue; }
+    } else {
+      int slot = ~cur;
+      while (true) {
+        if (kCount) cnt.prims++;
+        const std::uint32_t id = prim_slot_test(sc.prims, slot, o, d, tmin, probe);
+        if (probe.word != kHitMiss) return true;
+        if (id & kLastInLeaf) break;
+        ++slot;
+      }
+    }
+    if (!st.pop(cur)) break;
+  }
+  return false;
+}
+
+// Brute force over the scene's slots. Ties go to the lower primitive id, which
+// reproduces the reference's index-order loop (src/core/scene.cpp:200-215).
+template <bool kCount>
+__device__ __forceinline__ RayHit closest_brute(const RtgSceneDev& sc, float3 o, float3 d, float tmin, float tmax,
+                                                TraceCount& cnt) {
+  RayHit best{tmax, kHitMiss, 0.f, 0.f};
+  for (int i = 0; i < sc.n_planes; ++i) {
+    float t;
+    if (plane_test(sc.planes[i], o, d, tmin, best.t, t)) {
+      best.t = t;
+      best.word = kHitPlaneBit | static_cast<std::uint32_t>(i);
+    }
+  }
+  std::uint32_t best_id = 0xFFFFFFFFu;
+  const float plane_t = best.t;
+  float tb = tmax < plane_t ? tmax : plane_t;
+  bool have = false;
+  for (int slot = sc.slot_begin; slot < sc.slot_end; ++slot) {
+    if (kCount) cnt.prims++;
+    const float4 p0 = __ldg(&sc.prims[3 * slot]);
+    const float4 p1 = __ldg(&sc.prims[3 * slot + 1]);
+    const std::uint32_t id = __float_as_uint(p0.w);
+    float t, b1 = 0.f, b2 = 0.f;
+    bool hit;
+    // Accept t == current best too, so a lower id can take over an exact tie.
+    const float limit = have ? __int_as_float(__float_as_int(tb) + 1) : tb;
+    if (id & kSphereBit) {
+      hit = sphere_test(o, d, f3(p0), p1.x, tmin, limit, t);
+    } else {
+      const float4 p2 = __ldg(&sc.prims[3 * slot + 2]);
+      hit = tri_test(o, d, f3(p0), f3(p1), f3(p2), tmin, limit, t, b1, b2);
+    }
+    if (!hit) continue;
+    const std::uint32_t pid = id & kIdMask;
+    if (have && (t > tb || (t == tb && pid > best_id))) continue;
+    have = true;
+    tb = t;
+    best_id = pid;
+    best.t = t;
+    best.word = static_cast<std::uint32_t>(slot);
+    best.b1 = b1;
+    best.b2 = b2;
+  }
+  return best;
+}
+
+__device__ __forceinline__ bool any_brute(const RtgSceneDev& sc, float3 o, float3 d, float tmin, float tmax) {
+  for (int i = 0; i < sc.n_planes; ++i) {
+    float t;
+    if (plane_test(sc.planes[i], o, d, tmin, tmax, t)) return true;
+  }
+  RayHit probe{tmax, kHitMiss, 0.f, 0.f};
+  for (int slot = sc.slot_begin; slot < sc.slot_end; ++slot) {
+    prim_slot_test(sc.prims, slot, o, d, tmin, probe);
+    if (probe.word != kHitMiss) return true;
+  }
+  return false;
+}
+
+}  // namespace rtg

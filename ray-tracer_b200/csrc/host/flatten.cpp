@@ -1,0 +1,195 @@
+#include "host/flatten.hpp"
+
+#include <cmath>
+#include <cstring>
+#include <stdexcept>
+
+namespace rtg {
+
+namespace {
+
+std::uint32_t bits_of(float f) {
+  std::uint32_t u;
+  std::memcpy(&u, &f, 4);
+  return u;
+}
+float float_of(std::uint32_t u) {
+  float f;
+  std::memcpy(&f, &u, 4);
+  return f;
+}
+
+// Round a double down / up to the nearest float, then widen by a few float ulps
+// so the fp32 slab test (whose FMA form rounds once per plane) never culls a box
+// that a primitive inside it would have been hit in.
+float down(double v) {
+  float f = static_cast<float>(v);
+  if (static_cast<double>(f) > v) f = std::nextafterf(f, -INFINITY);
+  f -= std::fabs(f) * 0x1p-22f;
+  return std::nextafterf(f, -INFINITY);
+}
+float up(double v) {
+  float f = static_cast<float>(v);
+  if (static_cast<double>(f) < v) f = std::nextafterf(f, INFINITY);
+  f += std::fabs(f) * 0x1p-22f;
+  return std::nextafterf(f, INFINITY);
+}
+
+float4 f4(D3 v, float w = 0.f) { return make_float4(float(v.x), float(v.y), float(v.z), w); }
+float3 f3h(D3 v) { return make_float3(float(v.x), float(v.y), float(v.z)); }
+
+DevMaterial material_record(const Material& m) {
+  DevMaterial r{};
+  if (const auto* l = std::get_if<Lambertian>(&m)) {
+    r.head = make_float4(float_of(kLambertian), float(l->albedo.checker_scale), 0.f, 0.f);
+    r.colour_a = f4(l->albedo.a);
+    r.colour_b = f4(l->albedo.b);
+  } else if (const auto* me = std::get_if<Metal>(&m)) {
+    r.head = make_float4(float_of(kMetal), 0.f, float(me->roughness), 0.f);
+    r.colour_a = f4(me->albedo);
+  } else if (const auto* d = std::get_if<Dielectric>(&m)) {
+    r.head = make_float4(float_of(kDielectric), 0.f, float(d->ior), 0.f);
+    r.colour_a = f4(d->tint);
+  } else {
+    const auto& e = std::get<Emissive>(m);
+    r.head = make_float4(float_of(kEmissive), 0.f, 0.f, e.two_sided ? 1.f : 0.f);
+    r.colour_a = f4(e.color);
+    r.emit = f4(e.color * e.intensity);
+  }
+  return r;
+}
+
+}  // namespace
+
+FlatScene flatten(const CompiledScene& s) {
+  FlatScene f;
+  const BinaryBvh& bvh = s.bvh;
+
+  // Primitive slots in leaf order; mark the last slot of every leaf.
+  const std::size_t nslots = bvh.order.size();
+  std::vector<bool> last(nslots, false);
+  for (const BinaryNode& n : bvh.nodes)
+    if (n.leaf()) last[n.first + n.count - 1] = true;
+  f.prims.resize(nslots * 3);
+  f.slot_material.resize(nslots);
+  f.slot_normals.resize(nslots * 3, make_float4(0.f, 0.f, 0.f, 0.f));
+  f.slot_prim.resize(nslots);
+  for (std::size_t k = 0; k < nslots; ++k) {
+    const std::uint32_t id = bvh.order[k];
+    if (id > kIdMask) throw std::runtime_error("too many primitives for the device layout");
+    const Prim& p = s.prims[id];
+    std::uint32_t word = id | (last[k] ? kLastInLeaf : 0u);
+    if (p.kind == Prim::kSphere) {
+      word |= kSphereBit;
+      f.prims[3 * k] = f4(p.a, float_of(word));
+      f.prims[3 * k + 1] = make_float4(float(p.b.x), float(p.b.x * p.b.x), 0.f, 0.f);
+      f.prims[3 * k + 2] = make_float4(0.f, 0.f, 0.f, 0.f);
+    } else {
+      f.prims[3 * k] = f4(p.a, float_of(word));
+      f.prims[3 * k + 1] = f4(p.b - p.a);
+      f.prims[3 * k + 2] = f4(p.c - p.a);
+      if (p.smooth) {
+        f.slot_normals[3 * k] = f4(p.n0);
+        f.slot_normals[3 * k + 1] = f4(p.n1);
+        f.slot_normals[3 * k + 2] = f4(p.n2);
+      }
+    }
+    f.slot_material[k] = p.material | ((p.kind == Prim::kTriangle && p.smooth) ? 0x80000000u : 0u);
+    f.slot_prim[k] = id;
+  }
+
+  // Interior nodes in depth-first order -> DevNode indices.
+  std::vector<std::int32_t> dev_index(bvh.nodes.size(), -1);
+  std::int32_t ninterior = 0;
+  for (std::size_t i = 0; i < bvh.nodes.size(); ++i)
+    if (!bvh.nodes[i].leaf()) dev_index[i] = ninterior++;
+  auto link_of = [&](std::size_t child) -> std::int32_t {
+    const BinaryNode& c = bvh.nodes[child];
+    return c.leaf() ? ~static_cast<std::int32_t>(c.first) : dev_index[child];
+  };
+  f.nodes.resize(static_cast<std::size_t>(ninterior));
+  for (std::size_t i = 0; i < bvh.nodes.size(); ++i) {
+    const BinaryNode& n = bvh.nodes[i];
+    if (n.leaf()) continue;
+    const Box& L = bvh.nodes[i + 1].box;
+    const Box& R = bvh.nodes[n.first].box;
+    DevNode& d = f.nodes[static_cast<std::size_t>(dev_index[i])];
+    d.xy0 = make_float4(down(L.lo.x), up(L.hi.x), down(L.lo.y), up(L.hi.y));
+    d.xy1 = make_float4(down(R.lo.x), up(R.hi.x), down(R.lo.y), up(R.hi.y));
+    d.zz = make_float4(down(L.lo.z), up(L.hi.z), down(R.lo.z), up(R.hi.z));
+    d.link = make_int4(link_of(i + 1), link_of(n.first), static_cast<int>(n.axis) << 16, 0);
+  }
+  if (!bvh.nodes.empty()) f.root = link_of(0);
+
+  for (const PlanePrim& pl : s.planes) {
+    DevPlane dp;
+    dp.point = f4(pl.point, float_of(pl.material));
+    dp.normal = f4(pl.normal);
+    f.planes.push_back(dp);
+  }
+  for (const Material& m : s.materials) f.materials.push_back(material_record(m));
+
+  for (const LightEntry& le : s.lights) {
+    DevLight L{};
+    if (le.kind == LightEntry::kPoint) {
+      const PointLight& pl = s.point_lights[le.index];
+      L.q0 = f4(pl.position, float_of(kLightPoint));
+      L.q1 = f4(pl.intensity);
+    } else {
+      const Prim& p = s.prims[le.index];
+      const Material& m = s.materials[p.material];
+      const auto& e = std::get<Emissive>(m);
+      const D3 emit = e.color * e.intensity;
+      if (p.kind == Prim::kSphere) {
+        L.q0 = f4(p.a, float_of(kLightSphere));
+        L.q1 = make_float4(float(p.b.x), float(p.b.x * p.b.x), float(p.area()), e.two_sided ? 1.f : 0.f);
+        L.q2 = f4(emit);
+      } else {
+        L.q0 = f4(p.a, float_of(kLightTriangle));
+        L.q1 = f4(p.b, float(p.area()));
+        L.q2 = f4(p.c, e.two_sided ? 1.f : 0.f);
+        L.q3 = f4(unit(cross(p.b - p.a, p.c - p.a)));
+        L.q4 = f4(emit);
+      }
+    }
+    f.lights.push_back(L);
+  }
+  return f;
+}
+
+void describe(const CompiledScene& s, const RenderSettings& r, RtgSceneDev& d) {
+  CameraFrame c;
+  c.setup(s.camera_desc, r.width, r.height);
+  d.cam_origin = f3h(c.origin);
+  d.cam_corner = f3h(c.corner);
+  d.cam_du = f3h(c.du);
+  d.cam_dv = f3h(c.dv);
+  d.cam_u = f3h(c.u);
+  d.cam_v = f3h(c.v);
+  d.lens_radius = float(c.lens_radius);
+  d.width = r.width;
+  d.height = r.height;
+  d.max_depth = r.max_depth;
+  d.rr_min_depth = r.rr_min_depth;
+  d.integrator = static_cast<std::int32_t>(r.integrator);
+  d.light_sampling = r.light_sampling ? 1 : 0;
+  d.use_bvh = r.use_bvh ? 1 : 0;
+  d.seed = r.seed;
+  d.bg_top = f3h(s.background.top);
+  d.bg_bottom = f3h(s.background.bottom);
+  d.bg_intensity = float(s.background.intensity);
+  d.bg_solid = s.background.kind == Background::Kind::Solid ? 1 : 0;
+}
+
+void rebase(FlatScene& f, std::int32_t node_offset, std::int32_t slot_offset, std::uint32_t material_offset) {
+  auto shift = [&](std::int32_t link) { return link >= 0 ? link + node_offset : ~(~link + slot_offset); };
+  for (DevNode& n : f.nodes) {
+    n.link.x = shift(n.link.x);
+    n.link.y = shift(n.link.y);
+  }
+  if (f.root != kNoRoot) f.root = shift(f.root);
+  for (std::uint32_t& m : f.slot_material) m = ((m & 0x7FFFFFFFu) + material_offset) | (m & 0x80000000u);
+  for (DevPlane& p : f.planes) p.point.w = float_of(bits_of(p.point.w) + material_offset);
+}
+
+}  // namespace rtg

@@ -1,0 +1,40 @@
+#pragma once
+// CompiledScene (double, reference order) -> device layout (fp32 records).
+//
+// The node array keeps the host tree's topology: every interior node becomes one
+// DevNode holding both children's boxes, rounded outward to fp32 so the boxes
+// still enclose what they enclosed in double. Primitive slots follow the tree's
+// leaf order so a leaf's primitives are contiguous (one streaming read per leaf);
+// the last slot of each leaf carries kLastInLeaf, so leaves need no count.
+#include <cstdint>
+#include <vector>
+
+#include "device/layout.h"
+#include "host/compiled_scene.hpp"
+
+namespace rtg {
+
+constexpr std::int32_t kNoRoot = INT32_MIN;
+
+struct FlatScene {
+  std::vector<DevNode> nodes;
+  std::vector<float4> prims;                // 3 per slot
+  std::vector<std::uint32_t> slot_material; // material | smooth << 31 (scene-local material index)
+  std::vector<float4> slot_normals;         // 3 per slot
+  std::vector<std::uint32_t> slot_prim;     // slot -> primitive id
+  std::vector<DevPlane> planes;             // material scene-local
+  std::vector<DevMaterial> materials;
+  std::vector<DevLight> lights;
+  std::int32_t root = kNoRoot;              // >= 0 node; < 0: ~slot of a root leaf; kNoRoot: none
+};
+
+FlatScene flatten(const CompiledScene& s);
+
+// Camera (set up for r's resolution), settings and background of a descriptor;
+// pointers and pass fields are filled in by the engine.
+void describe(const CompiledScene& s, const RenderSettings& r, RtgSceneDev& d);
+
+// Shift a flattened scene's indices by pool offsets (nodes, slots, materials).
+void rebase(FlatScene& f, std::int32_t node_offset, std::int32_t slot_offset, std::uint32_t material_offset);
+
+}  // namespace rtg
