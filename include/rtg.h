@@ -67,9 +67,12 @@ typedef struct rtg_progress {
  * device counters behind the roofline figures. */
 typedef struct rtg_stats {
   uint64_t camera_samples, rays, shadow_rays, rr_terminated, invalid_samples, passes;
-  uint64_t iterations, node_visits, prim_tests, extend_launches;
-  double elapsed_ms;
-  double extend_ms, shade_ms, shadow_ms, accumulate_ms, direct_ms; /* CUDA-event kernel time */
+  uint64_t iterations, node_visits, prim_tests, sphere_tests, extend_launches; /* closest-hit kernel */
+  uint64_t shadow_node_visits, shadow_prim_tests, shadow_sphere_tests;         /* any-hit kernel */
+  uint64_t kernel_launches; /* every kernel of this library launched by the render */
+  double elapsed_ms;        /* host wall time of the render call */
+  double device_ms;         /* CUDA-event time on the context's stream, first to last launch */
+  double extend_ms, shade_ms, shadow_ms, accumulate_ms, direct_ms; /* per-kernel event time (time_kernels) */
 } rtg_stats;
 
 /* SceneBuildInfo (include/raytracer/core/scene.hpp:24-27) and BvhBuildStats

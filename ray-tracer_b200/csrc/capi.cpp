@@ -487,7 +487,13 @@ int rtg_render_stats(rtg_context* ctx, rtg_stats* out) {
     out->node_visits = s.node_visits;
     out->prim_tests = s.prim_tests;
     out->extend_launches = s.extend_launches;
+    out->sphere_tests = s.sphere_tests;
+    out->shadow_node_visits = s.shadow_node_visits;
+    out->shadow_prim_tests = s.shadow_prim_tests;
+    out->shadow_sphere_tests = s.shadow_sphere_tests;
+    out->kernel_launches = s.kernel_launches;
     out->elapsed_ms = s.elapsed_ms;
+    out->device_ms = s.device_ms;
     out->extend_ms = s.extend_ms;
     out->shade_ms = s.shade_ms;
     out->shadow_ms = s.shadow_ms;

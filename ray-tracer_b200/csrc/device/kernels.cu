@@ -163,6 +163,7 @@ __global__ void __launch_bounds__(kBlock) k_extend(WaveBuffers wb, PassTable pt,
   if (kCount) {
     warp_add_u64(tc.nodes, &C->node_visits);
     warp_add_u64(tc.prims, &C->prim_tests);
+    warp_add_u64(tc.spheres, &C->sphere_tests);
   }
 }
 
@@ -234,11 +235,10 @@ __global__ void __launch_bounds__(kBlock) k_shade(WaveBuffers wb, PassTable pt, 
             if (ls.valid) {
               const float3 f = brdf_cos(m, s, ls.wi);
               if (!is_zero3(f) && !is_zero3(ls.li_over_pdf)) {
-                sh_o = spawn_towards(s.p, s.gn, ls.wi);
-                const float3 target = s.p + ls.dist * ls.wi;
-                const float3 span = target - sh_o;
-                sh_tmax = fmaxf(sqrtf(dot3(span, span)) - shadow_margin(target), 0.f);
-                sh_d = ls.wi;
+                const ShadowRay sray = shadow_ray(s, ls);
+                sh_o = sray.o;
+                sh_d = sray.d;
+                sh_tmax = sray.tmax;
                 sh_c = beta * (f * ls.li_over_pdf) * static_cast<float>(nl);
                 shadow = true;
               }
@@ -310,8 +310,9 @@ __global__ void __launch_bounds__(kBlock) k_shadow(WaveBuffers wb, PassTable pt)
   }
   warp_add_u64(rays, &C->shadow_rays);
   if (kCount) {
-    warp_add_u64(tc.nodes, &C->node_visits);
-    warp_add_u64(tc.prims, &C->prim_tests);
+    warp_add_u64(tc.nodes, &C->shadow_node_visits);
+    warp_add_u64(tc.prims, &C->shadow_prim_tests);
+    warp_add_u64(tc.spheres, &C->shadow_sphere_tests);
   }
 }
 
@@ -336,13 +337,10 @@ __device__ __forceinline__ float3 direct_light_all(const RtgSceneDev& J, const D
     if (!ls.valid) continue;
     const float3 f = brdf_cos(m, s, ls.wi);
     if (is_zero3(f) || is_zero3(ls.li_over_pdf)) continue;
-    const float3 so = spawn_towards(s.p, s.gn, ls.wi);
-    const float3 target = s.p + ls.dist * ls.wi;
-    const float3 span = target - so;
-    const float tmax = fmaxf(sqrtf(dot3(span, span)) - shadow_margin(target), 0.f);
+    const ShadowRay sr = shadow_ray(s, ls);
     ++shadow_rays;
-    const bool blocked = J.use_bvh ? any_hit<kStackSmem, kBlock, false>(J, so, ls.wi, kRayTMin, tmax, stack, tc)
-                                   : any_brute(J, so, ls.wi, kRayTMin, tmax);
+    const bool blocked = J.use_bvh ? any_hit<kStackSmem, kBlock, false>(J, sr.o, sr.d, kRayTMin, sr.tmax, stack, tc)
+                                   : any_brute(J, sr.o, sr.d, kRayTMin, sr.tmax);
     if (!blocked) sum = sum + f * ls.li_over_pdf;
   }
   return sum;
@@ -498,8 +496,9 @@ __global__ void __launch_bounds__(kBlock) k_ray_closest(const RtgSceneDev* __res
   if (i >= n) return;
   const float4 a = rays[2 * i], b = rays[2 * i + 1];
   TraceCount tc;
-  const RayHit h = brute ? closest_brute<false>(*job, f3(a), f3(b), a.w, b.w, tc)
-                         : closest_hit<kStackSmem, kBlock, false>(*job, f3(a), f3(b), a.w, b.w, stack, tc);
+  RayHit h = brute ? closest_brute<false>(*job, f3(a), f3(b), a.w, b.w, tc)
+                   : closest_hit<kStackSmem, kBlock, false>(*job, f3(a), f3(b), a.w, b.w, stack, tc);
+  refine_hit(*job, f3(a), f3(b), h);
   out[i] = make_float4(h.t, __uint_as_float(h.word), h.b1, h.b2);
 }
 

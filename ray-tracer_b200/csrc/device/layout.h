@@ -105,6 +105,11 @@ struct alignas(16) RtgSceneDev {
   double* fb_sumsq;           // 4 doubles per pixel: running sum of squares
   std::uint32_t* fb_count;    // samples accumulated per pixel
   std::uint64_t* stats;       // [0] invalid samples
+  // Double-precision originals for the ray-query API's distance refinement
+  // (null unless that API has been used on the scene): per slot 9 doubles
+  // (sphere: centre, radius; triangle: v0, v1, v2); per plane 6 (point, normal).
+  const double* prims64;
+  const double* planes64;
 };
 
 // Path-state stream record, four float4 (SoA): one element per live path.
@@ -127,8 +132,12 @@ struct alignas(16) WaveCounters {
   std::uint64_t shadow_rays;
   std::uint64_t rr_terminated;
   std::uint64_t invalid_samples;
-  std::uint64_t node_visits;  // filled only by the counting kernel variants
+  std::uint64_t node_visits;  // closest-hit kernel; filled only by the counting kernel variants
   std::uint64_t prim_tests;
+  std::uint64_t sphere_tests; // of which spheres (32-byte reads; triangles read 48)
+  std::uint64_t shadow_node_visits;  // any-hit kernel, same meaning
+  std::uint64_t shadow_prim_tests;
+  std::uint64_t shadow_sphere_tests;
   std::uint32_t error;        // non-zero: a bounds check failed (index recorded in error_info)
   std::uint32_t error_info;
 };

@@ -24,6 +24,11 @@ struct Surface {
   std::uint32_t material;  // absolute index into the material pool
 };
 
+// The hit point is rebuilt from the surface (barycentrics, or a projection onto
+// the sphere or plane) rather than taken as o + t d: far from the ray origin that
+// sum carries an absolute error of ulps of |o|, which can exceed the spawn offset
+// and put the point behind the surface (Waechter and Binder's method assumes a
+// surface-accurate point).
 __device__ __forceinline__ Surface make_surface(const RtgSceneDev& sc, float3 o, float3 d, const RayHit& h) {
   Surface s;
   s.p = o + h.t * d;
@@ -31,6 +36,7 @@ __device__ __forceinline__ Surface make_surface(const RtgSceneDev& sc, float3 o,
   if (s.is_plane) {
     const DevPlane pl = sc.planes[h.word & ~kHitPlaneBit];
     const float3 nrm = f3(pl.normal);
+    s.p = s.p - dot3(s.p - f3(pl.point), nrm) * nrm;
     s.front = dot3(d, nrm) < 0.f;
     s.gn = s.front ? nrm : -nrm;
     s.n = s.gn;
@@ -43,13 +49,15 @@ __device__ __forceinline__ Surface make_surface(const RtgSceneDev& sc, float3 o,
   const std::uint32_t mword = __ldg(&sc.slot_material[slot]);
   s.material = mword & 0x7FFFFFFFu;
   if (__float_as_uint(p0.w) & kSphereBit) {
-    const float3 outward = (s.p - f3(p0)) * (1.f / p1.x);
+    const float3 outward = unit_or((s.p - f3(p0)) * (1.f / p1.x), f3(0.f, 1.f, 0.f));
+    s.p = f3(p0) + p1.x * outward;
     s.front = dot3(d, outward) < 0.f;
     s.gn = s.front ? outward : -outward;
     s.n = s.gn;
     return s;
   }
   const float4 p2 = __ldg(&sc.prims[3 * slot + 2]);
+  s.p = f3(p0) + h.b1 * f3(p1) + h.b2 * f3(p2);
   const float3 ng = unit_or(cross3(f3(p1), f3(p2)), f3(0.f, 0.f, 0.f));
   s.front = dot3(d, ng) < 0.f;
   s.gn = s.front ? ng : -ng;
@@ -149,6 +157,26 @@ struct LightSample {
   float3 li_over_pdf;  // incident radiance / pdf (I / d^2 for point lights)
   bool valid;
 };
+
+// Visibility ray for a light sample: from the surface point offset to the
+// light's side, aimed at the sampled point on the light and stopping short of
+// it by the reference's margin. Aiming at the point (rather than reusing wi from
+// the un-offset point) keeps the ray from clipping the light itself when the
+// offset is larger than the margin, e.g. near the rim of a sphere light.
+struct ShadowRay {
+  float3 o, d;
+  float tmax;
+};
+__device__ __forceinline__ ShadowRay shadow_ray(const Surface& s, const LightSample& ls) {
+  ShadowRay r;
+  r.o = spawn_towards(s.p, s.gn, ls.wi);
+  const float3 target = s.p + ls.dist * ls.wi;
+  const float3 span = target - r.o;
+  const float len = sqrtf(dot3(span, span));
+  r.d = len > 0.f ? span * (1.f / len) : ls.wi;
+  r.tmax = fmaxf(len - shadow_margin(target), 0.f);
+  return r;
+}
 
 // One sample of one light as seen from s.p (no shadow test).
 __device__ __forceinline__ LightSample sample_light(const DevLight& L, const Surface& s, Pcg& rng) {

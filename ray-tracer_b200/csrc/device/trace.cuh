@@ -25,7 +25,11 @@ struct RayHit {
 };
 
 struct TraceCount {
-  std::uint32_t nodes = 0, prims = 0;
+  std::uint32_t nodes = 0, prims = 0, spheres = 0;
+  __device__ __forceinline__ void add_prim(std::uint32_t id) {
+    ++prims;
+    spheres += (id & kSphereBit) ? 1u : 0u;
+  }
 };
 
 // Precomputed per-ray slab-test terms: t = box * inv - o * inv.
@@ -198,8 +202,8 @@ __device__ __forceinline__ RayHit closest_hit(const RtgSceneDev& sc, float3 o, f
     } else {
       int slot = ~cur;
       while (true) {
-        if (kCount) cnt.prims++;
         const std::uint32_t id = prim_slot_test(sc.prims, slot, o, d, tmin, best);
+        if (kCount) cnt.add_prim(id);
         if (id & kLastInLeaf) break;
         ++slot;
       }
@@ -238,8 +242,8 @@ __device__ __forceinline__ bool any_hit(const RtgSceneDev& sc, float3 o, float3 
     } else {
       int slot = ~cur;
       while (true) {
-        if (kCount) cnt.prims++;
         const std::uint32_t id = prim_slot_test(sc.prims, slot, o, d, tmin, probe);
+        if (kCount) cnt.add_prim(id);
         if (probe.word != kHitMiss) return true;
         if (id & kLastInLeaf) break;
         ++slot;
@@ -268,10 +272,10 @@ __device__ __forceinline__ RayHit closest_brute(const RtgSceneDev& sc, float3 o,
   float tb = tmax < plane_t ? tmax : plane_t;
   bool have = false;
   for (int slot = sc.slot_begin; slot < sc.slot_end; ++slot) {
-    if (kCount) cnt.prims++;
     const float4 p0 = __ldg(&sc.prims[3 * slot]);
     const float4 p1 = __ldg(&sc.prims[3 * slot + 1]);
     const std::uint32_t id = __float_as_uint(p0.w);
+    if (kCount) cnt.add_prim(id);
     float t, b1 = 0.f, b2 = 0.f;
     bool hit;
     // Accept t == current best too, so a lower id can take over an exact tie.
@@ -294,6 +298,54 @@ __device__ __forceinline__ RayHit closest_brute(const RtgSceneDev& sc, float3 o,
     best.b2 = b2;
   }
   return best;
+}
+
+// Recomputes the winning primitive's distance (and barycentrics) in double from
+// its fp32 record, for the ray-query API: fp32 loses digits of t for near-tangent
+// sphere and grazing triangle hits. Which primitive wins stays the fp32 decision.
+__device__ __forceinline__ void refine_hit(const RtgSceneDev& sc, float3 of, float3 df, RayHit& h) {
+  if (h.word == kHitMiss || !sc.prims64) return;
+  const double ox = of.x, oy = of.y, oz = of.z, dx = df.x, dy = df.y, dz = df.z;
+  double t = h.t, b1 = h.b1, b2 = h.b2;
+  if (h.word & kHitPlaneBit) {
+    const double* pl = sc.planes64 + 6 * (h.word & ~kHitPlaneBit);
+    const double nx = pl[3], ny = pl[4], nz = pl[5];
+    const double denom = nx * dx + ny * dy + nz * dz;
+    t = ((pl[0] - ox) * nx + (pl[1] - oy) * ny + (pl[2] - oz) * nz) / denom;
+  } else {
+    const int slot = static_cast<int>(h.word);
+    const double* g = sc.prims64 + 9 * slot;
+    if (__float_as_uint(sc.prims[3 * slot].w) & kSphereBit) {
+      const double r = g[3];
+      const double ocx = g[0] - ox, ocy = g[1] - oy, ocz = g[2] - oz;
+      const double a = dx * dx + dy * dy + dz * dz;
+      const double hh = dx * ocx + dy * ocy + dz * ocz;
+      const double cc = ocx * ocx + ocy * ocy + ocz * ocz - r * r;
+      const double px = ocx - hh / a * dx, py = ocy - hh / a * dy, pz = ocz - hh / a * dz;
+      const double disc = a * (r * r - (px * px + py * py + pz * pz));
+      if (disc >= 0) {
+        const double q = hh + copysign(sqrt(disc), hh);
+        const double t0 = q != 0 ? cc / q : hh / a, t1 = q != 0 ? q / a : hh / a;
+        t = fabs(t0 - h.t) < fabs(t1 - h.t) ? t0 : t1;  // the root the fp32 test chose
+      }
+    } else {
+      const double e1x = g[3] - g[0], e1y = g[4] - g[1], e1z = g[5] - g[2];
+      const double e2x = g[6] - g[0], e2y = g[7] - g[1], e2z = g[8] - g[2];
+      const double pvx = dy * e2z - dz * e2y, pvy = dz * e2x - dx * e2z, pvz = dx * e2y - dy * e2x;
+      const double det = e1x * pvx + e1y * pvy + e1z * pvz;
+      const double tvx = ox - g[0], tvy = oy - g[1], tvz = oz - g[2];
+      const double qvx = tvy * e1z - tvz * e1y, qvy = tvz * e1x - tvx * e1z, qvz = tvx * e1y - tvy * e1x;
+      const double inv = 1.0 / det;
+      b1 = (tvx * pvx + tvy * pvy + tvz * pvz) * inv;
+      b2 = (dx * qvx + dy * qvy + dz * qvz) * inv;
+      t = (e2x * qvx + e2y * qvy + e2z * qvz) * inv;
+    }
+  }
+  if (isfinite(t) && fabs(t - h.t) <= 1e-3 * fabs(static_cast<double>(h.t))) {
+    h.t = static_cast<float>(t);
+    h.b1 = static_cast<float>(b1);
+    h.b2 = static_cast<float>(b2);
+  }
 }
 
 __device__ __forceinline__ bool any_brute(const RtgSceneDev& sc, float3 o, float3 d, float tmin, float tmax) {

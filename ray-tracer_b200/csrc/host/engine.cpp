@@ -66,6 +66,16 @@ struct Engine::Wave {
 Engine::Engine(int device) : device_(device) {
   CK(cudaSetDevice(device));
   CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  CK(cudaEventCreate(&ev_begin_));
+  CK(cudaEventCreate(&ev_end_));
+}
+
+void Engine::finish_timing() {
+  CK(cudaEventRecord(ev_end_, stream_));
+  CK(cudaEventSynchronize(ev_end_));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, ev_begin_, ev_end_));
+  stats_.device_ms = ms;
 }
 
 Engine::~Engine() {
@@ -76,8 +86,11 @@ Engine::~Engine() {
     GpuScene& s = *kv.second;
     dev_free(s.nodes); dev_free(s.prims); dev_free(s.slot_material); dev_free(s.slot_normals);
     dev_free(s.planes); dev_free(s.materials); dev_free(s.lights);
+    dev_free(s.prims64); dev_free(s.planes64);
   }
   reset_wave();
+  cudaEventDestroy(ev_begin_);
+  cudaEventDestroy(ev_end_);
   cudaStreamDestroy(stream_);
 }
 
@@ -127,6 +140,7 @@ void Engine::release_scene(int id) {
   GpuScene& s = *it->second;
   dev_free(s.nodes); dev_free(s.prims); dev_free(s.slot_material); dev_free(s.slot_normals);
   dev_free(s.planes); dev_free(s.materials); dev_free(s.lights);
+    dev_free(s.prims64); dev_free(s.planes64);
   scenes_.erase(it);
 }
 
@@ -200,6 +214,8 @@ RtgSceneDev Engine::job_descriptor(const GpuScene& sc, const RenderSettings& s, 
   d.n_lights = sc.n_lights;
   d.slot_begin = 0;
   d.slot_end = sc.n_slots;
+  d.prims64 = sc.prims64;
+  d.planes64 = sc.planes64;
   d.fb_sum = f.sum;
   d.fb_sumsq = f.sumsq;
   d.fb_count = f.count;
@@ -243,6 +259,7 @@ bool Engine::run_pass(std::vector<RtgSceneDev>& jobs, const std::vector<std::uin
   if (direct) {
     if (timed) CK(cudaEventRecord(W.tev[0], stream_));
     CK(launch_direct(pt, total, W.wb.radiance, W.wb.cnt, stream_));
+    stats_.kernel_launches += 1;
     if (timed) {
       CK(cudaEventRecord(W.tev[1], stream_));
       CK(cudaEventSynchronize(W.tev[1]));
@@ -279,6 +296,7 @@ bool Engine::run_pass(std::vector<RtgSceneDev>& jobs, const std::vector<std::uin
       } else {
         CK(launch_iteration(W.wb, pt, par, cfg_.shape, cfg_.count_traversal, stream_));
       }
+      stats_.kernel_launches += 3;
       const int slot = static_cast<int>(it % kRing);
       CK(cudaMemcpyAsync(&W.ring[slot], W.wb.cnt, sizeof(WaveCounters), cudaMemcpyDeviceToHost, stream_));
       CK(cudaEventRecord(W.ring_ev[slot], stream_));
@@ -300,6 +318,7 @@ bool Engine::run_pass(std::vector<RtgSceneDev>& jobs, const std::vector<std::uin
   if (!cancelled) {
     if (timed) CK(cudaEventRecord(W.tev[6], stream_));
     for (std::uint32_t id : ids) CK(launch_accumulate(W.jobs_dev + id, jobs[id], W.wb.radiance, stream_));
+    stats_.kernel_launches += ids.size();
     if (timed) CK(cudaEventRecord(W.tev[7], stream_));
   }
   CK(cudaStreamSynchronize(stream_));
@@ -317,6 +336,10 @@ bool Engine::run_pass(std::vector<RtgSceneDev>& jobs, const std::vector<std::uin
   stats_.rr_terminated += end.rr_terminated;
   stats_.node_visits += end.node_visits;
   stats_.prim_tests += end.prim_tests;
+  stats_.sphere_tests += end.sphere_tests;
+  stats_.shadow_node_visits += end.shadow_node_visits;
+  stats_.shadow_prim_tests += end.shadow_prim_tests;
+  stats_.shadow_sphere_tests += end.shadow_sphere_tests;
   stats_.passes++;
   return !cancelled;
 }
@@ -332,6 +355,7 @@ RenderProgress Engine::render(int scene_id, const RenderSettings& settings, cons
 
   frames_.push_back(make_frame(settings.width, settings.height));
   std::vector<RtgSceneDev> jobs(1, job_descriptor(sc, settings, frames_[0]));
+  CK(cudaEventRecord(ev_begin_, stream_));
 
   const std::uint64_t pixels = std::uint64_t(settings.width) * std::uint64_t(settings.height);
   const std::uint32_t target = static_cast<std::uint32_t>(settings.spp);
@@ -367,6 +391,7 @@ RenderProgress Engine::render(int scene_id, const RenderSettings& settings, cons
     prog.finished = done >= target;
     if (on_pass) on_pass(prog);
   }
+  finish_timing();
   std::uint64_t invalid = 0;
   CK(cudaMemcpy(&invalid, frames_[0].stats, sizeof(invalid), cudaMemcpyDeviceToHost));
   stats_.invalid_samples = invalid;
@@ -388,6 +413,7 @@ std::vector<RenderProgress> Engine::render_batch(const std::vector<BatchJob>& ba
     frames_.push_back(make_frame(batch[j].settings.width, batch[j].settings.height));
     jobs.push_back(job_descriptor(scene(batch[j].scene_id), batch[j].settings, frames_.back()));
   }
+  CK(cudaEventRecord(ev_begin_, stream_));
   std::vector<RenderProgress> prog(n);
   std::vector<std::uint32_t> done(n, 0);
   for (std::size_t j = 0; j < n; ++j) prog[j].spp_target = batch[j].settings.spp;
@@ -430,11 +456,13 @@ std::vector<RenderProgress> Engine::render_batch(const std::vector<BatchJob>& ba
       }
       if (!complete || (cancel && *cancel)) {
         for (auto& p : prog) p.cancelled = !p.finished;
+        finish_timing();
         stats_.elapsed_ms = ms;
         return prog;
       }
     }
   }
+  finish_timing();
   std::uint64_t samples = 0, invalid = 0;
   for (std::size_t j = 0; j < n; ++j) {
     std::uint64_t inv = 0;
@@ -509,6 +537,29 @@ void Engine::trace_closest(int scene_id, const float* rays, std::uint64_t n, boo
   GpuScene& sc = scene(scene_id);
   if (n == 0) return;
   if (n > 0xFFFFFFFFull) throw std::invalid_argument("too many rays in one call");
+  if (!sc.prims64) {
+    // Double originals in slot order, for the reported distance only.
+    std::vector<double> g(std::max<std::size_t>(1, sc.slot_prim.size()) * 9, 0.0);
+    for (std::size_t k = 0; k < sc.slot_prim.size(); ++k) {
+      const Prim& p = sc.host.prims[sc.slot_prim[k]];
+      const D3 v[3] = {p.a, p.kind == Prim::kSphere ? D3{p.b.x, 0, 0} : p.b, p.c};
+      for (int j = 0; j < 3; ++j) {
+        g[9 * k + 3 * j] = v[j].x;
+        g[9 * k + 3 * j + 1] = v[j].y;
+        g[9 * k + 3 * j + 2] = v[j].z;
+      }
+    }
+    std::vector<double> pl(std::max<std::size_t>(1, sc.host.planes.size()) * 6, 0.0);
+    for (std::size_t k = 0; k < sc.host.planes.size(); ++k) {
+      const PlanePrim& q = sc.host.planes[k];
+      const double r[6] = {q.point.x, q.point.y, q.point.z, q.normal.x, q.normal.y, q.normal.z};
+      std::copy(r, r + 6, pl.begin() + 6 * k);
+    }
+    std::size_t bytes = 0;
+    sc.prims64 = dev_upload(g, stream_, bytes);
+    sc.planes64 = dev_upload(pl, stream_, bytes);
+    CK(cudaStreamSynchronize(stream_));
+  }
   RenderSettings s = sc.host.settings;
   s.use_bvh = !brute;
   const RtgSceneDev d = job_descriptor(sc, s, GpuFrame{});

@@ -43,8 +43,10 @@ struct RenderProgress {
 
 struct RenderStats {
   std::uint64_t camera_samples = 0, rays = 0, shadow_rays = 0, rr_terminated = 0, invalid_samples = 0, passes = 0;
-  std::uint64_t iterations = 0, node_visits = 0, prim_tests = 0;
+  std::uint64_t iterations = 0, node_visits = 0, prim_tests = 0, sphere_tests = 0, kernel_launches = 0;
+  std::uint64_t shadow_node_visits = 0, shadow_prim_tests = 0, shadow_sphere_tests = 0;
   double elapsed_ms = 0;
+  double device_ms = 0;  // CUDA events on the engine stream around the whole render
   // Summed CUDA-event time of each kernel family (when kernel timing is on).
   double extend_ms = 0, shade_ms = 0, shadow_ms = 0, accumulate_ms = 0, direct_ms = 0;
   std::uint64_t extend_launches = 0;
@@ -63,6 +65,8 @@ struct GpuScene {
   DevPlane* planes = nullptr;
   DevMaterial* materials = nullptr;
   DevLight* lights = nullptr;
+  double* prims64 = nullptr;   // ray-query refinement geometry (lazily uploaded)
+  double* planes64 = nullptr;
   std::size_t device_bytes = 0;
 };
 
@@ -139,8 +143,11 @@ class Engine {
   bool run_pass(std::vector<RtgSceneDev>& jobs, const std::vector<std::uint32_t>& ids, std::uint64_t total,
                 bool direct, const volatile std::int32_t* cancel);
 
+  void finish_timing();  // records the end event and fills stats_.device_ms
+
   int device_;
   cudaStream_t stream_ = nullptr;
+  cudaEvent_t ev_begin_ = nullptr, ev_end_ = nullptr;
   EngineConfig cfg_;
   std::unordered_map<int, std::unique_ptr<GpuScene>> scenes_;
   int next_scene_ = 1;

@@ -73,8 +73,10 @@ class _Progress(C.Structure):
 class _Stats(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in (
         "camera_samples", "rays", "shadow_rays", "rr_terminated", "invalid_samples", "passes",
-        "iterations", "node_visits", "prim_tests", "extend_launches")] + [
-        (n, C.c_double) for n in ("elapsed_ms", "extend_ms", "shade_ms", "shadow_ms", "accumulate_ms", "direct_ms")]
+        "iterations", "node_visits", "prim_tests", "sphere_tests", "extend_launches", "shadow_node_visits",
+        "shadow_prim_tests", "shadow_sphere_tests", "kernel_launches")] + [
+        (n, C.c_double) for n in ("elapsed_ms", "device_ms", "extend_ms", "shade_ms", "shadow_ms", "accumulate_ms",
+                                  "direct_ms")]
 
 
 class _SceneInfo(C.Structure):

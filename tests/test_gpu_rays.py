@@ -1,0 +1,147 @@
+"""GPU ray queries (the closest-hit and any-hit kernels, through the C ABI)
+against the reference's own results and the oracle."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import rtg
+import rtoracle
+import workloads
+from conftest import GOLDEN
+from parity import hit_parity
+
+pytestmark = pytest.mark.gpu
+
+CONFIGS = {"cornell": workloads.cornell, "spheres": workloads.sphere_field, "mesh": workloads.mesh_stress}
+
+
+@pytest.fixture(scope="module")
+def scenes(ctx):
+    out = {}
+    for name, make in CONFIGS.items():
+        host = rtg.parse_scene(json.dumps(make()))
+        out[name] = (host, host.view(), ctx.upload(host))
+    return out
+
+
+@pytest.mark.parametrize("cfg", list(CONFIGS))
+def test_closest_hit_matches_reference_fixture(ctx, scenes, cfg):
+    g = np.load(os.path.join(GOLDEN, f"rays_{cfg}.npz"))
+    _, _, sid = scenes[cfg]
+    t, prim, plane, _ = ctx.trace_closest(sid, g["rays"])
+    ref_t = np.where(g["hit"] == 1, g["t"], 0.0)
+    p = hit_parity(t, prim, plane, ref_t, g["prim"], g["is_plane"])
+    assert p["hit_rate"] > 0.1
+    assert p["accepted"] >= 0.999, p
+    # Brute-force kernel against the reference's intersect_brute.
+    tb, pb, plb, _ = ctx.trace_closest(sid, g["rays"], brute=True)
+    pbr = hit_parity(tb, pb, plb, np.where(g["brute_hit"] == 1, g["brute_t"], 0.0), g["brute_prim"], g["brute_plane"])
+    assert pbr["accepted"] >= 0.999, pbr
+
+
+@pytest.mark.parametrize("cfg", ["cornell", "spheres"])
+def test_closest_hit_200k_rays_vs_oracle(ctx, scenes, cfg):
+    _, view, sid = scenes[cfg]
+    rays = workloads.random_rays(view, 200_000, seed=202)
+    t, prim, plane, _ = ctx.trace_closest(sid, rays)
+    ot, op, opl, _ = rtoracle.OracleScene(view).closest_parallel(rays.astype(np.float64))
+    p = hit_parity(t, prim, plane, ot, op, opl)
+    print(cfg, {k: v for k, v in p.items() if k != "fail_idx"})
+    assert p["accepted"] >= 0.9999, p
+
+
+def test_mesh_1m_rays_vs_oracle_and_brute_force(ctx, scenes):
+    """Config 3's fixed set: 1M seeded fp32 rays against the 174k-triangle scene.
+    GPU BVH vs CPU BVH (oracle, all 1M), GPU BVH vs GPU brute force (all 1M),
+    GPU vs CPU brute force (10k subset)."""
+    _, view, sid = scenes["mesh"]
+    rays = workloads.random_rays(view, 1_000_000, seed=1)
+    t, prim, plane, _ = ctx.trace_closest(sid, rays)
+    oracle = rtoracle.OracleScene(view)
+    ot, op, opl, _ = oracle.closest_parallel(rays.astype(np.float64))
+    p = hit_parity(t, prim, plane, ot, op, opl)
+    print("mesh 1M vs oracle BVH", {k: v for k, v in p.items() if k != "fail_idx"})
+    assert p["accepted"] >= 0.9999 and p["strict"] >= 0.999, p
+    tb, pb, plb, _ = ctx.trace_closest(sid, rays, brute=True)
+    pg = hit_parity(t, prim, plane, tb, pb, plb)
+    print("mesh 1M GPU BVH vs GPU brute", {k: v for k, v in pg.items() if k != "fail_idx"})
+    assert pg["accepted"] >= 0.9999, pg
+    sub = rays[:10_000].astype(np.float64)
+    ct, cp, cpl, _ = oracle.closest_parallel(sub, brute=True)
+    ps = hit_parity(t[:10_000], prim[:10_000], plane[:10_000], ct, cp, cpl)
+    assert ps["accepted"] >= 0.999, ps
+
+
+@pytest.mark.parametrize("cfg", list(CONFIGS))
+def test_any_hit_agrees_with_closest_hit(ctx, scenes, cfg):
+    """occluded(r, tmax) == (hit && t < tmax), the reference's BVH test rule."""
+    _, view, sid = scenes[cfg]
+    rays = workloads.random_rays(view, 100_000, seed=303)
+    t, prim, _, _ = ctx.trace_closest(sid, rays)
+    scale = float(np.median(t[prim >= 0]))
+    for f in (0.1, 1.0, 10.0):
+        tmax = scale * f
+        r = rays.copy()
+        r[:, 7] = tmax
+        occ = ctx.trace_any(sid, r)
+        expect = (prim >= 0) & (t < tmax)
+        near = np.abs(t - tmax) <= 1e-5 * tmax
+        assert np.array_equal(occ[~near].astype(bool), expect[~near]), (cfg, f)
+        occ_b = ctx.trace_any(sid, r, brute=True)
+        assert np.array_equal(occ_b[~near].astype(bool), expect[~near]), (cfg, f)
+
+
+@pytest.mark.parametrize("cfg", list(CONFIGS))
+def test_any_hit_matches_reference_fixture(ctx, scenes, cfg):
+    g = np.load(os.path.join(GOLDEN, f"rays_{cfg}.npz"))
+    _, _, sid = scenes[cfg]
+    for k, tmax in enumerate(g["occluded_tmax"]):
+        r = g["rays"].copy()
+        r[:, 3] = 1e-6
+        r[:, 7] = tmax
+        occ = ctx.trace_any(sid, r)
+        ref = g["occluded"][:, k]
+        t = np.where(g["hit"] == 1, g["t"], np.inf)
+        near = np.abs(t - tmax) <= 1e-5 * tmax
+        assert np.mean(occ[~near] == ref[~near]) >= 0.999
+
+
+def test_edge_cases(ctx):
+    mat = '"materials": {"m": {"type": "lambertian"}}'
+    # Empty scene: everything misses.
+    empty = ctx.upload(rtg.parse_scene("{" + mat + "}"))
+    rays = np.zeros((64, 8), np.float32)
+    rays[:, 4] = 1
+    rays[:, 7] = 1e30
+    t, prim, plane, _ = ctx.trace_closest(empty, rays)
+    assert (prim == -1).all()
+    assert not ctx.trace_any(empty, rays).any()
+    # Zero rays.
+    t, prim, plane, _ = ctx.trace_closest(empty, np.zeros((0, 8), np.float32))
+    assert len(prim) == 0
+    # Single primitive (the root is a leaf) and axis-parallel rays, also through a plane.
+    one = ctx.upload(rtg.parse_scene("{" + mat + ', "objects": [{"type": "sphere", "center": [0,0,-5], "material": "m"},'
+                                     '{"type": "plane", "point": [0,-1,0], "normal": [0,1,0], "material": "m"}]}'))
+    r = np.array([[0, 0, 0, 1e-6, 0, 0, -1, 1e30],     # head-on: t = 4
+                  [0, 2, 0, 1e-6, 0, 0, -1, 1e30],     # misses the sphere, parallel to the plane
+                  [0, 0, -5, 1e-6, 0, 0, -1, 1e30],    # from inside: far root t = 1
+                  [1, 0, 0, 1e-6, 0, 0, -1, 1e30],     # tangent: t = 5
+                  [0, 1, 0, 1e-6, 0, -1, 0, 1e30]],    # straight down onto the plane: t = 2
+                 np.float32)
+    t, prim, plane, _ = ctx.trace_closest(one, r)
+    assert prim.tolist() == [0, -1, 0, 0, 0] and plane.tolist() == [0, 0, 0, 0, 1]
+    assert np.allclose(t[[0, 2, 4]], [4, 1, 2], rtol=1e-6) and abs(t[3] - 5) < 1e-2
+    # Tiny far sphere (stable quadratic).
+    tiny = ctx.upload(rtg.parse_scene("{" + mat + ', "objects": [{"type": "sphere", "center": [0,0,-1e4], '
+                                      '"radius": 1e-3, "material": "m"}]}'))
+    t, prim, _, _ = ctx.trace_closest(tiny, r[:1])
+    assert prim[0] == 0 and abs(t[0] - (1e4 - 1e-3)) <= 1e-6 * 1e4
+    # 1000 identical boxes: every primitive reachable, the lowest id wins the exact tie in brute force.
+    objs = ",".join('{"type": "sphere", "center": [0.5,0.5,0.5], "radius": 0.5, "material": "m"}' for _ in range(1000))
+    same = ctx.upload(rtg.parse_scene("{" + mat + ', "objects": [' + objs + "]}"))
+    q = np.array([[0.5, 0.5, -5, 1e-6, 0, 0, 1, 1e30]], np.float32)
+    t, prim, _, _ = ctx.trace_closest(same, q)
+    tb, pb, _, _ = ctx.trace_closest(same, q, brute=True)
+    assert abs(t[0] - 5) < 1e-5 and pb[0] == 0 and t[0] == tb[0]

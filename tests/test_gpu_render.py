@@ -1,0 +1,244 @@
+"""GPU rendering through the C ABI: unbiasedness on analytic scenes, statistics
+against the oracle and the reference's converged images, determinism, batched ==
+plain, the progressive pass schedule and cancellation. Known answers restate the
+reference's integration tests (tests/test_render.cpp:27-278)."""
+import ctypes
+import json
+import os
+import threading
+import time
+
+import numpy as np
+import pytest
+
+import rtg
+import rtoracle
+import workloads
+from conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+
+def render(ctx, scene, opts=None, on_pass=None, cancel=None):
+    sid = ctx.load_json(json.dumps(scene))
+    st = ctx.scene_settings(sid)
+    prog = ctx.render(sid, st, opts or rtg.RenderOptions(), on_pass, cancel)
+    s, q, n = ctx.framebuffer_moments(-1, st.width, st.height)
+    stats = ctx.stats()
+    ctx.release(sid)
+    return prog, s, q, n, stats
+
+
+def mean_luminance(s, n):
+    return float((s[..., 1] / n).mean())
+
+
+def sphere_light_over_plane(nee: bool) -> dict:
+    return {"camera": {"look_from": [3, 3, 0], "look_at": [0, 0, 0], "vfov": 0.2},
+            "background": {"type": "solid", "color": [0, 0, 0]},
+            "render": {"width": 4, "height": 4, "spp": 4096 if nee else 65536, "max_depth": 16,
+                       "light_sampling": nee},
+            "materials": {"plane": {"type": "lambertian", "albedo": 0.8},
+                          "glow": {"type": "emissive", "color": 1, "intensity": 4}},
+            "objects": [{"type": "plane", "point": [0, 0, 0], "normal": [0, 1, 0], "material": "plane"},
+                        {"type": "sphere", "center": [0, 2, 0], "radius": 0.5, "material": "glow"}]}
+
+
+@pytest.mark.parametrize("nee,tol", [(True, 0.01), (False, 0.03)])
+def test_sphere_light_over_plane_converges_to_analytic(ctx, nee, tol):
+    # a * Le * (r/d)^2 = 0.8 * 4 * 0.25 / 4 = 0.2
+    prog, s, q, n, stats = render(ctx, sphere_light_over_plane(nee))
+    assert prog.finished and stats["invalid_samples"] == 0
+    assert abs(mean_luminance(s, n) - 0.2) <= tol * 0.2
+
+
+@pytest.mark.parametrize("nee", [True, False])
+def test_ball_inside_two_sided_emitter_is_exact(ctx, nee):
+    scene = {"camera": {"look_from": [0, 0, 2.5], "look_at": [0, 0, 0], "vfov": 5},
+             "render": {"width": 4, "height": 4, "spp": 512, "light_sampling": nee},
+             "materials": {"ball": {"type": "lambertian", "albedo": 0.6},
+                           "shell": {"type": "emissive", "color": 1, "intensity": 2, "two_sided": True}},
+             "objects": [{"type": "sphere", "center": [0, 0, 0], "radius": 1, "material": "ball"},
+                         {"type": "sphere", "center": [0, 0, 0], "radius": 5, "material": "shell"}]}
+    _, s, q, n, _ = render(ctx, scene)
+    assert abs(mean_luminance(s, n) - 1.2) <= 0.01 * 1.2
+
+
+def test_uniform_sky_over_diffuse_plane(ctx):
+    scene = sphere_light_over_plane(True)
+    scene["objects"].pop()
+    scene["background"] = {"type": "solid", "color": [0.5, 0.5, 0.5]}
+    scene["render"]["spp"] = 2048
+    _, s, q, n, _ = render(ctx, scene)
+    assert abs(mean_luminance(s, n) - 0.4) <= 0.02 * 0.4
+
+
+def test_light_sampling_and_bsdf_sampling_agree(ctx):
+    a = workloads.cornell(width=16, height=16, spp=1024)
+    b = json.loads(json.dumps(a))
+    b["render"]["light_sampling"] = False
+    _, sa, _, na, _ = render(ctx, a)
+    _, sb, _, nb, _ = render(ctx, b)
+    la, lb = mean_luminance(sa, na), mean_luminance(sb, nb)
+    assert abs(la - lb) <= 0.04 * lb, (la, lb)
+
+
+def test_point_light_inverse_square_and_hard_shadow(ctx):
+    """Direct integrator, one sample straight down: L = albedo/pi * I/d^2 = 2/pi."""
+    scene = {"camera": {"look_from": [0, 1, 0], "look_at": [0, 0, 0], "vup": [0, 0, 1], "vfov": 0.01},
+             "render": {"width": 1, "height": 1, "spp": 1, "integrator": "direct"},
+             "background": {"type": "solid", "color": [0, 0, 0]},
+             "materials": {"white": {"type": "lambertian", "albedo": 1}},
+             "objects": [{"type": "plane", "point": [0, 0, 0], "normal": [0, 1, 0], "material": "white"}],
+             "lights": [{"type": "point", "position": [0, 2, 0], "intensity": [8, 8, 8]}]}
+    _, s, _, n, _ = render(ctx, scene)
+    assert abs(s[0, 0, 0] - 2 / np.pi) <= 1e-4
+    scene["camera"]["look_from"] = [0, 0.5, 0]
+    scene["objects"].append({"type": "sphere", "center": [0, 1, 0], "radius": 0.2, "material": "white"})
+    _, s, _, n, _ = render(ctx, scene)
+    assert s[0, 0, 0] == 0
+
+
+def test_matches_oracle_statistics_on_the_same_samples(ctx):
+    scene = workloads.cornell(width=48, height=48, spp=64)
+    _, s, q, n, stats = render(ctx, scene)
+    o = rtoracle.OracleScene(rtg.parse_scene(json.dumps(scene)).view())
+    cs, cq, cst = o.render()
+    spp = 64
+    for c in range(3):
+        g, m = s[..., c].mean() / spp, cs[..., c].mean() / spp
+        var_g = (q[..., c] / spp - (s[..., c] / spp) ** 2).sum() / spp / s[..., c].size ** 2
+        var_c = (cq[..., c] / spp - (cs[..., c] / spp) ** 2).sum() / spp / cs[..., c].size ** 2
+        assert abs(g - m) <= 3 * np.sqrt(var_g + var_c), (c, g, m)
+    assert stats["invalid_samples"] == 0
+    # Same workload: the GPU traces as many closest-hit rays as the CPU within noise.
+    assert abs(stats["rays"] - cst["rays"]) <= 0.02 * cst["rays"]
+
+
+@pytest.mark.parametrize("cfg", ["cornell", "spheres", "mesh"])
+def test_rmse_against_converged_reference_matches_cpu(ctx, cfg):
+    """GPU at 64 spp vs the reference's 4096-spp image: per-channel mean within 3
+    sigma of the Monte Carlo error, and RMSE within 5% of the CPU image's RMSE."""
+    g = np.load(os.path.join(GOLDEN, f"converged_{cfg}.npz"))
+    scene = json.loads(str(g["scene"]))
+    scene["render"]["spp"] = int(g["cpu_spp"])
+    scene["render"]["seed"] = int(g["cpu_seed"])
+    _, s, q, n, stats = render(ctx, scene, rtg.RenderOptions(progressive=False))
+    spp = int(g["cpu_spp"])
+    gpu = s / spp
+    ref, cpu = g["ref_mean"].astype(np.float64), g["cpu_mean"].astype(np.float64)
+    rs = int(g["ref_spp"])
+    P = gpu[..., 0].size
+    for c in range(3):
+        var_g = (q[..., c] / spp - gpu[..., c] ** 2).clip(0).sum() / spp / P ** 2
+        var_r = (g["ref_sumsq"][..., c] / rs - ref[..., c] ** 2).clip(0).sum() / rs / P ** 2
+        assert abs(gpu[..., c].mean() - ref[..., c].mean()) <= 3 * np.sqrt(var_g + var_r) + 1e-12, c
+    rmse_gpu = np.sqrt(((gpu - ref) ** 2).mean())
+    rmse_cpu = np.sqrt(((cpu - ref) ** 2).mean())
+    print(cfg, "rmse gpu", rmse_gpu, "cpu", rmse_cpu)
+    assert abs(rmse_gpu / rmse_cpu - 1) <= 0.05
+    assert stats["invalid_samples"] == 0
+
+
+def test_bit_identical_across_runs_and_seeds_differ(ctx):
+    scene = workloads.sphere_field(width=64, height=48, spp=8)
+    a = render(ctx, scene)
+    b = render(ctx, scene, rtg.RenderOptions(progressive=True, max_pass_spp=2))
+    assert a[1].tobytes() == b[1].tobytes() and a[2].tobytes() == b[2].tobytes()
+    scene["render"]["seed"] = 99
+    c = render(ctx, scene)
+    assert a[1].tobytes() != c[1].tobytes()
+
+
+def test_batch_is_bit_identical_to_plain(ctx):
+    scenes = [workloads.cornell(width=40, height=32, spp=6), workloads.sphere_field(width=24, height=24, spp=11),
+              workloads.mesh_stress(width=16, height=20, spp=5), workloads.mix_scene(4)]
+    scenes[3]["render"].update(width=20, height=20, spp=3)
+    sids = [ctx.load_json(json.dumps(s)) for s in scenes]
+    settings = [ctx.scene_settings(i) for i in sids]
+    plain = []
+    for sid, st in zip(sids, settings):
+        ctx.render(sid, st)
+        plain.append(ctx.framebuffer_moments(-1, st.width, st.height))
+    progs = ctx.render_batch(sids, settings)
+    assert all(p.finished for p in progs)
+    for j, st in enumerate(settings):
+        s, q, n = ctx.framebuffer_moments(j, st.width, st.height)
+        assert s.tobytes() == plain[j][0].tobytes() and q.tobytes() == plain[j][1].tobytes(), j
+        assert (n == st.spp).all()
+    # A different batch composition leaves each job's result unchanged.
+    ctx.render_batch(sids[::-1], settings[::-1])
+    s, q, n = ctx.framebuffer_moments(len(sids) - 1, settings[0].width, settings[0].height)
+    assert s.tobytes() == plain[0][0].tobytes()
+    for sid in sids:
+        ctx.release(sid)
+
+
+def test_progressive_pass_schedule(ctx):
+    scene = workloads.cornell(width=32, height=32, spp=20)
+    seen = []
+
+    def on_pass(p):
+        seen.append(p.spp_done)
+        _, _, n = ctx.framebuffer_moments(-1, 32, 32)
+        assert (n == p.spp_done).all()
+
+    prog, s, q, n, _ = render(ctx, scene, rtg.RenderOptions(progressive=True, max_pass_spp=8), on_pass)
+    assert seen == [1, 2, 4, 8, 16, 20] and prog.finished and prog.pass_ == 6
+
+
+def test_cancellation_stops_quickly_and_leaves_a_consistent_buffer(ctx):
+    scene = workloads.cornell(width=128, height=128, spp=100000)
+    flag = ctypes.c_int32(0)
+    calls = []
+    timer = threading.Timer(0.15, lambda: setattr(flag, "value", 1))
+    t0 = time.time()
+    timer.start()
+    prog, s, q, n, _ = render(ctx, scene, None, lambda p: calls.append(p.spp_done), flag)
+    elapsed = time.time() - t0
+    timer.join()
+    assert prog.cancelled and not prog.finished
+    assert elapsed < 0.15 + 1.0
+    assert calls and (n == prog.spp_done).all()
+    assert np.isfinite(s).all()
+    # The context stays usable: a small render afterwards completes.
+    prog2, *_ = render(ctx, workloads.cornell(width=16, height=16, spp=4))
+    assert prog2.finished and not prog2.cancelled
+
+
+def test_normals_and_direct_integrators_match_oracle(ctx):
+    for integ in ("normals", "direct"):
+        scene = workloads.cornell(width=32, height=32, spp=4)
+        scene["render"]["integrator"] = integ
+        _, s, q, n, stats = render(ctx, scene)
+        o = rtoracle.OracleScene(rtg.parse_scene(json.dumps(scene)).view())
+        cs, cq, _ = o.render()
+        gpu, cpu = s / 4, cs / 4
+        if integ == "normals":
+            close = np.abs(gpu - cpu).max(-1) <= 1e-4
+            assert close.mean() >= 0.98, close.mean()
+        else:
+            assert np.allclose(gpu.mean((0, 1)), cpu.mean((0, 1)), rtol=0.02)
+        assert stats["invalid_samples"] == 0
+
+
+def test_image_is_the_reference_tone_map_of_the_means(ctx):
+    scene = workloads.sphere_field(width=48, height=40, spp=4)
+    sid = ctx.load_json(json.dumps(scene))
+    st = ctx.scene_settings(sid)
+    ctx.render(sid, st)
+    mean = ctx.framebuffer_mean(-1, st.width, st.height)
+    for tm, op in (("clamp", 0), ("reinhard", 1), ("aces", 2)):
+        img = ctx.image(-1, st.width, st.height, tm, 1.3)
+        ref = rtoracle.tone_map_srgb8(mean.reshape(-1, 3), op, 1.3).reshape(img.shape)
+        diff = np.abs(img.astype(int) - ref.astype(int))
+        assert diff.max() <= 1 and (diff > 0).mean() <= 1e-3, tm
+    ctx.release(sid)
+
+
+@pytest.mark.parametrize("make", [workloads.cornell, workloads.sphere_field, workloads.mesh_stress])
+def test_workloads_render_with_no_invalid_samples(ctx, make):
+    scene = make()
+    scene["render"].update(width=64, height=64, spp=8)
+    prog, s, q, n, stats = render(ctx, scene)
+    assert prog.finished and stats["invalid_samples"] == 0 and np.isfinite(s).all() and s.max() > 0
