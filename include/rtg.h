@@ -201,6 +201,23 @@ int rtg_trace_closest(rtg_context* ctx, rtg_scene_id scene, const float* rays, u
 int rtg_trace_any(rtg_context* ctx, rtg_scene_id scene, const float* rays, uint64_t n, int32_t brute,
                   uint8_t* occluded);
 
+/* No counterpart in the reference. rtg_trace_closest for callers that must not
+ * allocate device memory during the call: a loop sharing the GPU with other
+ * streams (freeing device memory synchronises the whole device), a host that
+ * pre-reserves all device memory in its own pool, or code that issues work while
+ * a stream is being captured, where allocation calls are refused. Same arguments
+ * and results; at most RTG_NOALLOC_MAX_RAYS rays per call (RTG_ERR_LIMIT beyond).
+ * Its rays and results pass through one static device array of about 13 MiB that
+ * the library reserves on every GPU it runs on until the process exits. The first
+ * call on a device sets that array up (make it before any stream capture). All
+ * calls share the array, so calls whose GPU work overlaps (other streams or
+ * contexts on the same device) race. t is refined in double only when the
+ * scene's double-precision copy is already resident (after an rtg_trace_closest
+ * call on the same scene); this entry point never uploads it itself. */
+#define RTG_NOALLOC_MAX_RAYS 262144
+int rtg_trace_closest_noalloc(rtg_context* ctx, rtg_scene_id scene, const float* rays, uint64_t n, int32_t brute,
+                              float* t, int32_t* prim, int32_t* is_plane, float* bary);
+
 /* ---- engine tuning (no reference counterpart) ---- */
 typedef struct rtg_tuning {
   uint32_t pool_paths;       /* wavefront path slots (default 1 << 20) */

@@ -13,6 +13,7 @@
 #include <sstream>
 #include <string>
 
+#include "device/noalloc.h"
 #include "host/engine.hpp"
 #include "host/scene_io.hpp"
 
@@ -517,6 +518,24 @@ int rtg_trace_any(rtg_context* ctx, rtg_scene_id scene, const float* rays, uint6
   return guarded(ctx, [&]() {
     if ((!rays || !occluded) && n) throw std::invalid_argument("null argument");
     ctx->engine->trace_any(scene, rays, n, brute != 0, occluded);
+    return RTG_OK;
+  });
+}
+
+int rtg_trace_closest_noalloc(rtg_context* ctx, rtg_scene_id scene, const float* rays, uint64_t n, int32_t brute,
+                              float* t, int32_t* prim, int32_t* is_plane, float* bary) {
+  static_assert(RTG_NOALLOC_MAX_RAYS == rtg::kNoAllocMaxRays, "header and scratch sizes disagree");
+  return guarded(ctx, [&]() {
+    if (!rays && n) throw std::invalid_argument("null rays");
+    if (n > rtg::kNoAllocMaxRays) {
+      ctx->error = "rtg_trace_closest_noalloc: " + std::to_string(n) + " rays exceed the limit of " +
+                   std::to_string(rtg::kNoAllocMaxRays) + " per call (RTG_NOALLOC_MAX_RAYS)";
+      return RTG_ERR_LIMIT;
+    }
+    const rtg::RtgSceneDev d = ctx->engine->query_descriptor(scene, brute != 0);
+    const cudaError_t e = rtg::noalloc_trace_closest(ctx->engine->device(), d, rays, n, brute, t, prim, is_plane,
+                                                     bary, ctx->engine->stream());
+    if (e != cudaSuccess) throw rtg::CudaFailure(std::string("rtg_trace_closest_noalloc: ") + cudaGetErrorString(e));
     return RTG_OK;
   });
 }

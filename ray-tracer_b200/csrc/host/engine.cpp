@@ -614,3 +614,14 @@ void Engine::trace_any(int scene_id, const float* rays, std::uint64_t n, bool br
 }
 
 }  // namespace rtg
+
+namespace rtg {
+
+RtgSceneDev Engine::query_descriptor(int scene_id, bool brute) {
+  GpuScene& sc = scene(scene_id);
+  RenderSettings s = sc.host.settings;
+  s.use_bvh = !brute;
+  return job_descriptor(sc, s, GpuFrame{});
+}
+
+}  // namespace rtg

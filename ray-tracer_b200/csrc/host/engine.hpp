@@ -132,6 +132,8 @@ class Engine {
   void trace_closest(int scene_id, const float* rays, std::uint64_t n, bool brute, float* t, std::int32_t* prim,
                      std::int32_t* is_plane, float* bary);
   void trace_any(int scene_id, const float* rays, std::uint64_t n, bool brute, std::uint8_t* occluded);
+  // Descriptor of one scene for a ray query (a host struct; allocates nothing).
+  RtgSceneDev query_descriptor(int scene_id, bool brute);
 
  private:
   struct Wave;

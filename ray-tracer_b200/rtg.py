@@ -35,6 +35,7 @@ RTG_ERR_NO_DEVICE = -4
 RTG_ERR_DEVICE = -5
 RTG_ERR_BUSY = -6
 RTG_ERR_LIMIT = -7
+NOALLOC_MAX_RAYS = 262144
 
 INTEGRATORS = {"path": 0, "direct": 1, "normals": 2}
 TONE_MAPS = {"clamp": 0, "reinhard": 1, "aces": 2}
@@ -138,6 +139,9 @@ _SIGNATURES = {
                                     C.POINTER(C.c_float)]),
     "rtg_trace_any": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_float), C.c_uint64, C.c_int32,
                                 C.POINTER(C.c_uint8)]),
+    "rtg_trace_closest_noalloc": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_float), C.c_uint64, C.c_int32,
+                                            C.POINTER(C.c_float), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                            C.POINTER(C.c_float)]),
     "rtg_get_tuning": (C.c_int, [C.c_void_p, C.POINTER(_Tuning)]),
     "rtg_set_tuning": (C.c_int, [C.c_void_p, C.POINTER(_Tuning)]),
     "rtg_encode_png": (C.c_int64, [C.POINTER(C.c_uint8), C.c_int32, C.c_int32, C.POINTER(C.c_uint8), C.c_size_t]),
@@ -449,6 +453,20 @@ class Context:
         self._check(lib().rtg_trace_closest(self._h, scene_id, _ptr(rays, C.c_float), n, int(brute),
                                             _ptr(t, C.c_float), _ptr(prim, C.c_int32), _ptr(plane, C.c_int32),
                                             _ptr(bary, C.c_float)))
+        return t, prim, plane, bary
+
+    def trace_closest_noalloc(self, scene_id: int, rays: np.ndarray, brute: bool = False):
+        """trace_closest through the entry point that allocates no device memory
+        (at most NOALLOC_MAX_RAYS rays per call)."""
+        rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+        n = rays.shape[0]
+        t = np.zeros(n, np.float32)
+        prim = np.zeros(n, np.int32)
+        plane = np.zeros(n, np.int32)
+        bary = np.zeros((n, 2), np.float32)
+        self._check(lib().rtg_trace_closest_noalloc(self._h, scene_id, _ptr(rays, C.c_float), n, int(brute),
+                                                    _ptr(t, C.c_float), _ptr(prim, C.c_int32),
+                                                    _ptr(plane, C.c_int32), _ptr(bary, C.c_float)))
         return t, prim, plane, bary
 
     def trace_any(self, scene_id: int, rays: np.ndarray, brute: bool = False) -> np.ndarray:
