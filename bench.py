@@ -44,6 +44,8 @@ def args():
     p.add_argument("--workload", choices=["mix", "cornell", "spheres", "mesh"], default="mix")
     p.add_argument("--no-plain", action="store_true", help="skip the plain one-scene-per-launch comparison")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--single-pass", action="store_true",
+                   help="render every scene in one pass (the CPU baseline's --single-pass); keeps the pool full")
     return p.parse_args()
 
 
@@ -242,7 +244,7 @@ def run_rtg(a, dist, scenes, desc):
 
     dev = dist.local
     ctx = rtg.Context(dev)
-    opts = rtg.RenderOptions(progressive=True, max_pass_spp=32)
+    opts = rtg.RenderOptions(progressive=not a.single_pass, max_pass_spp=32)
     hosts = [rtg.parse_scene(json.dumps(s)) for s in scenes]
     sids = [ctx.upload(h) for h in hosts]
     settings = [ctx.scene_settings(i) for i in sids]
@@ -355,7 +357,8 @@ def run_rtg(a, dist, scenes, desc):
             "vs_baseline": None, "dtype": "fp32 (f64 accumulation)", "data": "synthetic (seeded scene generators)",
             "config": {"workload": desc, "scenes": len(scenes), "samples_per_step": samples_of(scenes),
                        "primitives": int(sum(len(h.view()["prims"]) for h in hosts)) if len(hosts) <= 64 else None,
-                       "progressive": True, "max_pass_spp": 32, "pool_paths": ctx.tuning()["pool_paths"],
+                       "progressive": not a.single_pass, "max_pass_spp": 32,
+                       "pool_paths": ctx.tuning()["pool_paths"],
                        "mode": "batched (one shared wavefront per pass)" if batched else "plain",
                        "parallelism": f"replicas x{dist.world}",
                        "l2": f"inputs larger than L2: {scene_bytes / 2**20:.0f} MiB of scenes + GBs of per-pass "
