@@ -45,7 +45,10 @@ def args():
     p.add_argument("--no-plain", action="store_true", help="skip the plain one-scene-per-launch comparison")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--single-pass", action="store_true",
-                   help="render every scene in one pass (the CPU baseline's --single-pass); keeps the pool full")
+                   help="render every scene in one pass (the CPU baseline's --single-pass)")
+    p.add_argument("--serve-seconds", type=float, default=10.0,
+                   help="length of the serving run (Poisson arrivals over 32 resident scenes of the mix)")
+    p.add_argument("--no-serve", action="store_true", help="skip the serving run")
     return p.parse_args()
 
 
@@ -331,7 +334,7 @@ def run_rtg(a, dist, scenes, desc):
     avg_ms = t_st["extend_ms"] / launches_ext
     achieved = ext_bytes / launches_ext / (avg_ms / 1e3) / 1e9
     peak, peak_src = peaks()
-    kernel_total = t_st["extend_ms"] + t_st["shade_ms"] + t_st["shadow_ms"] + t_st["accumulate_ms"]
+    kernel_total = t_st["extend_ms"] + t_st["shade_ms"] + t_st["shadow_ms"] + t_st["accumulate_ms"] + t_st["plan_ms"]
     roofline = {
         "kernel": "k_extend (closest-hit BVH traversal + camera-path generation)",
         "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -340,8 +343,16 @@ def run_rtg(a, dist, scenes, desc):
         "share_of_kernel_time": t_st["extend_ms"] / kernel_total if kernel_total else None,
         "per_ray": {"nodes": c_st["node_visits"] / max(1, c_st["rays"]),
                     "prim_tests": c_st["prim_tests"] / max(1, c_st["rays"])},
-        "kernel_ms": {k: t_st[k] for k in ("extend_ms", "shade_ms", "shadow_ms", "accumulate_ms")},
+        "kernel_ms": {k: t_st[k] for k in ("extend_ms", "shade_ms", "shadow_ms", "accumulate_ms", "plan_ms")},
     }
+
+    # Serving: Poisson arrivals of previews and finals over 32 resident scenes.
+    serve = None
+    if batched and not a.no_serve and a.serve_seconds > 0:
+        import serving
+
+        serve = serving.serve(ctx, sids[:32], seconds=a.serve_seconds, rate=200.0, preview_share=0.9, seed=2025)
+        serve["scenes"] = min(32, len(sids))
 
     cpu = None
     if dist.rank == 0 and dist.world == 1 and not a.no_cpu_baseline:
@@ -359,7 +370,8 @@ def run_rtg(a, dist, scenes, desc):
                        "primitives": int(sum(len(h.view()["prims"]) for h in hosts)) if len(hosts) <= 64 else None,
                        "progressive": not a.single_pass, "max_pass_spp": 32,
                        "pool_paths": ctx.tuning()["pool_paths"],
-                       "mode": "batched (one shared wavefront per pass)" if batched else "plain",
+                       "mode": ("batched: every scene's passes in one continuous wavefront" if batched
+                                else "plain: one scene, its passes overlapping in the wavefront"),
                        "parallelism": f"replicas x{dist.world}",
                        "l2": f"inputs larger than L2: {scene_bytes / 2**20:.0f} MiB of scenes + GBs of per-pass "
                              "radiance and path state rewritten every step (L2 126 MiB)"},
@@ -370,6 +382,7 @@ def run_rtg(a, dist, scenes, desc):
             "roofline": roofline,
             "cpu_baseline": cpu,
             "plain": plain,
+            "serving": serve,
             "invalid_samples": c_st["invalid_samples"],
         }
         print(json.dumps(line), flush=True)

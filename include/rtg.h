@@ -73,6 +73,7 @@ typedef struct rtg_stats {
   double elapsed_ms;        /* host wall time of the render call */
   double device_ms;         /* CUDA-event time on the context's stream, first to last launch */
   double extend_ms, shade_ms, shadow_ms, accumulate_ms, direct_ms; /* per-kernel event time (time_kernels) */
+  double plan_ms;           /* generation-plan kernel (time_kernels) */
 } rtg_stats;
 
 /* SceneBuildInfo (include/raytracer/core/scene.hpp:24-27) and BvhBuildStats
@@ -83,8 +84,10 @@ typedef struct rtg_scene_info {
   double bvh_build_ms, bvh_sah_cost;
 } rtg_scene_info;
 
-/* Called on the rendering thread after each pass, with no kernel of this render
- * in flight: the framebuffer accessors below may be called from inside it.
+/* Called on the rendering thread after each pass, when the framebuffer holds
+ * exactly the passes reported so far: the framebuffer accessors below may be
+ * called from inside it (later passes may be tracing meanwhile; they do not touch
+ * the framebuffer until the callback returns).
  * ProgressFn (include/raytracer/rendering/renderer.hpp:46-48). */
 typedef void (*rtg_pass_fn)(void* user, const rtg_progress* progress);
 
@@ -222,13 +225,56 @@ int rtg_trace_closest_noalloc(rtg_context* ctx, rtg_scene_id scene, const float*
 typedef struct rtg_tuning {
   uint32_t pool_paths;       /* wavefront path slots (default 1 << 20) */
   uint32_t block;            /* threads per block of the wavefront kernels: 64, 128, 256 */
-  uint64_t max_pass_samples; /* radiance slots per pass (default 1 << 27) */
+  uint64_t max_pass_samples; /* radiance slots shared by all passes in flight (default 1 << 27) */
   int32_t extend_blocks, shade_blocks, shadow_blocks; /* 0 = occupancy-derived persistent grid */
   int32_t time_kernels;      /* CUDA events around each kernel (rtg_stats.*_ms) */
   int32_t count_traversal;   /* node / primitive counters (rtg_stats.node_visits, prim_tests) */
+  uint32_t backlog_pools;    /* samples kept open for generation, in pools (default 3) */
+  uint32_t reserved;
+  uint64_t serve_budget_bytes; /* admission limit of the open requests' device footprint */
+  uint64_t serve_reserve_bytes; /* part of that budget only priority-0 requests (previews) may use */
 } rtg_tuning;
 int rtg_get_tuning(rtg_context* ctx, rtg_tuning* out);
 int rtg_set_tuning(rtg_context* ctx, const rtg_tuning* in);
+
+/* ---- serving (no reference counterpart: the reference renders one scene per
+ * Renderer). Requests on resident scenes share one continuous wavefront with each
+ * other: a request's passes are folded into its own framebuffer in pass order, so
+ * its image is bit-identical to rendering it alone with rtg_render. Lower
+ * priority values get free path slots first (previews before finals). ---- */
+typedef int32_t rtg_request_id;
+typedef struct rtg_request_event {
+  rtg_request_id request;
+  int32_t reserved;
+  rtg_progress progress; /* after the pass that just finished */
+} rtg_request_event;
+
+/* Admission by footprint: RTG_ERR_LIMIT (and nothing opened) when the request's
+ * framebuffer plus its first pass's radiance would take the open requests past
+ * rtg_tuning.serve_budget_bytes, or, for priority > 0, past that budget less
+ * serve_reserve_bytes (so previews are never locked out by finals).
+ * settings = NULL: the scene's own. The request starts tracing on the next
+ * rtg_serve_pump. */
+int rtg_request_submit(rtg_context* ctx, rtg_scene_id scene, const rtg_settings* settings,
+                       const rtg_render_options* opts, int32_t priority, rtg_request_id* out);
+/* Runs the wavefront for up to budget_ms of host time, or until the first pass
+ * event when return_on_event is set, or until no request has work. Writes up to
+ * cap events in completion order (*n of them); events that do not fit are kept
+ * for the next call. */
+int rtg_serve_pump(rtg_context* ctx, double budget_ms, int32_t return_on_event, rtg_request_event* events,
+                   int32_t cap, int32_t* n);
+/* Stops a request; passes already reported stay in its framebuffer. */
+int rtg_request_cancel(rtg_context* ctx, rtg_request_id request);
+/* Frees a finished or cancelled request (RTG_ERR_BUSY while passes are in flight). */
+int rtg_request_release(rtg_context* ctx, rtg_request_id request);
+int rtg_request_progress(rtg_context* ctx, rtg_request_id request, rtg_progress* out);
+/* The request's framebuffer: means (3 doubles per pixel) or the tone-mapped RGB8
+ * image (tone_map < 0: the request's own settings, as rtg_image_rgb8). */
+int rtg_request_mean(rtg_context* ctx, rtg_request_id request, double* rgb);
+int rtg_request_image_rgb8(rtg_context* ctx, rtg_request_id request, int32_t tone_map, double exposure, uint8_t* rgb);
+/* Device bytes the open requests hold against the admission budget, the number
+ * of open requests, and how many of them still have passes to render or in flight. */
+int rtg_serve_footprint(rtg_context* ctx, uint64_t* bytes, int32_t* open_requests, int32_t* rendering);
 
 /* ---- image output (encode_png / write_image, src/io/image_io.cpp:45-70) ---- */
 /* PNG bytes of an RGB8 image into out (cap bytes); returns the PNG size, or a

@@ -7,7 +7,10 @@
 
 #include <cmath>
 #include <cstring>
+#include <deque>
 #include <exception>
+#include <stdexcept>
+#include <unordered_map>
 #include <fstream>
 #include <memory>
 #include <sstream>
@@ -34,6 +37,14 @@ struct rtg_context {
   bool busy = false;
   // Settings of the last plain render (for rtg_image_rgb8 with tone_map < 0).
   std::vector<rtg::RenderSettings> last_settings;
+  // Serving: events not yet handed out, the admission budget and what the open
+  // requests hold against it.
+  std::deque<rtg_request_event> pending;
+  std::uint64_t serve_budget = 16ull << 30;
+  std::uint64_t serve_reserve = 2ull << 30;
+  std::uint64_t serve_used = 0;
+  std::unordered_map<int, std::uint64_t> footprint;
+  std::unordered_map<int, rtg::RenderSettings> request_settings;
 };
 
 namespace {
@@ -121,6 +132,12 @@ int guarded(rtg_context* ctx, F&& body) {
   } catch (const std::invalid_argument& e) {
     ctx->error = e.what();
     return RTG_ERR_INVALID;
+  } catch (const std::length_error& e) {  // a fixed table is full
+    ctx->error = e.what();
+    return RTG_ERR_LIMIT;
+  } catch (const std::logic_error& e) {   // the call conflicts with work in flight
+    ctx->error = e.what();
+    return RTG_ERR_BUSY;
   } catch (const std::exception& e) {
     ctx->error = e.what();
     return RTG_ERR_SCENE;
@@ -398,6 +415,10 @@ int rtg_render(rtg_context* ctx, rtg_scene_id scene, const rtg_settings* setting
       const rtg_progress c = to_c(p);
       on_pass(user, &c);
     };
+    if (ctx->engine->open_requests() > 0) {
+      ctx->error = "rtg_render: serving requests are open on this context";
+      return RTG_ERR_BUSY;
+    }
     const rtg::RenderProgress p = ctx->engine->render(scene, s, o, cb, cancel);
     if (out) *out = to_c(p);
     return RTG_OK;
@@ -425,6 +446,10 @@ int rtg_render_batch(rtg_context* ctx, int32_t n, const rtg_scene_id* scenes, co
     BusyGuard guard(ctx);
     ctx->last_settings.clear();
     for (const auto& j : jobs) ctx->last_settings.push_back(j.settings);
+    if (ctx->engine->open_requests() > 0) {
+      ctx->error = "rtg_render_batch: serving requests are open on this context";
+      return RTG_ERR_BUSY;
+    }
     const std::vector<rtg::RenderProgress> p = ctx->engine->render_batch(jobs, o, cancel);
     if (out)
       for (int32_t j = 0; j < n; ++j) out[j] = to_c(p[static_cast<std::size_t>(j)]);
@@ -500,6 +525,7 @@ int rtg_render_stats(rtg_context* ctx, rtg_stats* out) {
     out->shadow_ms = s.shadow_ms;
     out->accumulate_ms = s.accumulate_ms;
     out->direct_ms = s.direct_ms;
+    out->plan_ms = s.plan_ms;
     return RTG_OK;
   });
 }
@@ -553,6 +579,9 @@ int rtg_get_tuning(rtg_context* ctx, rtg_tuning* out) {
     out->shadow_blocks = c.shape.shadow_blocks;
     out->time_kernels = c.time_kernels ? 1 : 0;
     out->count_traversal = c.count_traversal ? 1 : 0;
+    out->backlog_pools = c.backlog_pools;
+    out->serve_budget_bytes = ctx->serve_budget;
+    out->serve_reserve_bytes = ctx->serve_reserve;
     return RTG_OK;
   });
 }
@@ -562,10 +591,15 @@ int rtg_set_tuning(rtg_context* ctx, const rtg_tuning* in) {
     if (!in) throw std::invalid_argument("null argument");
     if (ctx->busy) return RTG_ERR_BUSY;
     if (in->block != 64 && in->block != 128 && in->block != 256) throw std::invalid_argument("block must be 64, 128 or 256");
-    if (in->pool_paths < 1024 || in->pool_paths > (1u << 26)) throw std::invalid_argument("pool_paths must be in [1024, 2^26]");
+    if (in->pool_paths < 1024 || in->pool_paths > (1u << 23)) throw std::invalid_argument("pool_paths must be in [1024, 2^23]");
     if (in->max_pass_samples < 1 || in->max_pass_samples > (1ull << 31)) throw std::invalid_argument("max_pass_samples must be in [1, 2^31]");
+    if (in->backlog_pools < 1 || in->backlog_pools > 64) throw std::invalid_argument("backlog_pools must be in [1, 64]");
     rtg::EngineConfig& c = ctx->engine->config();
-    const bool realloc = c.pool_paths != in->pool_paths;
+    const bool realloc = c.pool_paths != in->pool_paths || c.max_pass_samples != in->max_pass_samples;
+    if (realloc && ctx->engine->open_requests() > 0) {
+      ctx->error = "rtg_set_tuning: the pool cannot change while serving requests are open";
+      return RTG_ERR_BUSY;
+    }
     c.pool_paths = in->pool_paths;
     c.shape.extend_block = static_cast<int>(in->block);
     c.max_pass_samples = in->max_pass_samples;
@@ -574,7 +608,144 @@ int rtg_set_tuning(rtg_context* ctx, const rtg_tuning* in) {
     c.shape.shadow_blocks = in->shadow_blocks;
     c.time_kernels = in->time_kernels != 0;
     c.count_traversal = in->count_traversal != 0;
+    c.backlog_pools = in->backlog_pools;
+    if (in->serve_budget_bytes) ctx->serve_budget = in->serve_budget_bytes;
+    if (in->serve_reserve_bytes > ctx->serve_budget) throw std::invalid_argument("serve_reserve_bytes exceeds the budget");
+    ctx->serve_reserve = in->serve_reserve_bytes;
     if (realloc) ctx->engine->reset_wave();
+    return RTG_OK;
+  });
+}
+
+int rtg_request_submit(rtg_context* ctx, rtg_scene_id scene, const rtg_settings* settings,
+                       const rtg_render_options* opts, int32_t priority, rtg_request_id* out) {
+  return guarded(ctx, [&]() {
+    if (!out) throw std::invalid_argument("null argument");
+    if (ctx->busy) return RTG_ERR_BUSY;
+    if (settings)
+      if (const char* bad = settings_problem(*settings)) throw rtg::SceneError(bad);
+    rtg::JobSpec spec;
+    spec.scene_id = scene;
+    spec.settings = settings ? from_c(*settings) : ctx->engine->scene(scene).host.settings;
+    if (const char* bad = settings_problem(spec.settings)) throw rtg::SceneError(bad);
+    if (opts) {
+      spec.opts.progressive = opts->progressive != 0;
+      spec.opts.max_pass_spp = opts->max_pass_spp;
+    }
+    spec.priority = priority;
+    const std::uint64_t bytes = ctx->engine->request_bytes(spec);
+    const std::uint64_t limit = priority > 0 ? ctx->serve_budget - ctx->serve_reserve : ctx->serve_budget;
+    if (ctx->serve_used + bytes > limit) {
+      ctx->error = "rtg_request_submit: " + std::to_string(bytes) + " bytes would exceed the serving budget (" +
+                   std::to_string(ctx->serve_used) + " of " + std::to_string(limit) + " in use at priority " +
+                   std::to_string(priority) + ")";
+      return RTG_ERR_LIMIT;
+    }
+    const int h = ctx->engine->submit(spec);
+    ctx->footprint[h] = bytes;
+    ctx->serve_used += bytes;
+    ctx->request_settings[h] = spec.settings;
+    *out = h;
+    return RTG_OK;
+  });
+}
+
+int rtg_serve_pump(rtg_context* ctx, double budget_ms, int32_t return_on_event, rtg_request_event* events,
+                   int32_t cap, int32_t* n) {
+  return guarded(ctx, [&]() {
+    if (!n || (cap > 0 && !events)) throw std::invalid_argument("null argument");
+    if (ctx->busy) return RTG_ERR_BUSY;
+    *n = 0;
+    if (ctx->pending.empty() || !return_on_event) {
+      std::vector<rtg::Engine::PassEvent> ev;
+      ctx->engine->pump(budget_ms, return_on_event != 0, ev);
+      for (const auto& e : ev) {
+        rtg_request_event c{};
+        c.request = e.request;
+        c.progress = to_c(e.progress);
+        ctx->pending.push_back(c);
+      }
+    }
+    while (*n < cap && !ctx->pending.empty()) {
+      events[(*n)++] = ctx->pending.front();
+      ctx->pending.pop_front();
+    }
+    return RTG_OK;
+  });
+}
+
+int rtg_request_cancel(rtg_context* ctx, rtg_request_id request) {
+  return guarded(ctx, [&]() {
+    ctx->engine->cancel_request(request);
+    return RTG_OK;
+  });
+}
+
+int rtg_request_release(rtg_context* ctx, rtg_request_id request) {
+  return guarded(ctx, [&]() {
+    if (!ctx->engine->request_exists(request)) throw std::invalid_argument("unknown request " + std::to_string(request));
+    const rtg::RenderProgress& p = ctx->engine->request_progress(request);
+    if (!p.finished && !p.cancelled) {
+      ctx->error = "rtg_request_release: request " + std::to_string(request) + " is still rendering";
+      return RTG_ERR_BUSY;
+    }
+    try {
+      ctx->engine->release_request(request);
+    } catch (const std::logic_error& e) {
+      ctx->error = e.what();
+      return RTG_ERR_BUSY;
+    }
+    ctx->serve_used -= ctx->footprint[request];
+    ctx->footprint.erase(request);
+    ctx->request_settings.erase(request);
+    return RTG_OK;
+  });
+}
+
+int rtg_request_progress(rtg_context* ctx, rtg_request_id request, rtg_progress* out) {
+  return guarded(ctx, [&]() {
+    if (!out) throw std::invalid_argument("null argument");
+    *out = to_c(ctx->engine->request_progress(request));
+    return RTG_OK;
+  });
+}
+
+int rtg_request_mean(rtg_context* ctx, rtg_request_id request, double* rgb) {
+  return guarded(ctx, [&]() {
+    if (!rgb) throw std::invalid_argument("null argument");
+    ctx->engine->read_mean_frame(ctx->engine->request_frame(request), rgb);
+    return RTG_OK;
+  });
+}
+
+int rtg_request_image_rgb8(rtg_context* ctx, rtg_request_id request, int32_t tone_map, double exposure, uint8_t* rgb) {
+  return guarded(ctx, [&]() {
+    if (!rgb) throw std::invalid_argument("null argument");
+    const rtg::GpuFrame& f = ctx->engine->request_frame(request);
+    rtg::ToneMap op = rtg::ToneMap::Clamp;
+    double ex = exposure;
+    if (tone_map < 0) {
+      const rtg::RenderSettings& s = ctx->request_settings.at(request);
+      if (s.integrator == rtg::Integrator::Normals) {
+        ex = 1.0;
+      } else {
+        op = s.tone_map;
+        ex = s.exposure;
+      }
+    } else {
+      if (tone_map > 2) throw std::invalid_argument("tone_map must be 0, 1 or 2");
+      op = static_cast<rtg::ToneMap>(tone_map);
+    }
+    ctx->engine->read_image_frame(f, op, ex, rgb);
+    return RTG_OK;
+  });
+}
+
+int rtg_serve_footprint(rtg_context* ctx, uint64_t* bytes, int32_t* open_requests, int32_t* rendering) {
+  return guarded(ctx, [&]() {
+    if (bytes) *bytes = ctx->serve_used;
+    if (open_requests) *open_requests = static_cast<int32_t>(ctx->engine->open_requests());
+    if (rendering) *rendering = static_cast<int32_t>(ctx->engine->requests_rendering());
     return RTG_OK;
   });
 }

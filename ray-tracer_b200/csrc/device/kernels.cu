@@ -1,6 +1,9 @@
 // Wavefront path tracer for sm_100a.
 //
 // One iteration of the wavefront over a pool of path slots:
+//   k_plan    — one block: decides which open segments (passes of renders) the
+//               free slots go to, in the host's priority order, and copies the
+//               counters and segment progress to the pinned snapshot ring;
 //   k_extend  — fills free slots with new camera paths (thin-lens generation,
 //               src/rendering/renderer.cpp:33-37 + include/raytracer/core/camera.hpp:54-62)
 //               and finds every live path's closest hit (Scene::intersect).
@@ -10,11 +13,13 @@
 //               rays into the shadow queue with one atomic per warp (ballot + popc).
 //   k_shadow  — any-hit test of each shadow ray (Scene::occluded); unoccluded ones
 //               add their contribution to the sample's radiance slot.
-// Every path owns one radiance slot addressed by (pixel, sample-in-pass); all
-// adds to it happen in path order from kernels that are stream-ordered, so the
-// result does not depend on queue order, batch composition or timing. After the
-// pass, k_accumulate folds each pixel's samples into the double framebuffer in
-// sample order (Framebuffer::add, include/raytracer/rendering/framebuffer.hpp:31).
+// Every path owns one radiance slot addressed by (segment, pixel, sample-in-pass);
+// all adds to it happen in path order from kernels that are stream-ordered, so
+// the result does not depend on queue order, batch composition or timing. Paths
+// that end count themselves done in their segment's progress record; once a
+// segment is done, k_accumulate folds each pixel's samples into the double
+// framebuffer in sample order (Framebuffer::add,
+// include/raytracer/rendering/framebuffer.hpp:31), passes of one render in order.
 //
 // Work distribution: persistent warps fetch 32 items at a time from a cursor in
 // WaveCounters (Aila & Laine, "Understanding the Efficiency of Ray Traversal on
@@ -62,34 +67,19 @@ __device__ __forceinline__ std::uint32_t warp_fetch(std::uint32_t* cursor) {
   return __shfl_sync(kFull, base, 0);
 }
 
-// Job owning global work index w (binary search over the pass table).
-__device__ __forceinline__ int find_job(const PassTable& pt, std::uint64_t w) {
-  int lo = 0, hi = pt.n - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (pt.job_begin[mid] <= w) lo = mid;
-    else hi = mid - 1;
-  }
-  return lo;
-}
-
 struct CameraSample {
   float3 o, d;
   Pcg rng;
   std::uint32_t sample;  // radiance slot
-  std::uint32_t job;
 };
 
-// Camera ray for work index w: jitter (2 draws), then the lens (2 draws).
-__device__ __forceinline__ CameraSample camera_sample(const PassTable& pt, std::uint64_t w) {
-  const int k = find_job(pt, w);
+// Camera ray for local sample `local` of a segment (pixel-major, then sample):
+// jitter (2 draws), then the lens (2 draws).
+__device__ __forceinline__ CameraSample camera_sample(const RtgSceneDev& J, const DevSegment& S, std::uint64_t local) {
   CameraSample cs;
-  cs.job = pt.job_ids[k];
-  const RtgSceneDev& J = pt.jobs[cs.job];
-  const std::uint64_t local = w - pt.job_begin[k];
-  const std::uint32_t spp = J.pass_spp;
+  const std::uint32_t spp = S.pass_spp;
   const std::uint64_t pixel = local / spp;
-  const std::uint32_t s = J.pass_s0 + static_cast<std::uint32_t>(local - pixel * spp);
+  const std::uint32_t s = S.pass_s0 + static_cast<std::uint32_t>(local - pixel * spp);
   const std::uint32_t px = static_cast<std::uint32_t>(pixel % static_cast<std::uint32_t>(J.width));
   const std::uint32_t py = static_cast<std::uint32_t>(pixel / static_cast<std::uint32_t>(J.width));
   cs.rng = Pcg::for_sample(J.seed, pixel, s);
@@ -102,27 +92,92 @@ __device__ __forceinline__ CameraSample camera_sample(const PassTable& pt, std::
     cs.o = cs.o + J.lens_radius * (dk.x * J.cam_u + dk.y * J.cam_v);
   }
   cs.d = unit_or(target - cs.o, f3(0.f, 0.f, 0.f));
-  cs.sample = static_cast<std::uint32_t>(J.sample_base + local);
+  cs.sample = static_cast<std::uint32_t>(S.sample_base + local);
   return cs;
 }
 
 // ---------------------------------------------------------------------------
+// Generation plan: free slots go to the open segments greedily in the host's
+// order. One block of kMaxGen threads, one table entry each.
+__global__ void __launch_bounds__(kMaxGen) k_plan(WaveBuffers wb, int par) {
+  __shared__ std::uint32_t scan[kMaxGen];
+  __shared__ std::uint32_t fscan[kMaxGen];
+  WaveCounters* C = wb.cnt;
+  const int t = threadIdx.x;
+  const std::uint32_t live = C->live[par];
+  const std::uint32_t room = wb.capacity - live;
+  const std::uint32_t ng = min(wb.gen->n, static_cast<std::uint32_t>(kMaxGen));
+  // Snapshot of the state the previous iteration left, before this plan changes it.
+  const std::uint64_t iter = C->iteration;
+  WaveSnapshot* snap = wb.ring + (iter % wb.ring_size);
+  const std::uint32_t ns = min(wb.gen->snapshot_slots, static_cast<std::uint32_t>(kMaxSegments));
+  for (std::uint32_t k = t; k < ns; k += kMaxGen) snap->seg[k] = wb.seg_prog[k];
+  if (t == 0) snap->c = *C;
+  std::uint32_t slot = 0, rem = 0;
+  std::uint64_t gen0 = 0;
+  if (t < static_cast<int>(ng)) {
+    slot = wb.gen->slot[t];
+    if (slot < static_cast<std::uint32_t>(kMaxSegments)) {
+      gen0 = wb.seg_prog[slot].generated;
+      const std::uint64_t count = wb.segs[slot].count;
+      const std::uint64_t r = count > gen0 ? count - gen0 : 0;
+      rem = r < room ? static_cast<std::uint32_t>(r) : room;
+    } else {
+      atomicExch(&C->error, 3u);
+      C->error_info = slot;
+    }
+  }
+  // Inclusive scan of rem (each <= room <= 2^23, so the sum fits 32 bits).
+  scan[t] = rem;
+  __syncthreads();
+  for (int off = 1; off < kMaxGen; off <<= 1) {
+    const std::uint32_t v = t >= off ? scan[t - off] : 0u;
+    __syncthreads();
+    scan[t] += v;
+    __syncthreads();
+  }
+  const std::uint32_t excl = scan[t] - rem;
+  const std::uint32_t total = scan[kMaxGen - 1];
+  const std::uint32_t take = excl >= room ? 0u : min(rem, room - excl);
+  const std::uint32_t flag = take > 0 ? 1u : 0u;
+  fscan[t] = flag;
+  __syncthreads();
+  for (int off = 1; off < kMaxGen; off <<= 1) {
+    const std::uint32_t v = t >= off ? fscan[t - off] : 0u;
+    __syncthreads();
+    fscan[t] += v;
+    __syncthreads();
+  }
+  if (flag) {
+    const std::uint32_t k = fscan[t] - 1;
+    wb.plan->end[k] = excl + take;
+    wb.plan->seg[k] = slot;
+    wb.plan->start[k] = gen0;
+    wb.seg_prog[slot].generated = gen0 + take;
+  }
+  if (t == 0) {
+    const std::uint32_t n_new = total < room ? total : room;
+    wb.plan->n = fscan[kMaxGen - 1];
+    wb.plan->n_new = n_new;
+    C->n_extend = live + n_new;
+    C->live[par ^ 1] = 0;
+    C->n_shadow = 0;
+    C->fetch[0] = 0;
+    C->fetch[1] = 0;
+    C->fetch[2] = 0;
+    C->generated += n_new;
+    C->iteration = iter + 1;
+  }
+}
+
+// ---------------------------------------------------------------------------
 template <int kBlock, bool kCount>
-__global__ void __launch_bounds__(kBlock) k_extend(WaveBuffers wb, PassTable pt, int par) {
+__global__ void __launch_bounds__(kBlock) k_extend(WaveBuffers wb, int par) {
   __shared__ int stack[kStackSmem * kBlock];
   WaveCounters* C = wb.cnt;
   const std::uint32_t live = C->live[par];
-  const std::uint64_t next = C->next_work;
-  const std::uint64_t avail = C->total_work - next;
-  const std::uint32_t room = wb.capacity - live;
-  const std::uint32_t n_new = avail < room ? static_cast<std::uint32_t>(avail) : room;
-  const std::uint32_t n = live + n_new;
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    C->n_extend = n;
-    C->live[par ^ 1] = 0;
-    C->n_shadow = 0;
-    C->fetch[2] = 0;
-  }
+  const std::uint32_t n = C->n_extend;
+  const GenPlan& P = *wb.plan;
   float4* const A = wb.st_a[par];
   float4* const B = wb.st_b[par];
   TraceCount tc;
@@ -135,14 +190,25 @@ __global__ void __launch_bounds__(kBlock) k_extend(WaveBuffers wb, PassTable pt,
     float3 o, d;
     std::uint32_t job;
     if (i >= live) {
-      const CameraSample cs = camera_sample(pt, next + (i - live));
+      // New path j: plan entry k is the first with end[k] > j.
+      const std::uint32_t j = i - live;
+      int lo = 0, hi = static_cast<int>(P.n) - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (P.end[mid] > j) hi = mid;
+        else lo = mid + 1;
+      }
+      const std::uint32_t seg = P.seg[lo];
+      const std::uint64_t local = P.start[lo] + (j - (lo > 0 ? P.end[lo - 1] : 0u));
+      const DevSegment S = wb.segs[seg];
+      job = S.job;
+      const CameraSample cs = camera_sample(wb.jobs[job], S, local);
       o = cs.o;
       d = cs.d;
-      job = cs.job;
       A[i] = make_float4(o.x, o.y, o.z, __uint_as_float(cs.sample));
       // Camera rays count as a specular bounce (no NEE double-count guard).
       B[i] = make_float4(d.x, d.y, d.z, __uint_as_float(kFlagSpecular | (job << kMetaSceneShift)));
-      wb.st_c[par][i] = make_float4(1.f, 1.f, 1.f, 0.f);
+      wb.st_c[par][i] = make_float4(1.f, 1.f, 1.f, __uint_as_float(seg));
       wb.st_d[par][i] = make_uint4(static_cast<std::uint32_t>(cs.rng.state), static_cast<std::uint32_t>(cs.rng.state >> 32),
                                    static_cast<std::uint32_t>(cs.rng.inc), static_cast<std::uint32_t>(cs.rng.inc >> 32));
       wb.radiance[cs.sample] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -153,7 +219,7 @@ __global__ void __launch_bounds__(kBlock) k_extend(WaveBuffers wb, PassTable pt,
       d = f3(b);
       job = __float_as_uint(b.w) >> kMetaSceneShift;
     }
-    const RtgSceneDev& J = pt.jobs[job];
+    const RtgSceneDev& J = wb.jobs[job];
     const RayHit h = J.use_bvh ? closest_hit<kStackSmem, kBlock, kCount>(J, o, d, kRayTMin, FLT_MAX, stack, tc)
                                : closest_brute<kCount>(J, o, d, kRayTMin, FLT_MAX, tc);
     wb.hits[i] = make_float4(h.t, __uint_as_float(h.word), h.b1, h.b2);
@@ -169,13 +235,9 @@ __global__ void __launch_bounds__(kBlock) k_extend(WaveBuffers wb, PassTable pt,
 
 // ---------------------------------------------------------------------------
 template <int kBlock>
-__global__ void __launch_bounds__(kBlock) k_shade(WaveBuffers wb, PassTable pt, int par) {
+__global__ void __launch_bounds__(kBlock) k_shade(WaveBuffers wb, int par) {
   WaveCounters* C = wb.cnt;
   const std::uint32_t n = C->n_extend;
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    C->next_work += n - C->live[par];
-    C->fetch[0] = 0;
-  }
   const float4* const A = wb.st_a[par];
   const float4* const B = wb.st_b[par];
   const float4* const Cc = wb.st_c[par];
@@ -188,7 +250,7 @@ __global__ void __launch_bounds__(kBlock) k_shade(WaveBuffers wb, PassTable pt, 
     bool cont = false, shadow = false;
     float3 o_next = f3(0.f, 0.f, 0.f), d_next = o_next, beta = o_next, sh_o = o_next, sh_d = o_next, sh_c = o_next;
     float sh_tmax = 0.f;
-    std::uint32_t sample = 0, meta_next = 0, job = 0;
+    std::uint32_t sample = 0, meta_next = 0, job = 0, seg = 0;
     Pcg rng{0, 0};
     if (i < n) {
       const float4 a = A[i], b = B[i], c = Cc[i], hv = wb.hits[i];
@@ -199,10 +261,11 @@ __global__ void __launch_bounds__(kBlock) k_shade(WaveBuffers wb, PassTable pt, 
       const std::uint32_t depth = meta & kMetaDepthMask;
       const bool specular_bounce = (meta & kFlagSpecular) != 0;
       job = meta >> kMetaSceneShift;
+      seg = __float_as_uint(c.w);
       beta = f3(c);
       rng.state = ld_u64(r.x, r.y);
       rng.inc = ld_u64(r.z, r.w);
-      const RtgSceneDev& J = pt.jobs[job];
+      const RtgSceneDev& J = wb.jobs[job];
       const RayHit h{hv.x, __float_as_uint(hv.y), hv.z, hv.w};
       float4* const slot = &wb.radiance[sample];
       if (J.integrator == 2) {
@@ -266,10 +329,16 @@ __global__ void __launch_bounds__(kBlock) k_shade(WaveBuffers wb, PassTable pt, 
     }
     const std::uint32_t cpos = warp_append(cont, &C->live[par ^ 1]);
     const std::uint32_t spos = warp_append(shadow, &C->n_shadow);
+    // A path that ends here is done once this iteration's shadow stage has run:
+    // count it in its segment (one atomic per segment present in the warp).
+    const bool fin = i < n && !cont;
+    const unsigned same = __match_any_sync(kFull, fin ? seg : 0xFFFFFFFFu);
+    if (fin && (threadIdx.x & 31) == static_cast<unsigned>(__ffs(same) - 1))
+      atomicAdd(&wb.seg_prog[seg].done, static_cast<std::uint32_t>(__popc(same)));
     if (cont) {
       wb.st_a[par ^ 1][cpos] = make_float4(o_next.x, o_next.y, o_next.z, __uint_as_float(sample));
       wb.st_b[par ^ 1][cpos] = make_float4(d_next.x, d_next.y, d_next.z, __uint_as_float(meta_next));
-      wb.st_c[par ^ 1][cpos] = make_float4(beta.x, beta.y, beta.z, 0.f);
+      wb.st_c[par ^ 1][cpos] = make_float4(beta.x, beta.y, beta.z, __uint_as_float(seg));
       wb.st_d[par ^ 1][cpos] = make_uint4(static_cast<std::uint32_t>(rng.state), static_cast<std::uint32_t>(rng.state >> 32),
                                           static_cast<std::uint32_t>(rng.inc), static_cast<std::uint32_t>(rng.inc >> 32));
     }
@@ -284,11 +353,10 @@ __global__ void __launch_bounds__(kBlock) k_shade(WaveBuffers wb, PassTable pt, 
 
 // ---------------------------------------------------------------------------
 template <int kBlock, bool kCount>
-__global__ void __launch_bounds__(kBlock) k_shadow(WaveBuffers wb, PassTable pt) {
+__global__ void __launch_bounds__(kBlock) k_shadow(WaveBuffers wb) {
   __shared__ int stack[kStackSmem * kBlock];
   WaveCounters* C = wb.cnt;
   const std::uint32_t n = C->n_shadow;
-  if (blockIdx.x == 0 && threadIdx.x == 0) C->fetch[1] = 0;
   TraceCount tc;
   std::uint64_t rays = 0;
   while (true) {
@@ -297,7 +365,7 @@ __global__ void __launch_bounds__(kBlock) k_shadow(WaveBuffers wb, PassTable pt)
     const std::uint32_t i = base + (threadIdx.x & 31);
     if (i >= n) continue;
     const float4 a = wb.sh_a[i], b = wb.sh_b[i], c = wb.sh_c[i];
-    const RtgSceneDev& J = pt.jobs[__float_as_uint(c.w)];
+    const RtgSceneDev& J = wb.jobs[__float_as_uint(c.w)];
     const float3 o = f3(a), d = f3(b);
     const bool blocked = J.use_bvh ? any_hit<kStackSmem, kBlock, kCount>(J, o, d, kRayTMin, b.w, stack, tc)
                                    : any_brute(J, o, d, kRayTMin, b.w);
@@ -347,14 +415,15 @@ __device__ __forceinline__ float3 direct_light_all(const RtgSceneDev& J, const D
 }
 
 template <int kBlock>
-__global__ void __launch_bounds__(kBlock) k_direct(PassTable pt, std::uint64_t total, float4* radiance, WaveCounters* C) {
+__global__ void __launch_bounds__(kBlock) k_direct(const RtgSceneDev* __restrict__ job, DevSegment seg, float4* radiance,
+                                                   WaveCounters* C) {
   __shared__ int stack[kStackSmem * kBlock];
   TraceCount tc;
   std::uint64_t rays = 0, shadow_rays = 0;
+  const RtgSceneDev& J = *job;
   const std::uint64_t stride = static_cast<std::uint64_t>(gridDim.x) * kBlock;
-  for (std::uint64_t w = static_cast<std::uint64_t>(blockIdx.x) * kBlock + threadIdx.x; w < total; w += stride) {
-    CameraSample cs = camera_sample(pt, w);
-    const RtgSceneDev& J = pt.jobs[cs.job];
+  for (std::uint64_t w = static_cast<std::uint64_t>(blockIdx.x) * kBlock + threadIdx.x; w < seg.count; w += stride) {
+    CameraSample cs = camera_sample(J, seg, w);
     Pending todo[kDirectStack];
     int sp = 0;
     Pending cur{cs.o, cs.d, f3(1.f, 1.f, 1.f), 0};
@@ -416,14 +485,14 @@ __global__ void __launch_bounds__(kBlock) k_direct(PassTable pt, std::uint64_t t
 }
 
 // ---------------------------------------------------------------------------
-__global__ void k_accumulate(const RtgSceneDev* __restrict__ job, const float4* __restrict__ radiance) {
+__global__ void k_accumulate(const RtgSceneDev* __restrict__ job, DevSegment seg, const float4* __restrict__ radiance) {
   const RtgSceneDev& J = *job;
   const std::uint64_t pixels = static_cast<std::uint64_t>(J.width) * static_cast<std::uint64_t>(J.height);
   const std::uint64_t p = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   std::uint64_t bad = 0;
   if (p < pixels) {
-    const std::uint32_t k = J.pass_spp;
-    const float4* src = radiance + J.sample_base + p * k;
+    const std::uint32_t k = seg.pass_spp;
+    const float4* src = radiance + seg.sample_base + p * k;
     double s0 = J.fb_sum[4 * p], s1 = J.fb_sum[4 * p + 1], s2 = J.fb_sum[4 * p + 2];
     double q0 = J.fb_sumsq[4 * p], q1 = J.fb_sumsq[4 * p + 1], q2 = J.fb_sumsq[4 * p + 2];
     for (std::uint32_t j = 0; j < k; ++j) {
@@ -458,16 +527,15 @@ __device__ __forceinline__ std::uint8_t srgb8(double v) {
   return static_cast<std::uint8_t>(llround(s * 255.0));
 }
 
-__global__ void k_resolve(const RtgSceneDev* __restrict__ job, int op, double exposure, std::uint8_t* rgb8, double* mean_out) {
-  const RtgSceneDev& J = *job;
-  const std::uint64_t pixels = static_cast<std::uint64_t>(J.width) * static_cast<std::uint64_t>(J.height);
+__global__ void k_resolve(const double* __restrict__ fb_sum, const std::uint32_t* __restrict__ fb_count,
+                          std::uint64_t pixels, int op, double exposure, std::uint8_t* rgb8, double* mean_out) {
   const std::uint64_t p = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (p >= pixels) return;
-  const std::uint32_t n = J.fb_count[p];
+  const std::uint32_t n = fb_count[p];
   double c[3] = {0, 0, 0};
   if (n) {
     const double inv = 1.0 / static_cast<double>(n);
-    for (int k = 0; k < 3; ++k) c[k] = J.fb_sum[4 * p + k] * inv;
+    for (int k = 0; k < 3; ++k) c[k] = fb_sum[4 * p + k] * inv;
   }
   if (mean_out)
     for (int k = 0; k < 3; ++k) mean_out[3 * p + k] = c[k];
@@ -545,25 +613,28 @@ const BlockCounts& block_counts() {
 }
 
 template <int kBlock>
-cudaError_t stage_impl(Stage stage, const WaveBuffers& wb, const PassTable& pt, int par, const LaunchShape& shape,
-                       bool count, cudaStream_t stream) {
+cudaError_t stage_impl(Stage stage, const WaveBuffers& wb, int par, const LaunchShape& shape, bool count,
+                       cudaStream_t stream) {
   const BlockCounts& bc = block_counts<kBlock>();
   switch (stage) {
+    case Stage::Plan:
+      k_plan<<<1, kMaxGen, 0, stream>>>(wb, par);
+      break;
     case Stage::Extend: {
       const int blocks = shape.extend_blocks ? shape.extend_blocks : (count ? bc.extend_counting : bc.extend);
-      if (count) k_extend<kBlock, true><<<blocks, kBlock, 0, stream>>>(wb, pt, par);
-      else k_extend<kBlock, false><<<blocks, kBlock, 0, stream>>>(wb, pt, par);
+      if (count) k_extend<kBlock, true><<<blocks, kBlock, 0, stream>>>(wb, par);
+      else k_extend<kBlock, false><<<blocks, kBlock, 0, stream>>>(wb, par);
       break;
     }
     case Stage::Shade: {
       const int blocks = shape.shade_blocks ? shape.shade_blocks : bc.shade;
-      k_shade<kBlock><<<blocks, kBlock, 0, stream>>>(wb, pt, par);
+      k_shade<kBlock><<<blocks, kBlock, 0, stream>>>(wb, par);
       break;
     }
     case Stage::Shadow: {
       const int blocks = shape.shadow_blocks ? shape.shadow_blocks : (count ? bc.shadow_counting : bc.shadow);
-      if (count) k_shadow<kBlock, true><<<blocks, kBlock, 0, stream>>>(wb, pt);
-      else k_shadow<kBlock, false><<<blocks, kBlock, 0, stream>>>(wb, pt);
+      if (count) k_shadow<kBlock, true><<<blocks, kBlock, 0, stream>>>(wb);
+      else k_shadow<kBlock, false><<<blocks, kBlock, 0, stream>>>(wb);
       break;
     }
   }
@@ -572,44 +643,44 @@ cudaError_t stage_impl(Stage stage, const WaveBuffers& wb, const PassTable& pt, 
 
 }  // namespace
 
-cudaError_t launch_stage(Stage stage, const WaveBuffers& wb, const PassTable& pt, int parity, const LaunchShape& shape,
-                         bool count_traversal, cudaStream_t stream) {
+cudaError_t launch_stage(Stage stage, const WaveBuffers& wb, int parity, const LaunchShape& shape, bool count_traversal,
+                         cudaStream_t stream) {
   switch (shape.extend_block) {
-    case 64: return stage_impl<64>(stage, wb, pt, parity, shape, count_traversal, stream);
-    case 256: return stage_impl<256>(stage, wb, pt, parity, shape, count_traversal, stream);
-    default: return stage_impl<128>(stage, wb, pt, parity, shape, count_traversal, stream);
+    case 64: return stage_impl<64>(stage, wb, parity, shape, count_traversal, stream);
+    case 256: return stage_impl<256>(stage, wb, parity, shape, count_traversal, stream);
+    default: return stage_impl<128>(stage, wb, parity, shape, count_traversal, stream);
   }
 }
 
-cudaError_t launch_iteration(const WaveBuffers& wb, const PassTable& pt, int parity, const LaunchShape& shape,
-                             bool count_traversal, cudaStream_t stream) {
-  for (Stage st : {Stage::Extend, Stage::Shade, Stage::Shadow}) {
-    const cudaError_t e = launch_stage(st, wb, pt, parity, shape, count_traversal, stream);
+cudaError_t launch_iteration(const WaveBuffers& wb, int parity, const LaunchShape& shape, bool count_traversal,
+                             cudaStream_t stream) {
+  for (Stage st : {Stage::Plan, Stage::Extend, Stage::Shade, Stage::Shadow}) {
+    const cudaError_t e = launch_stage(st, wb, parity, shape, count_traversal, stream);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
 }
 
-cudaError_t launch_accumulate(const RtgSceneDev* job_dev, const RtgSceneDev& job_host, const float4* radiance,
-                              cudaStream_t stream) {
-  const std::uint64_t pixels = static_cast<std::uint64_t>(job_host.width) * job_host.height;
+cudaError_t launch_accumulate(const RtgSceneDev* job_dev, std::uint64_t pixels, const DevSegment& seg,
+                              const float4* radiance, cudaStream_t stream) {
   const unsigned blocks = static_cast<unsigned>((pixels + 255) / 256);
-  k_accumulate<<<blocks, 256, 0, stream>>>(job_dev, radiance);
+  k_accumulate<<<blocks, 256, 0, stream>>>(job_dev, seg, radiance);
   return cudaGetLastError();
 }
 
-cudaError_t launch_direct(const PassTable& pt, std::uint64_t total_work, float4* radiance, WaveCounters* cnt,
+cudaError_t launch_direct(const RtgSceneDev* job_dev, const DevSegment& seg, float4* radiance, WaveCounters* cnt,
                           cudaStream_t stream) {
   static int blocks = 0;
   if (!blocks) blocks = persistent_blocks(k_direct<128>, 128);
-  k_direct<128><<<blocks, 128, 0, stream>>>(pt, total_work, radiance, cnt);
+  k_direct<128><<<blocks, 128, 0, stream>>>(job_dev, seg, radiance, cnt);
   return cudaGetLastError();
 }
 
-cudaError_t launch_resolve(const RtgSceneDev* job_dev, std::uint64_t pixels, int tone_map, double exposure,
-                               std::uint8_t* rgb8, double* mean_out, cudaStream_t stream) {
+cudaError_t launch_resolve(const double* fb_sum, const std::uint32_t* fb_count, std::uint64_t pixels, int tone_map,
+                           double exposure, std::uint8_t* rgb8, double* mean_out, cudaStream_t stream) {
+  if (pixels == 0) return cudaSuccess;
   const unsigned blocks = static_cast<unsigned>((pixels + 255) / 256);
-  k_resolve<<<blocks, 256, 0, stream>>>(job_dev, tone_map, exposure, rgb8, mean_out);
+  k_resolve<<<blocks, 256, 0, stream>>>(fb_sum, fb_count, pixels, tone_map, exposure, rgb8, mean_out);
   return cudaGetLastError();
 }
 

@@ -94,12 +94,6 @@ struct alignas(16) RtgSceneDev {
   float3 bg_top, bg_bottom;
   float bg_intensity;
   std::int32_t bg_solid;
-  // pass bookkeeping for this scene inside a (possibly batched) pass
-  std::uint64_t work_begin;   // first global work index of this scene in the pass
-  std::uint64_t work_count;   // pixels * pass_spp
-  std::uint32_t pass_s0;      // first sample index of the pass
-  std::uint32_t pass_spp;     // samples per pixel in this pass
-  std::uint64_t sample_base;  // offset of this scene's radiance slots in the sample buffer
   // framebuffer of the render this descriptor belongs to (per pixel)
   double* fb_sum;             // 4 doubles per pixel: running sum r, g, b, (unused)
   double* fb_sumsq;           // 4 doubles per pixel: running sum of squares
@@ -112,13 +106,57 @@ struct alignas(16) RtgSceneDev {
   const double* planes64;
 };
 
+// A segment is one pass of one render: samples [pass_s0, pass_s0 + pass_spp) of every
+// pixel of a job. The continuous wavefront schedules segments; the host appends
+// them (and new jobs) between iterations, so passes and requests overlap.
+struct alignas(16) DevSegment {
+  std::uint32_t job;          // descriptor index
+  std::uint32_t pass_s0;      // first sample index of the pass
+  std::uint32_t pass_spp;     // samples per pixel in this pass
+  std::uint32_t pad;
+  std::uint64_t count;        // pixels * pass_spp camera samples
+  std::uint64_t sample_base;  // radiance slot of (pixel 0, sample pass_s0)
+};
+
+// Device-side progress of one segment slot (zeroed when the slot is assigned).
+struct alignas(16) SegmentProgress {
+  std::uint64_t generated;    // camera samples handed to the wavefront
+  std::uint32_t done;         // samples whose path (and last shadow ray) finished
+  std::uint32_t pad;
+};
+
+constexpr int kMaxSegments = 4096;  // segment slots (the path record carries the slot)
+constexpr int kMaxGen = 256;        // segments open for generation at once
+
+// Generation order written by the host between iterations: segment slots in
+// priority order. The plan kernel hands free pool slots to them greedily.
+struct alignas(16) GenTable {
+  std::uint32_t n;
+  std::uint32_t snapshot_slots;  // segment slots [0, this) copied into each snapshot
+  std::uint32_t pad[2];
+  std::uint32_t slot[kMaxGen];
+};
+
+// Where this iteration's new paths come from (written by the plan kernel):
+// new path j belongs to the first entry k with end[k] > j, and is local sample
+// start[k] + j - end[k - 1] of segment seg[k].
+struct alignas(16) GenPlan {
+  std::uint32_t n;
+  std::uint32_t n_new;
+  std::uint32_t pad[2];
+  std::uint32_t end[kMaxGen];
+  std::uint32_t seg[kMaxGen];
+  std::uint64_t start[kMaxGen];
+};
+
 // Path-state stream record, four float4 (SoA): one element per live path.
 //  a = (origin, sample id bits)         b = (direction, meta bits)
-//  c = (throughput, unused)             d = PCG32 state (lo, hi) and increment (lo, hi)
-// meta: depth (bits 0-11) | flags (bits 12-15) | scene (bits 16-31)
+//  c = (throughput, segment slot bits)  d = PCG32 state (lo, hi) and increment (lo, hi)
+// meta: depth (bits 0-11) | flags (bits 12-15) | job (bits 16-31)
 constexpr std::uint32_t kFlagSpecular = 1u << 12;
 constexpr std::uint32_t kMetaDepthMask = 0xFFFu;
 constexpr int kMetaSceneShift = 16;
+constexpr int kMaxJobs = 65536;  // job descriptors addressable from the path record
 
 // Wavefront counters in device memory.
 struct alignas(16) WaveCounters {
@@ -126,8 +164,8 @@ struct alignas(16) WaveCounters {
   std::uint32_t n_extend;     // paths traced this iteration (live + new)
   std::uint32_t n_shadow;     // shadow rays queued this iteration
   std::uint32_t fetch[4];     // persistent-kernel work-fetch cursors
-  std::uint64_t next_work;    // next unclaimed work index in the pass
-  std::uint64_t total_work;   // work items in the pass
+  std::uint64_t iteration;    // plan launches so far (selects the snapshot ring slot)
+  std::uint64_t generated;    // camera samples generated so far
   std::uint64_t rays;         // closest-hit rays traced
   std::uint64_t shadow_rays;
   std::uint64_t rr_terminated;
@@ -140,6 +178,13 @@ struct alignas(16) WaveCounters {
   std::uint64_t shadow_sphere_tests;
   std::uint32_t error;        // non-zero: a bounds check failed (index recorded in error_info)
   std::uint32_t error_info;
+};
+
+// What the plan kernel copies to pinned host memory at the start of each
+// iteration: the counters and segment progress as the previous iteration left them.
+struct alignas(16) WaveSnapshot {
+  WaveCounters c;
+  SegmentProgress seg[kMaxSegments];
 };
 
 }  // namespace rtg

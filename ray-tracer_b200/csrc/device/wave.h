@@ -9,7 +9,8 @@
 
 namespace rtg {
 
-// Device buffers of one wavefront (a pool of `capacity` path slots).
+// Device buffers of one continuous wavefront (a pool of `capacity` path slots)
+// and the segment tables it draws new paths from.
 struct WaveBuffers {
   float4* st_a[2];
   float4* st_b[2];
@@ -19,17 +20,16 @@ struct WaveBuffers {
   float4* sh_a;
   float4* sh_b;
   float4* sh_c;
-  float4* radiance;   // one float4 per sample of the current pass
+  float4* radiance;            // one float4 per sample of every open segment
   WaveCounters* cnt;
-  std::uint32_t capacity;
-};
-
-// One pass: which descriptors (jobs) have work, and where their work begins.
-struct PassTable {
-  const RtgSceneDev* jobs;         // device array of job descriptors
-  const std::uint32_t* job_ids;    // device: jobs with work in this pass
-  const std::uint64_t* job_begin;  // device: first work index of each (strictly increasing)
-  std::int32_t n;
+  const RtgSceneDev* jobs;     // job descriptors, indexed by job slot
+  const DevSegment* segs;      // indexed by segment slot
+  SegmentProgress* seg_prog;   // indexed by segment slot
+  const GenTable* gen;         // host-written generation order
+  GenPlan* plan;               // this iteration's generation plan
+  WaveSnapshot* ring;          // pinned, host-mapped snapshot ring
+  std::uint32_t ring_size;
+  std::uint32_t capacity;      // at most 2^23 path slots
 };
 
 struct LaunchShape {
@@ -37,29 +37,30 @@ struct LaunchShape {
   int extend_block = 128;  // 64, 128 or 256
 };
 
-enum class Stage { Extend, Shade, Shadow };
+enum class Stage { Plan, Extend, Shade, Shadow };
 
 // One stage of a wavefront iteration on `stream`; `parity` alternates 0/1
-// between iterations. The stages must run in the order extend, shade, shadow.
-cudaError_t launch_stage(Stage stage, const WaveBuffers& wb, const PassTable& pt, int parity, const LaunchShape& shape,
-                         bool count_traversal, cudaStream_t stream);
+// between iterations. The stages must run in the order plan, extend, shade, shadow.
+cudaError_t launch_stage(Stage stage, const WaveBuffers& wb, int parity, const LaunchShape& shape, bool count_traversal,
+                         cudaStream_t stream);
 
-// One wavefront iteration (generate+extend, shade, shadow) on `stream`.
-cudaError_t launch_iteration(const WaveBuffers& wb, const PassTable& pt, int parity, const LaunchShape& shape,
-                             bool count_traversal, cudaStream_t stream);
+// One wavefront iteration (plan, generate+extend, shade, shadow) on `stream`.
+cudaError_t launch_iteration(const WaveBuffers& wb, int parity, const LaunchShape& shape, bool count_traversal,
+                             cudaStream_t stream);
 
-// Per-pixel reduction of a finished pass into the job's framebuffer.
-cudaError_t launch_accumulate(const RtgSceneDev* job_dev, const RtgSceneDev& job_host, const float4* radiance,
-                              cudaStream_t stream);
+// Per-pixel reduction of a finished segment into its job's framebuffer.
+cudaError_t launch_accumulate(const RtgSceneDev* job_dev, std::uint64_t pixels, const DevSegment& seg,
+                              const float4* radiance, cudaStream_t stream);
 
-// Direct (Whitted) integrator: whole samples per thread (depth-first with an
-// explicit stack). Writes each sample's radiance into `radiance`.
-cudaError_t launch_direct(const PassTable& pt, std::uint64_t total_work, float4* radiance, WaveCounters* cnt,
+// Direct (Whitted) integrator over one whole segment: whole samples per thread
+// (depth-first with an explicit stack). Writes each sample's radiance slot.
+cudaError_t launch_direct(const RtgSceneDev* job_dev, const DevSegment& seg, float4* radiance, WaveCounters* cnt,
                           cudaStream_t stream);
 
-// Tone map + sRGB encode of a job's framebuffer means into rgb8 (w * h * 3).
-cudaError_t launch_resolve(const RtgSceneDev* job_dev, std::uint64_t pixels, int tone_map, double exposure,
-                           std::uint8_t* rgb8, double* mean_out, cudaStream_t stream);
+// Framebuffer means (mean_out, 3 doubles per pixel) and/or their tone-mapped
+// sRGB encoding (rgb8, 3 bytes per pixel); either output may be null.
+cudaError_t launch_resolve(const double* fb_sum, const std::uint32_t* fb_count, std::uint64_t pixels, int tone_map,
+                           double exposure, std::uint8_t* rgb8, double* mean_out, cudaStream_t stream);
 
 // Ray queries for parity tests and the ray API. rays: 2 float4 per ray
 // (origin, tmin), (direction, tmax). closest -> float4 (t, word, b1, b2) per ray.

@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <limits>
 #include <stdexcept>
 #include <string>
 
@@ -23,6 +24,14 @@ T* dev_alloc(std::size_t n) {
   return static_cast<T*>(p);
 }
 
+// Stream-ordered allocation: never synchronises with kernels in flight.
+template <class T>
+T* dev_alloc_async(std::size_t n, cudaStream_t s) {
+  void* p = nullptr;
+  CK(cudaMallocAsync(&p, std::max<std::size_t>(n, 1) * sizeof(T), s));
+  return static_cast<T*>(p);
+}
+
 template <class T>
 T* dev_upload(const std::vector<T>& v, cudaStream_t s, std::size_t& bytes) {
   T* p = dev_alloc<T>(v.size());
@@ -35,32 +44,70 @@ void dev_free(void* p) {
   if (p) cudaFree(p);
 }
 
-std::uint32_t pass_size(std::uint32_t done, std::uint32_t target, const RenderOptions& o) {
-  std::uint32_t k = target - done;
-  if (o.progressive) {
-    const std::uint32_t grow = std::max<std::uint32_t>(1u, done);
-    const std::uint32_t cap = static_cast<std::uint32_t>(std::max(1, o.max_pass_spp));
-    k = std::min({k, grow, cap});
-  }
-  return k;
+void free_scene_arrays(GpuScene& s) {
+  dev_free(s.nodes); dev_free(s.prims); dev_free(s.slot_material); dev_free(s.slot_normals);
+  dev_free(s.planes); dev_free(s.materials); dev_free(s.lights);
+  dev_free(s.prims64); dev_free(s.planes64);
 }
 
-constexpr int kRing = 8;  // pinned counter snapshots in flight
-constexpr int kLag = 2;   // iterations queued ahead of the termination check
+constexpr int kRing = 8;   // snapshot / staging slots (iterations in flight at most)
+constexpr int kLag = 2;    // iterations queued ahead of the snapshot being read
+constexpr std::size_t kStageBytes = std::size_t(1) << 20;  // host->device staging per iteration
+constexpr int kJobSlots = 4096;  // job descriptors resident at once
 
 }  // namespace
 
 struct Engine::Wave {
   WaveBuffers wb{};
-  std::uint64_t radiance_cap = 0;
   RtgSceneDev* jobs_dev = nullptr;
-  std::size_t jobs_cap = 0;
-  std::uint32_t* ids_dev = nullptr;
-  std::uint64_t* begin_dev = nullptr;
-  std::size_t table_cap = 0;
-  WaveCounters* ring = nullptr;  // pinned host
-  cudaEvent_t ring_ev[kRing]{};
-  cudaEvent_t tev[8]{};
+  DevSegment* segs_dev = nullptr;
+  SegmentProgress* prog_dev = nullptr;
+  GenTable* gen_dev = nullptr;
+  GenPlan* plan_dev = nullptr;
+  WaveSnapshot* ring = nullptr;        // pinned, device-mapped
+  unsigned char* staging = nullptr;    // pinned, kRing * kStageBytes
+  std::uint64_t stage_it = ~0ull;      // iteration the current staging slot belongs to
+  std::size_t stage_used = 0;
+  cudaEvent_t plan_ev[kRing]{};
+  bool plan_recorded[kRing]{};
+  cudaEvent_t tev[10]{};
+  std::uint64_t it = 0;                // iterations launched (the device's `iteration`)
+  std::uint64_t seen = 0;              // next snapshot to read: the one plan(seen) wrote
+  std::uint64_t rad_cap = 0;
+  std::map<std::uint64_t, std::uint64_t> rad_free;  // free radiance ranges: begin -> length
+  std::vector<int> free_jobs;          // descriptor slots, popped from the back
+  std::vector<int> free_segs;
+  std::uint32_t snapshot_slots = 0;
+  std::uint32_t hi_slot = 0;           // segment slots ever used are below this
+  std::uint64_t stall = 0;             // snapshots without a finished sample while work is open
+  std::uint64_t last_done_sum = 0;
+
+  bool rad_alloc(std::uint64_t n, std::uint64_t& at) {
+    for (auto itr = rad_free.begin(); itr != rad_free.end(); ++itr) {
+      if (itr->second < n) continue;
+      at = itr->first;
+      const std::uint64_t rest = itr->second - n;
+      rad_free.erase(itr);
+      if (rest) rad_free.emplace(at + n, rest);
+      return true;
+    }
+    return false;
+  }
+  void rad_release(std::uint64_t at, std::uint64_t n) {
+    auto nx = rad_free.lower_bound(at);
+    if (nx != rad_free.end() && at + n == nx->first) {
+      n += nx->second;
+      nx = rad_free.erase(nx);
+    }
+    if (nx != rad_free.begin()) {
+      auto pv = std::prev(nx);
+      if (pv->first + pv->second == at) {
+        pv->second += n;
+        return;
+      }
+    }
+    rad_free.emplace(at, n);
+  }
 };
 
 Engine::Engine(int device) : device_(device) {
@@ -82,12 +129,10 @@ Engine::~Engine() {
   cudaSetDevice(device_);
   cudaStreamSynchronize(stream_);
   for (auto& f : frames_) free_frame(f);
-  for (auto& kv : scenes_) {
-    GpuScene& s = *kv.second;
-    dev_free(s.nodes); dev_free(s.prims); dev_free(s.slot_material); dev_free(s.slot_normals);
-    dev_free(s.planes); dev_free(s.materials); dev_free(s.lights);
-    dev_free(s.prims64); dev_free(s.planes64);
-  }
+  for (auto& kv : jobs_) free_frame(kv.second.frame);
+  cudaStreamSynchronize(stream_);
+  for (auto& kv : scenes_) free_scene_arrays(*kv.second);
+  jobs_.clear();
   reset_wave();
   cudaEventDestroy(ev_begin_);
   cudaEventDestroy(ev_end_);
@@ -95,17 +140,21 @@ Engine::~Engine() {
 }
 
 void Engine::reset_wave() {
+  if (!jobs_.empty()) throw std::logic_error("the wavefront has open jobs");
   cudaStreamSynchronize(stream_);
   if (wave_) {
     WaveBuffers& b = wave_->wb;
     for (int i = 0; i < 2; ++i) { dev_free(b.st_a[i]); dev_free(b.st_b[i]); dev_free(b.st_c[i]); dev_free(b.st_d[i]); }
     dev_free(b.hits); dev_free(b.sh_a); dev_free(b.sh_b); dev_free(b.sh_c); dev_free(b.radiance); dev_free(b.cnt);
-    dev_free(wave_->jobs_dev); dev_free(wave_->ids_dev); dev_free(wave_->begin_dev);
+    dev_free(wave_->jobs_dev); dev_free(wave_->segs_dev); dev_free(wave_->prog_dev);
+    dev_free(wave_->gen_dev); dev_free(wave_->plan_dev);
     if (wave_->ring) cudaFreeHost(wave_->ring);
-    for (auto& e : wave_->ring_ev) if (e) cudaEventDestroy(e);
+    if (wave_->staging) cudaFreeHost(wave_->staging);
+    for (auto& e : wave_->plan_ev) if (e) cudaEventDestroy(e);
     for (auto& e : wave_->tev) if (e) cudaEventDestroy(e);
     wave_.reset();
   }
+  segs_.clear();
 }
 
 int Engine::add_scene(CompiledScene scene) {
@@ -136,11 +185,9 @@ int Engine::add_scene(CompiledScene scene) {
 void Engine::release_scene(int id) {
   auto it = scenes_.find(id);
   if (it == scenes_.end()) throw std::invalid_argument("unknown scene id " + std::to_string(id));
+  if (it->second->jobs_open > 0) throw std::logic_error("scene " + std::to_string(id) + " is used by an open request");
   cudaStreamSynchronize(stream_);
-  GpuScene& s = *it->second;
-  dev_free(s.nodes); dev_free(s.prims); dev_free(s.slot_material); dev_free(s.slot_normals);
-  dev_free(s.planes); dev_free(s.materials); dev_free(s.lights);
-    dev_free(s.prims64); dev_free(s.planes64);
+  free_scene_arrays(*it->second);
   scenes_.erase(it);
 }
 
@@ -150,32 +197,55 @@ GpuScene& Engine::scene(int id) {
   return *it->second;
 }
 
-void Engine::ensure_wave(std::uint64_t pass_samples) {
-  if (!wave_) {
-    wave_ = std::make_unique<Wave>();
-    WaveBuffers& b = wave_->wb;
-    const std::uint32_t P = cfg_.pool_paths;
-    b.capacity = P;
-    for (int i = 0; i < 2; ++i) {
-      b.st_a[i] = dev_alloc<float4>(P);
-      b.st_b[i] = dev_alloc<float4>(P);
-      b.st_c[i] = dev_alloc<float4>(P);
-      b.st_d[i] = dev_alloc<uint4>(P);
-    }
-    b.hits = dev_alloc<float4>(P);
-    b.sh_a = dev_alloc<float4>(P);
-    b.sh_b = dev_alloc<float4>(P);
-    b.sh_c = dev_alloc<float4>(P);
-    b.cnt = dev_alloc<WaveCounters>(1);
-    CK(cudaMallocHost(reinterpret_cast<void**>(&wave_->ring), sizeof(WaveCounters) * kRing));
-    for (auto& e : wave_->ring_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-    for (auto& e : wave_->tev) CK(cudaEventCreate(&e));
+void Engine::ensure_wave() {
+  if (wave_) return;
+  CK(cudaSetDevice(device_));
+  if (cfg_.pool_paths < 32 || cfg_.pool_paths > (1u << 23)) throw std::invalid_argument("pool_paths must be in [32, 2^23]");
+  wave_ = std::make_unique<Wave>();
+  Wave& W = *wave_;
+  WaveBuffers& b = W.wb;
+  const std::uint32_t P = cfg_.pool_paths;
+  b.capacity = P;
+  for (int i = 0; i < 2; ++i) {
+    b.st_a[i] = dev_alloc<float4>(P);
+    b.st_b[i] = dev_alloc<float4>(P);
+    b.st_c[i] = dev_alloc<float4>(P);
+    b.st_d[i] = dev_alloc<uint4>(P);
   }
-  if (pass_samples > wave_->radiance_cap) {
-    dev_free(wave_->wb.radiance);
-    wave_->wb.radiance = dev_alloc<float4>(pass_samples);
-    wave_->radiance_cap = pass_samples;
-  }
+  b.hits = dev_alloc<float4>(P);
+  b.sh_a = dev_alloc<float4>(P);
+  b.sh_b = dev_alloc<float4>(P);
+  b.sh_c = dev_alloc<float4>(P);
+  W.rad_cap = std::max<std::uint64_t>(1, std::min<std::uint64_t>(cfg_.max_pass_samples, 0xFFFFFFFFull));
+  b.radiance = dev_alloc<float4>(W.rad_cap);
+  W.rad_free.emplace(0, W.rad_cap);
+  b.cnt = dev_alloc<WaveCounters>(1);
+  W.jobs_dev = dev_alloc<RtgSceneDev>(kJobSlots);
+  W.segs_dev = dev_alloc<DevSegment>(kMaxSegments);
+  W.prog_dev = dev_alloc<SegmentProgress>(kMaxSegments);
+  W.gen_dev = dev_alloc<GenTable>(1);
+  W.plan_dev = dev_alloc<GenPlan>(1);
+  CK(cudaMemset(b.cnt, 0, sizeof(WaveCounters)));
+  CK(cudaMemset(W.prog_dev, 0, sizeof(SegmentProgress) * kMaxSegments));
+  CK(cudaMemset(W.gen_dev, 0, sizeof(GenTable)));
+  CK(cudaMemset(W.plan_dev, 0, sizeof(GenPlan)));
+  CK(cudaHostAlloc(reinterpret_cast<void**>(&W.ring), sizeof(WaveSnapshot) * kRing, cudaHostAllocMapped));
+  WaveSnapshot* ring_dev = nullptr;
+  CK(cudaHostGetDevicePointer(reinterpret_cast<void**>(&ring_dev), W.ring, 0));
+  CK(cudaMallocHost(reinterpret_cast<void**>(&W.staging), kStageBytes * kRing));
+  for (auto& e : W.plan_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  for (auto& e : W.tev) CK(cudaEventCreate(&e));
+  b.jobs = W.jobs_dev;
+  b.segs = W.segs_dev;
+  b.seg_prog = W.prog_dev;
+  b.gen = W.gen_dev;
+  b.plan = W.plan_dev;
+  b.ring = ring_dev;
+  b.ring_size = kRing;
+  for (int k = kJobSlots - 1; k >= 0; --k) W.free_jobs.push_back(k);
+  for (int k = kMaxSegments - 1; k >= 0; --k) W.free_segs.push_back(k);
+  segs_.assign(kMaxSegments, Seg{});
+  CK(cudaDeviceSynchronize());
 }
 
 GpuFrame Engine::make_frame(int w, int h) {
@@ -183,10 +253,10 @@ GpuFrame Engine::make_frame(int w, int h) {
   f.width = w;
   f.height = h;
   const std::size_t px = std::size_t(w) * std::size_t(h);
-  f.sum = dev_alloc<double>(px * 4);
-  f.sumsq = dev_alloc<double>(px * 4);
-  f.count = dev_alloc<std::uint32_t>(px);
-  f.stats = dev_alloc<std::uint64_t>(4);
+  f.sum = dev_alloc_async<double>(px * 4, stream_);
+  f.sumsq = dev_alloc_async<double>(px * 4, stream_);
+  f.count = dev_alloc_async<std::uint32_t>(px, stream_);
+  f.stats = dev_alloc_async<std::uint64_t>(4, stream_);
   CK(cudaMemsetAsync(f.sum, 0, px * 4 * sizeof(double), stream_));
   CK(cudaMemsetAsync(f.sumsq, 0, px * 4 * sizeof(double), stream_));
   CK(cudaMemsetAsync(f.count, 0, px * sizeof(std::uint32_t), stream_));
@@ -195,7 +265,9 @@ GpuFrame Engine::make_frame(int w, int h) {
 }
 
 void Engine::free_frame(GpuFrame& f) {
-  dev_free(f.sum); dev_free(f.sumsq); dev_free(f.count); dev_free(f.stats);
+  for (void* p : {static_cast<void*>(f.sum), static_cast<void*>(f.sumsq), static_cast<void*>(f.count),
+                  static_cast<void*>(f.stats)})
+    if (p) cudaFreeAsync(p, stream_);
   f = GpuFrame{};
 }
 
@@ -223,285 +295,575 @@ RtgSceneDev Engine::job_descriptor(const GpuScene& sc, const RenderSettings& s, 
   return d;
 }
 
-bool Engine::run_pass(std::vector<RtgSceneDev>& jobs, const std::vector<std::uint32_t>& ids, std::uint64_t total,
-                      bool direct, const volatile std::int32_t* cancel) {
+// ---------------------------------------------------------------------------
+// Host->device writes of the scheduler go through a pinned staging slot that
+// belongs to the next iteration, so they never wait for the stream.
+void Engine::stage(void* dst, const void* src, std::size_t n) {
   Wave& W = *wave_;
-  // Stage descriptors and the pass table.
-  if (jobs.size() > W.jobs_cap) {
-    dev_free(W.jobs_dev);
-    W.jobs_dev = dev_alloc<RtgSceneDev>(jobs.size());
-    W.jobs_cap = jobs.size();
+  const int r = static_cast<int>(W.it % kRing);
+  if (W.stage_it != W.it) {
+    if (W.plan_recorded[r]) CK(cudaEventSynchronize(W.plan_ev[r]));  // its last copies have run
+    W.stage_it = W.it;
+    W.stage_used = 0;
   }
-  if (ids.size() > W.table_cap) {
-    dev_free(W.ids_dev);
-    dev_free(W.begin_dev);
-    W.ids_dev = dev_alloc<std::uint32_t>(ids.size());
-    W.begin_dev = dev_alloc<std::uint64_t>(ids.size());
-    W.table_cap = ids.size();
+  const std::size_t at = (W.stage_used + 15) & ~std::size_t(15);
+  if (at + n > kStageBytes) {
+    // Burst larger than a staging slot: fall back to a synchronous copy.
+    CK(cudaStreamSynchronize(stream_));
+    CK(cudaMemcpy(dst, src, n, cudaMemcpyHostToDevice));
+    return;
   }
-  std::vector<std::uint64_t> begin(ids.size());
-  std::uint64_t acc = 0;
-  for (std::size_t k = 0; k < ids.size(); ++k) {
-    begin[k] = acc;
-    acc += jobs[ids[k]].work_count;
-  }
-  CK(cudaMemcpyAsync(W.jobs_dev, jobs.data(), jobs.size() * sizeof(RtgSceneDev), cudaMemcpyHostToDevice, stream_));
-  CK(cudaMemcpyAsync(W.ids_dev, ids.data(), ids.size() * sizeof(std::uint32_t), cudaMemcpyHostToDevice, stream_));
-  CK(cudaMemcpyAsync(W.begin_dev, begin.data(), begin.size() * sizeof(std::uint64_t), cudaMemcpyHostToDevice, stream_));
-  PassTable pt{W.jobs_dev, W.ids_dev, W.begin_dev, static_cast<std::int32_t>(ids.size())};
-
-  WaveCounters init{};
-  init.total_work = total;
-  CK(cudaMemcpyAsync(W.wb.cnt, &init, sizeof(init), cudaMemcpyHostToDevice, stream_));
-  const bool timed = cfg_.time_kernels;
-  bool cancelled = false;
-
-  if (direct) {
-    if (timed) CK(cudaEventRecord(W.tev[0], stream_));
-    CK(launch_direct(pt, total, W.wb.radiance, W.wb.cnt, stream_));
-    stats_.kernel_launches += 1;
-    if (timed) {
-      CK(cudaEventRecord(W.tev[1], stream_));
-      CK(cudaEventSynchronize(W.tev[1]));
-      float ms = 0;
-      CK(cudaEventElapsedTime(&ms, W.tev[0], W.tev[1]));
-      stats_.direct_ms += ms;
-    }
-  } else {
-    // Generous bound on iterations: every path needs at most max_depth of them
-    // and the pool refills at least once per max_depth iterations.
-    int max_depth = 1;
-    for (std::uint32_t id : ids) max_depth = std::max(max_depth, jobs[id].max_depth);
-    const std::uint64_t fills = total / W.wb.capacity + 2;
-    const std::uint64_t it_cap = fills * static_cast<std::uint64_t>(max_depth + 2) * 4 + 64;
-    std::uint64_t it = 0;
-    bool done = false;
-    while (!done) {
-      if (it > it_cap) throw CudaFailure("wavefront did not drain (iteration bound exceeded)");
-      const int par = static_cast<int>(it & 1);
-      if (timed) {
-        float ms[3] = {0, 0, 0};
-        const Stage stages[3] = {Stage::Extend, Stage::Shade, Stage::Shadow};
-        for (int k = 0; k < 3; ++k) {
-          CK(cudaEventRecord(W.tev[2 * k], stream_));
-          CK(launch_stage(stages[k], W.wb, pt, par, cfg_.shape, cfg_.count_traversal, stream_));
-          CK(cudaEventRecord(W.tev[2 * k + 1], stream_));
-        }
-        CK(cudaEventSynchronize(W.tev[5]));
-        for (int k = 0; k < 3; ++k) CK(cudaEventElapsedTime(&ms[k], W.tev[2 * k], W.tev[2 * k + 1]));
-        stats_.extend_ms += ms[0];
-        stats_.shade_ms += ms[1];
-        stats_.shadow_ms += ms[2];
-        stats_.extend_launches++;
-      } else {
-        CK(launch_iteration(W.wb, pt, par, cfg_.shape, cfg_.count_traversal, stream_));
-      }
-      stats_.kernel_launches += 3;
-      const int slot = static_cast<int>(it % kRing);
-      CK(cudaMemcpyAsync(&W.ring[slot], W.wb.cnt, sizeof(WaveCounters), cudaMemcpyDeviceToHost, stream_));
-      CK(cudaEventRecord(W.ring_ev[slot], stream_));
-      stats_.iterations++;
-      if (it >= static_cast<std::uint64_t>(kLag)) {
-        const std::uint64_t j = it - kLag;
-        CK(cudaEventSynchronize(W.ring_ev[j % kRing]));
-        const WaveCounters& c = W.ring[j % kRing];
-        if (c.error) throw CudaFailure("device error flag " + std::to_string(c.error));
-        if (c.live[(j + 1) & 1] == 0 && c.next_work >= c.total_work) done = true;
-      }
-      ++it;
-      if (cancel && *cancel) {
-        cancelled = true;
-        break;
-      }
-    }
-  }
-  if (!cancelled) {
-    if (timed) CK(cudaEventRecord(W.tev[6], stream_));
-    for (std::uint32_t id : ids) CK(launch_accumulate(W.jobs_dev + id, jobs[id], W.wb.radiance, stream_));
-    stats_.kernel_launches += ids.size();
-    if (timed) CK(cudaEventRecord(W.tev[7], stream_));
-  }
-  CK(cudaStreamSynchronize(stream_));
-  if (timed && !cancelled) {
-    float ms = 0;
-    CK(cudaEventElapsedTime(&ms, W.tev[6], W.tev[7]));
-    stats_.accumulate_ms += ms;
-  }
-  WaveCounters end{};
-  CK(cudaMemcpy(&end, W.wb.cnt, sizeof(end), cudaMemcpyDeviceToHost));
-  if (end.error) throw CudaFailure("device error flag " + std::to_string(end.error) +
-                                   (end.error == 2 ? " (direct integrator branch stack overflow)" : ""));
-  stats_.rays += end.rays;
-  stats_.shadow_rays += end.shadow_rays;
-  stats_.rr_terminated += end.rr_terminated;
-  stats_.node_visits += end.node_visits;
-  stats_.prim_tests += end.prim_tests;
-  stats_.sphere_tests += end.sphere_tests;
-  stats_.shadow_node_visits += end.shadow_node_visits;
-  stats_.shadow_prim_tests += end.shadow_prim_tests;
-  stats_.shadow_sphere_tests += end.shadow_sphere_tests;
-  stats_.passes++;
-  return !cancelled;
+  unsigned char* p = W.staging + std::size_t(r) * kStageBytes + at;
+  std::memcpy(p, src, n);
+  CK(cudaMemcpyAsync(dst, p, n, cudaMemcpyHostToDevice, stream_));
+  W.stage_used = at + n;
 }
 
+void Engine::write_gen_table() {
+  Wave& W = *wave_;
+  // Open segments still generating, in priority order: previews before finals,
+  // then earlier passes before later ones (a new render's first pass overtakes
+  // the later passes of renders already running), then submission order.
+  std::vector<int> open;
+  std::uint32_t hi = 0;
+  for (int k = 0; k < static_cast<int>(W.hi_slot); ++k) {
+    Seg& s = segs_[k];
+    if (!s.used) continue;
+    hi = static_cast<std::uint32_t>(k + 1);
+    s.in_gen = false;
+    if (s.complete || s.abandoned || s.generated >= s.d.count) continue;
+    open.push_back(k);
+  }
+  std::sort(open.begin(), open.end(), [&](int a, int b) {
+    const Job& ja = jobs_.at(segs_[a].job);
+    const Job& jb = jobs_.at(segs_[b].job);
+    if (ja.priority != jb.priority) return ja.priority < jb.priority;
+    if (segs_[a].d.pass_s0 != segs_[b].d.pass_s0) return segs_[a].d.pass_s0 < segs_[b].d.pass_s0;
+    return ja.seq < jb.seq;
+  });
+  GenTable g{};
+  g.n = static_cast<std::uint32_t>(std::min<std::size_t>(open.size(), kMaxGen));
+  for (std::uint32_t k = 0; k < g.n; ++k) {
+    g.slot[k] = static_cast<std::uint32_t>(open[k]);
+    segs_[open[k]].in_gen = true;
+  }
+  g.snapshot_slots = hi;
+  W.snapshot_slots = hi;
+  stage(W.gen_dev, &g, offsetof(GenTable, slot) + sizeof(std::uint32_t) * std::max<std::uint32_t>(g.n, 1));
+  gen_dirty_ = false;
+}
+
+int Engine::open_job(const JobSpec& spec, bool serving, PassCallback cb) {
+  ensure_wave();
+  Wave& W = *wave_;
+  GpuScene& sc = scene(spec.scene_id);
+  if (W.free_jobs.empty()) throw std::length_error("too many open renders");
+  Job j;
+  j.handle = next_job_++;
+  j.desc_slot = W.free_jobs.back();
+  W.free_jobs.pop_back();
+  j.scene_id = spec.scene_id;
+  j.settings = spec.settings;
+  j.opts = spec.opts;
+  j.priority = spec.priority;
+  j.seq = job_seq_++;
+  j.pixels = std::uint64_t(spec.settings.width) * std::uint64_t(spec.settings.height);
+  j.target = static_cast<std::uint32_t>(spec.settings.spp);
+  j.direct = spec.settings.integrator == Integrator::Direct;
+  j.serving = serving;
+  j.on_pass = std::move(cb);
+  j.t0 = std::chrono::steady_clock::now();
+  j.prog.spp_target = spec.settings.spp;
+  j.frame = make_frame(spec.settings.width, spec.settings.height);
+  const RtgSceneDev d = job_descriptor(sc, spec.settings, j.frame);
+  stage(W.jobs_dev + j.desc_slot, &d, sizeof(d));
+  sc.jobs_open++;
+  const int h = j.handle;
+  jobs_.emplace(h, std::move(j));
+  return h;
+}
+
+void Engine::close_job(Job& j) {
+  Wave& W = *wave_;
+  W.free_jobs.push_back(j.desc_slot);
+  auto it = scenes_.find(j.scene_id);
+  if (it != scenes_.end()) it->second->jobs_open--;
+}
+
+bool Engine::all_jobs_drained() const {
+  for (const auto& kv : jobs_)
+    if (!kv.second.drained()) return false;
+  return true;
+}
+
+std::uint32_t Engine::next_pass_size(const Job& j) const {
+  std::uint32_t k = j.target - j.issued;
+  if (j.opts.progressive) {
+    const std::uint32_t grow = std::max<std::uint32_t>(1u, j.issued);
+    const std::uint32_t cap = static_cast<std::uint32_t>(std::max(1, j.opts.max_pass_spp));
+    k = std::min({k, grow, cap});
+  }
+  const std::uint64_t fit = std::max<std::uint64_t>(1, wave_->rad_cap / std::max<std::uint64_t>(1, j.pixels));
+  return static_cast<std::uint32_t>(std::min<std::uint64_t>(k, fit));
+}
+
+bool Engine::issue_pass(Job& j) {
+  Wave& W = *wave_;
+  const std::uint32_t k = next_pass_size(j);
+  const std::uint64_t count = j.pixels * k;
+  if (W.free_segs.empty()) return false;
+  std::uint64_t at = 0;
+  if (!W.rad_alloc(count, at)) return false;
+  const int slot = W.free_segs.back();
+  W.free_segs.pop_back();
+  W.hi_slot = std::max<std::uint32_t>(W.hi_slot, static_cast<std::uint32_t>(slot + 1));
+  Seg& s = segs_[slot];
+  s = Seg{};
+  s.used = true;
+  s.job = j.handle;
+  s.d.job = static_cast<std::uint32_t>(j.desc_slot);
+  s.d.pass_s0 = j.issued;
+  s.d.pass_spp = k;
+  s.d.count = count;
+  s.d.sample_base = at;
+  s.rad_begin = at;
+  s.assigned_at = W.it;
+  const SegmentProgress zero{};
+  stage(W.segs_dev + slot, &s.d, sizeof(s.d));
+  stage(W.prog_dev + slot, &zero, sizeof(zero));
+  j.issued += k;
+  j.passes_issued++;
+  j.segs.push_back(slot);
+  gen_dirty_ = true;
+  return true;
+}
+
+bool Engine::run_direct_pass(Job& j) {
+  Wave& W = *wave_;
+  const std::uint32_t k = next_pass_size(j);
+  const std::uint64_t count = j.pixels * k;
+  std::uint64_t at = 0;
+  if (!W.rad_alloc(count, at)) return false;  // retried once radiance space frees up
+  DevSegment d{};
+  d.job = static_cast<std::uint32_t>(j.desc_slot);
+  d.pass_s0 = j.issued;
+  d.pass_spp = k;
+  d.count = count;
+  d.sample_base = at;
+  const bool timed = cfg_.time_kernels;
+  if (timed) CK(cudaEventRecord(W.tev[8], stream_));
+  CK(launch_direct(W.jobs_dev + j.desc_slot, d, W.wb.radiance, W.wb.cnt, stream_));
+  if (timed) CK(cudaEventRecord(W.tev[9], stream_));
+  CK(launch_accumulate(W.jobs_dev + j.desc_slot, j.pixels, d, W.wb.radiance, stream_));
+  stats_.kernel_launches += 2;
+  // Reported once it has run, so progress times are device-complete.
+  CK(cudaStreamSynchronize(stream_));
+  if (timed) {
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, W.tev[8], W.tev[9]));
+    stats_.direct_ms += ms;
+  }
+  W.rad_release(at, count);
+  WaveCounters c{};
+  CK(cudaMemcpy(&c, W.wb.cnt, sizeof(c), cudaMemcpyDeviceToHost));
+  if (c.error) throw CudaFailure("device error flag " + std::to_string(c.error) +
+                                 (c.error == 2 ? " (direct integrator branch stack overflow)" : ""));
+  last_counters_ = c;
+  j.issued += k;
+  j.passes_issued++;
+  j.done += k;
+  j.prog.pass++;
+  j.prog.spp_done = j.done;
+  j.prog.finished = j.done >= j.target;
+  j.prog.elapsed_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - j.t0).count();
+  j.prog.rays = (c.rays - base_counters_.rays) + (c.shadow_rays - base_counters_.shadow_rays);
+  stats_.passes++;
+  return true;
+}
+
+void Engine::refill() {
+  Wave& W = *wave_;
+  // Samples not yet finished in the open segments, per priority level.
+  std::map<int, std::uint64_t> backlog;
+  for (int k = 0; k < static_cast<int>(W.hi_slot); ++k) {
+    const Seg& s = segs_[k];
+    if (!s.used || s.complete || s.abandoned) continue;
+    backlog[jobs_.at(s.job).priority] += s.d.count - std::min<std::uint64_t>(s.done, s.d.count);
+  }
+  const std::uint64_t target = std::uint64_t(cfg_.backlog_pools) * W.wb.capacity;
+  while (true) {
+    Job* best = nullptr;
+    for (auto& kv : jobs_) {
+      Job& j = kv.second;
+      if (j.cancelled || j.issued >= j.target) continue;
+      if (!best || j.priority < best->priority ||
+          (j.priority == best->priority &&
+           (j.passes_issued < best->passes_issued || (j.passes_issued == best->passes_issued && j.seq < best->seq))))
+        best = &j;
+    }
+    if (!best) return;
+    if (best->direct) {
+      // One whole pass per call, so cancellation is checked between passes.
+      if (run_direct_pass(*best) && best->on_pass) best->on_pass(best->prog);
+      return;
+    }
+    std::uint64_t ahead = 0;
+    for (const auto& kv : backlog)
+      if (kv.first <= best->priority) ahead += kv.second;
+    if (ahead >= target && !best->segs.empty()) return;
+    const std::uint64_t before = best->issued;
+    if (!issue_pass(*best)) return;
+    backlog[best->priority] += best->pixels * (best->issued - before);
+  }
+}
+
+// Folds finished segments at the head of a job into its framebuffer (pass order)
+// and reports each pass.
+void Engine::retire_segments(Job& j, std::vector<PassEvent>* events) {
+  Wave& W = *wave_;
+  auto free_seg = [&](int slot) {
+    Seg& s = segs_[slot];
+    W.rad_release(s.rad_begin, s.d.count);
+    s = Seg{};
+    W.free_segs.push_back(slot);
+    gen_dirty_ = true;
+  };
+  if (j.cancelled) {
+    for (auto it = j.segs.begin(); it != j.segs.end();) {
+      if (segs_[*it].complete) {
+        free_seg(*it);
+        it = j.segs.erase(it);
+      } else {
+        ++it;
+      }
+    }
+    return;
+  }
+  while (!j.segs.empty() && segs_[j.segs.front()].complete) {
+    const int slot = j.segs.front();
+    const Seg& s = segs_[slot];
+    const bool timed = cfg_.time_kernels;
+    if (timed) CK(cudaEventRecord(W.tev[8], stream_));
+    CK(launch_accumulate(W.jobs_dev + j.desc_slot, j.pixels, s.d, W.wb.radiance, stream_));
+    stats_.kernel_launches++;
+    if (timed) {
+      CK(cudaEventRecord(W.tev[9], stream_));
+      CK(cudaEventSynchronize(W.tev[9]));
+      float ms = 0;
+      CK(cudaEventElapsedTime(&ms, W.tev[8], W.tev[9]));
+      stats_.accumulate_ms += ms;
+    }
+    j.done += s.d.pass_spp;
+    free_seg(slot);
+    j.segs.pop_front();
+    stats_.passes++;
+    j.prog.pass++;
+    j.prog.spp_done = j.done;
+    j.prog.finished = j.done >= j.target;
+    j.prog.elapsed_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - j.t0).count();
+    j.prog.rays = (last_counters_.rays - base_counters_.rays) + (last_counters_.shadow_rays - base_counters_.shadow_rays);
+    if (events) events->push_back(PassEvent{j.handle, j.prog});
+    if (j.on_pass) j.on_pass(j.prog);
+  }
+}
+
+void Engine::process_snapshot(std::uint64_t iter, std::vector<PassEvent>* events) {
+  Wave& W = *wave_;
+  const int r = static_cast<int>(iter % kRing);
+  CK(cudaEventSynchronize(W.plan_ev[r]));
+  const WaveSnapshot& S = W.ring[r];
+  if (S.c.error) {
+    const std::uint32_t e = S.c.error;
+    throw CudaFailure("device error flag " + std::to_string(e) +
+                      (e == 3 ? " (generation table names segment slot " + std::to_string(S.c.error_info) + ")" : ""));
+  }
+  last_counters_ = S.c;
+  std::uint64_t done_sum = 0;
+  bool open = false;
+  int max_depth = 1;
+  const std::uint32_t ns = std::min<std::uint32_t>(W.snapshot_slots, kMaxSegments);
+  for (std::uint32_t k = 0; k < ns; ++k) {
+    Seg& s = segs_[k];
+    // A slot assigned after this plan ran has no data in it yet.
+    if (!s.used || s.complete || iter < s.assigned_at) continue;
+    s.done = S.seg[k].done;
+    s.generated = S.seg[k].generated;
+    done_sum += s.done;
+    open = true;
+    max_depth = std::max(max_depth, jobs_.at(s.job).settings.max_depth);
+    if (s.abandoned ? (iter >= s.closed_at && s.done >= s.generated) : s.done >= s.d.count) {
+      s.complete = true;
+      gen_dirty_ = true;
+    } else if (s.in_gen && s.generated >= s.d.count) {
+      gen_dirty_ = true;  // fully generated: leaves the table
+    }
+  }
+  // Watchdog: a path lives at most max_depth iterations, so open work that
+  // finishes nothing for much longer than that means the wavefront is stuck.
+  if (open && done_sum == W.last_done_sum) {
+    if (++W.stall > static_cast<std::uint64_t>(max_depth) + kRing + 64)
+      throw CudaFailure("wavefront stalled: no sample finished for " + std::to_string(W.stall) + " iterations");
+  } else {
+    W.stall = 0;
+  }
+  W.last_done_sum = done_sum;
+  for (auto& kv : jobs_) retire_segments(kv.second, events);
+}
+
+void Engine::launch_one_iteration() {
+  Wave& W = *wave_;
+  if (gen_dirty_) write_gen_table();
+  const int par = static_cast<int>(W.it & 1);
+  const int r = static_cast<int>(W.it % kRing);
+  const bool timed = cfg_.time_kernels;
+  const bool count = cfg_.count_traversal;
+  const Stage stages[4] = {Stage::Plan, Stage::Extend, Stage::Shade, Stage::Shadow};
+  for (int k = 0; k < 4; ++k) {
+    if (timed) CK(cudaEventRecord(W.tev[2 * k], stream_));
+    CK(launch_stage(stages[k], W.wb, par, cfg_.shape, count, stream_));
+    if (timed) CK(cudaEventRecord(W.tev[2 * k + 1], stream_));
+    if (k == 0) {
+      CK(cudaEventRecord(W.plan_ev[r], stream_));
+      W.plan_recorded[r] = true;
+    }
+  }
+  if (timed) {
+    CK(cudaEventSynchronize(W.tev[7]));
+    float ms[4] = {0, 0, 0, 0};
+    for (int k = 0; k < 4; ++k) CK(cudaEventElapsedTime(&ms[k], W.tev[2 * k], W.tev[2 * k + 1]));
+    stats_.plan_ms += ms[0];
+    stats_.extend_ms += ms[1];
+    stats_.shade_ms += ms[2];
+    stats_.shadow_ms += ms[3];
+  }
+  stats_.extend_launches++;
+  stats_.kernel_launches += 4;
+  stats_.iterations++;
+  W.it++;
+}
+
+void Engine::drain(const volatile std::int32_t* cancel, std::vector<PassEvent>* events, double budget_ms,
+                   bool return_on_event) {
+  Wave& W = *wave_;
+  const auto t0 = std::chrono::steady_clock::now();
+  const std::size_t events0 = events ? events->size() : 0;
+  while (true) {
+    if (cancel && *cancel) return;
+    refill();
+    if (all_jobs_drained()) return;
+    launch_one_iteration();
+    while (W.seen + kLag < W.it) process_snapshot(W.seen++, events);
+    if (return_on_event && events && events->size() > events0) return;
+    if (budget_ms < std::numeric_limits<double>::infinity() &&
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count() >= budget_ms)
+      return;
+  }
+}
+
+void Engine::abort_all() {
+  Wave& W = *wave_;
+  CK(cudaStreamSynchronize(stream_));
+  WaveCounters c{};
+  CK(cudaMemcpy(&c, W.wb.cnt, sizeof(c), cudaMemcpyDeviceToHost));
+  c.live[0] = c.live[1] = 0;
+  c.n_extend = c.n_shadow = 0;
+  CK(cudaMemcpy(W.wb.cnt, &c, sizeof(c), cudaMemcpyHostToDevice));
+  for (int k = 0; k < kMaxSegments; ++k)
+    if (segs_[k].used) {
+      segs_[k] = Seg{};
+      W.free_segs.push_back(k);
+    }
+  W.rad_free.clear();
+  W.rad_free.emplace(0, W.rad_cap);
+  for (auto& kv : jobs_) kv.second.segs.clear();
+  W.seen = W.it;
+  W.stall = 0;
+  W.last_done_sum = 0;
+  gen_dirty_ = true;
+  write_gen_table();
+}
+
+void Engine::begin_stats() {
+  stats_ = RenderStats{};
+  CK(cudaStreamSynchronize(stream_));
+  CK(cudaMemcpy(&base_counters_, wave_->wb.cnt, sizeof(base_counters_), cudaMemcpyDeviceToHost));
+  last_counters_ = base_counters_;
+  CK(cudaEventRecord(ev_begin_, stream_));
+}
+
+void Engine::end_stats() {
+  finish_timing();
+  WaveCounters end{};
+  CK(cudaMemcpy(&end, wave_->wb.cnt, sizeof(end), cudaMemcpyDeviceToHost));
+  if (end.error) throw CudaFailure("device error flag " + std::to_string(end.error));
+  const WaveCounters& b = base_counters_;
+  stats_.rays = end.rays - b.rays;
+  stats_.shadow_rays = end.shadow_rays - b.shadow_rays;
+  stats_.rr_terminated = end.rr_terminated - b.rr_terminated;
+  stats_.node_visits = end.node_visits - b.node_visits;
+  stats_.prim_tests = end.prim_tests - b.prim_tests;
+  stats_.sphere_tests = end.sphere_tests - b.sphere_tests;
+  stats_.shadow_node_visits = end.shadow_node_visits - b.shadow_node_visits;
+  stats_.shadow_prim_tests = end.shadow_prim_tests - b.shadow_prim_tests;
+  stats_.shadow_sphere_tests = end.shadow_sphere_tests - b.shadow_sphere_tests;
+}
+
+// ---------------------------------------------------------------------------
 RenderProgress Engine::render(int scene_id, const RenderSettings& settings, const RenderOptions& opts,
                               const PassCallback& on_pass, const volatile std::int32_t* cancel) {
-  CK(cudaSetDevice(device_));
-  GpuScene& sc = scene(scene_id);
-  for (auto& f : frames_) free_frame(f);
-  frames_.clear();
-  stats_ = RenderStats{};
-  const auto t0 = std::chrono::steady_clock::now();
-
-  frames_.push_back(make_frame(settings.width, settings.height));
-  std::vector<RtgSceneDev> jobs(1, job_descriptor(sc, settings, frames_[0]));
-  CK(cudaEventRecord(ev_begin_, stream_));
-
-  const std::uint64_t pixels = std::uint64_t(settings.width) * std::uint64_t(settings.height);
-  const std::uint32_t target = static_cast<std::uint32_t>(settings.spp);
-  const bool direct = settings.integrator == Integrator::Direct;
-  RenderProgress prog;
-  prog.spp_target = settings.spp;
-  std::uint32_t done = 0;
-  while (done < target) {
-    std::uint32_t k = pass_size(done, target, opts);
-    const std::uint64_t fit = std::max<std::uint64_t>(1, cfg_.max_pass_samples / std::max<std::uint64_t>(1, pixels));
-    k = static_cast<std::uint32_t>(std::min<std::uint64_t>(k, fit));
-    ensure_wave(pixels * k);
-    RtgSceneDev& J = jobs[0];
-    J.pass_s0 = done;
-    J.pass_spp = k;
-    J.work_begin = 0;
-    J.work_count = pixels * k;
-    J.sample_base = 0;
-    const bool complete = run_pass(jobs, {0u}, pixels * k, direct, cancel);
-    prog.pass++;
-    prog.elapsed_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-    prog.rays = stats_.rays + stats_.shadow_rays;
-    if (complete) done += k;
-    stats_.camera_samples = pixels * done;
-    stats_.elapsed_ms = prog.elapsed_ms;
-    if (!complete || (cancel && *cancel)) {
-      prog.cancelled = true;
-      prog.spp_done = done;
-      if (on_pass) on_pass(prog);
-      break;
-    }
-    prog.spp_done = done;
-    prog.finished = done >= target;
-    if (on_pass) on_pass(prog);
-  }
-  finish_timing();
-  std::uint64_t invalid = 0;
-  CK(cudaMemcpy(&invalid, frames_[0].stats, sizeof(invalid), cudaMemcpyDeviceToHost));
-  stats_.invalid_samples = invalid;
-  stats_.elapsed_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-  return prog;
+  std::vector<RenderProgress> p =
+      render_batch({BatchJob{scene_id, settings}}, opts, cancel, on_pass);
+  return p[0];
 }
 
 std::vector<RenderProgress> Engine::render_batch(const std::vector<BatchJob>& batch, const RenderOptions& opts,
-                                                 const volatile std::int32_t* cancel) {
+                                                 const volatile std::int32_t* cancel, const PassCallback& on_pass) {
   CK(cudaSetDevice(device_));
+  if (serve_open_ > 0) throw std::logic_error("serving requests are open on this context");
   for (auto& f : frames_) free_frame(f);
   frames_.clear();
-  stats_ = RenderStats{};
+  frame_settings_.clear();
+  ensure_wave();
+  begin_stats();
   const auto t0 = std::chrono::steady_clock::now();
-  const std::size_t n = batch.size();
-  std::vector<RtgSceneDev> jobs;
-  jobs.reserve(n);
-  for (std::size_t j = 0; j < n; ++j) {
-    frames_.push_back(make_frame(batch[j].settings.width, batch[j].settings.height));
-    jobs.push_back(job_descriptor(scene(batch[j].scene_id), batch[j].settings, frames_.back()));
+  std::vector<int> handles;
+  handles.reserve(batch.size());
+  for (const BatchJob& b : batch) {
+    JobSpec spec;
+    spec.scene_id = b.scene_id;
+    spec.settings = b.settings;
+    spec.opts = opts;
+    handles.push_back(open_job(spec, false, on_pass));
   }
-  CK(cudaEventRecord(ev_begin_, stream_));
-  std::vector<RenderProgress> prog(n);
-  std::vector<std::uint32_t> done(n, 0);
-  for (std::size_t j = 0; j < n; ++j) prog[j].spp_target = batch[j].settings.spp;
-  // Direct-integrator jobs run through their own kernel; everything else shares the wavefront.
-  for (int direct_group = 0; direct_group < 2; ++direct_group) {
-    while (true) {
-      std::vector<std::uint32_t> ids;
-      std::uint64_t total = 0;
-      for (std::size_t j = 0; j < n; ++j) {
-        const RenderSettings& s = batch[j].settings;
-        const bool is_direct = s.integrator == Integrator::Direct;
-        if (is_direct != (direct_group == 1)) continue;
-        const std::uint32_t target = static_cast<std::uint32_t>(s.spp);
-        if (done[j] >= target) continue;
-        const std::uint64_t pixels = std::uint64_t(s.width) * std::uint64_t(s.height);
-        std::uint32_t k = pass_size(done[j], target, opts);
-        const std::uint64_t fit = std::max<std::uint64_t>(1, cfg_.max_pass_samples / std::max<std::uint64_t>(1, pixels));
-        k = static_cast<std::uint32_t>(std::min<std::uint64_t>(k, fit));
-        // Keep one batched pass within the radiance buffer; later passes pick up the rest.
-        if (!ids.empty() && total + pixels * k > cfg_.max_pass_samples) continue;
-        RtgSceneDev& J = jobs[j];
-        J.pass_s0 = done[j];
-        J.pass_spp = k;
-        J.work_begin = total;
-        J.work_count = pixels * k;
-        J.sample_base = total;
-        ids.push_back(static_cast<std::uint32_t>(j));
-        total += pixels * k;
-      }
-      if (ids.empty()) break;
-      ensure_wave(total);
-      const bool complete = run_pass(jobs, ids, total, direct_group == 1, cancel);
-      const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-      for (std::uint32_t id : ids) {
-        if (complete) done[id] += jobs[id].pass_spp;
-        prog[id].pass++;
-        prog[id].spp_done = done[id];
-        prog[id].elapsed_ms = ms;
-        prog[id].finished = done[id] >= static_cast<std::uint32_t>(batch[id].settings.spp);
-      }
-      if (!complete || (cancel && *cancel)) {
-        for (auto& p : prog) p.cancelled = !p.finished;
-        finish_timing();
-        stats_.elapsed_ms = ms;
-        return prog;
-      }
+  rendering_ = handles;
+  bool cancelled = false;
+  try {
+    drain(cancel, nullptr, std::numeric_limits<double>::infinity(), false);
+    cancelled = cancel && *cancel && !all_jobs_drained();
+  } catch (...) {
+    rendering_.clear();
+    abort_all();
+    for (int h : handles) {
+      Job& j = jobs_.at(h);
+      free_frame(j.frame);
+      close_job(j);
+      jobs_.erase(h);
     }
+    throw;
   }
-  finish_timing();
+  if (cancelled) abort_all();
+  std::vector<RenderProgress> out;
   std::uint64_t samples = 0, invalid = 0;
-  for (std::size_t j = 0; j < n; ++j) {
+  if (cancelled)
+    for (int h : handles) {
+      Job& j = jobs_.at(h);
+      if (j.prog.finished) continue;
+      j.prog.cancelled = true;
+      j.prog.spp_done = j.done;
+      if (j.on_pass) j.on_pass(j.prog);
+    }
+  rendering_.clear();
+  for (int h : handles) {
+    Job& j = jobs_.at(h);
+    out.push_back(j.prog);
+    samples += j.pixels * j.done;
+    frames_.push_back(j.frame);
+    frame_settings_.push_back(j.settings);
+    close_job(j);
+    jobs_.erase(h);
+  }
+  end_stats();
+  for (const GpuFrame& f : frames_) {
     std::uint64_t inv = 0;
-    CK(cudaMemcpy(&inv, frames_[j].stats, sizeof(inv), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&inv, f.stats, sizeof(inv), cudaMemcpyDeviceToHost));
     invalid += inv;
-    samples += std::uint64_t(batch[j].settings.width) * batch[j].settings.height * done[j];
   }
   stats_.camera_samples = samples;
   stats_.invalid_samples = invalid;
   stats_.elapsed_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-  for (auto& p : prog) p.rays = stats_.rays + stats_.shadow_rays;
-  return prog;
+  for (auto& p : out) p.rays = stats_.rays + stats_.shadow_rays;
+  return out;
 }
 
+// ---- serving ----
+std::size_t Engine::request_bytes(const JobSpec& spec) const {
+  const std::uint64_t px = std::uint64_t(spec.settings.width) * std::uint64_t(spec.settings.height);
+  const std::uint32_t first = spec.opts.progressive ? 1u : static_cast<std::uint32_t>(spec.settings.spp);
+  return static_cast<std::size_t>(px * (64 + 4) + 32 + px * first * sizeof(float4));
+}
+
+int Engine::submit(const JobSpec& spec) {
+  CK(cudaSetDevice(device_));
+  const int h = open_job(spec, true, nullptr);
+  serve_open_++;
+  return h;
+}
+
+void Engine::pump(double budget_ms, bool return_on_event, std::vector<PassEvent>& events) {
+  CK(cudaSetDevice(device_));
+  if (!wave_) return;
+  drain(nullptr, &events, budget_ms, return_on_event);
+}
+
+void Engine::cancel_request(int request) {
+  auto it = jobs_.find(request);
+  if (it == jobs_.end() || !it->second.serving) throw std::invalid_argument("unknown request " + std::to_string(request));
+  Job& j = it->second;
+  if (j.cancelled || j.prog.finished) return;
+  j.cancelled = true;
+  j.prog.cancelled = true;
+  for (int slot : j.segs) {
+    Seg& s = segs_[slot];
+    if (s.complete) continue;
+    s.abandoned = true;
+    s.closed_at = wave_->it;  // the next plan no longer lists it
+  }
+  gen_dirty_ = true;
+  retire_segments(j, nullptr);
+}
+
+void Engine::release_request(int request) {
+  auto it = jobs_.find(request);
+  if (it == jobs_.end() || !it->second.serving) throw std::invalid_argument("unknown request " + std::to_string(request));
+  Job& j = it->second;
+  if (!j.drained()) throw std::logic_error("request " + std::to_string(request) + " is still rendering");
+  free_frame(j.frame);
+  close_job(j);
+  jobs_.erase(it);
+  serve_open_--;
+}
+
+std::size_t Engine::requests_rendering() const {
+  std::size_t n = 0;
+  for (const auto& kv : jobs_)
+    if (kv.second.serving && !kv.second.drained()) ++n;
+  return n;
+}
+
+const GpuFrame& Engine::request_frame(int request) const {
+  auto it = jobs_.find(request);
+  if (it == jobs_.end() || !it->second.serving) throw std::invalid_argument("unknown request " + std::to_string(request));
+  return it->second.frame;
+}
+
+const RenderProgress& Engine::request_progress(int request) const {
+  auto it = jobs_.find(request);
+  if (it == jobs_.end() || !it->second.serving) throw std::invalid_argument("unknown request " + std::to_string(request));
+  return it->second.prog;
+}
+
+// ---- framebuffer reads ----
 const GpuFrame& Engine::frame(int job) const {
   const std::size_t j = job < 0 ? 0 : static_cast<std::size_t>(job);
+  if (!rendering_.empty()) {  // inside a pass callback: the render in progress
+    if (j >= rendering_.size()) throw std::invalid_argument("no framebuffer for job " + std::to_string(job));
+    return jobs_.at(rendering_[j]).frame;
+  }
   if (j >= frames_.size()) throw std::invalid_argument("no framebuffer for job " + std::to_string(job));
   return frames_[j];
 }
 
-void Engine::read_mean(int job, double* rgb) const {
-  const GpuFrame& f = frame(job);
-  const std::uint64_t px = std::uint64_t(f.width) * f.height;
-  double* tmp = dev_alloc<double>(px * 3);
-  // The resolve kernel reads the framebuffer through a descriptor.
-  RtgSceneDev d{};
-  d.width = f.width;
-  d.height = f.height;
-  d.fb_sum = f.sum;
-  d.fb_sumsq = f.sumsq;
-  d.fb_count = f.count;
-  RtgSceneDev* dd = dev_alloc<RtgSceneDev>(1);
-  CK(cudaMemcpyAsync(dd, &d, sizeof(d), cudaMemcpyHostToDevice, stream_));
-  CK(launch_resolve(dd, px, 0, 1.0, nullptr, tmp, stream_));
-  CK(cudaMemcpyAsync(rgb, tmp, px * 3 * sizeof(double), cudaMemcpyDeviceToHost, stream_));
-  CK(cudaStreamSynchronize(stream_));
-  dev_free(tmp);
-  dev_free(dd);
-}
+void Engine::read_mean(int job, double* rgb) const { read_mean_frame(frame(job), rgb); }
 
 void Engine::read_moments(int job, double* sum, double* sumsq, std::uint32_t* count) const {
   const GpuFrame& f = frame(job);
@@ -513,24 +875,28 @@ void Engine::read_moments(int job, double* sum, double* sumsq, std::uint32_t* co
 }
 
 void Engine::read_image(int job, ToneMap op, double exposure, std::uint8_t* rgb) const {
-  const GpuFrame& f = frame(job);
-  const std::uint64_t px = std::uint64_t(f.width) * f.height;
-  std::uint8_t* tmp = dev_alloc<std::uint8_t>(px * 3);
-  RtgSceneDev d{};
-  d.width = f.width;
-  d.height = f.height;
-  d.fb_sum = f.sum;
-  d.fb_sumsq = f.sumsq;
-  d.fb_count = f.count;
-  RtgSceneDev* dd = dev_alloc<RtgSceneDev>(1);
-  CK(cudaMemcpyAsync(dd, &d, sizeof(d), cudaMemcpyHostToDevice, stream_));
-  CK(launch_resolve(dd, px, static_cast<int>(op), exposure, tmp, nullptr, stream_));
-  CK(cudaMemcpyAsync(rgb, tmp, px * 3, cudaMemcpyDeviceToHost, stream_));
-  CK(cudaStreamSynchronize(stream_));
-  dev_free(tmp);
-  dev_free(dd);
+  read_image_frame(frame(job), op, exposure, rgb);
 }
 
+void Engine::read_mean_frame(const GpuFrame& f, double* rgb) const {
+  const std::uint64_t px = std::uint64_t(f.width) * f.height;
+  double* tmp = dev_alloc_async<double>(px * 3, stream_);
+  CK(launch_resolve(f.sum, f.count, px, 0, 1.0, nullptr, tmp, stream_));
+  CK(cudaMemcpyAsync(rgb, tmp, px * 3 * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+  CK(cudaFreeAsync(tmp, stream_));
+  CK(cudaStreamSynchronize(stream_));
+}
+
+void Engine::read_image_frame(const GpuFrame& f, ToneMap op, double exposure, std::uint8_t* rgb) const {
+  const std::uint64_t px = std::uint64_t(f.width) * f.height;
+  std::uint8_t* tmp = dev_alloc_async<std::uint8_t>(px * 3, stream_);
+  CK(launch_resolve(f.sum, f.count, px, static_cast<int>(op), exposure, tmp, nullptr, stream_));
+  CK(cudaMemcpyAsync(rgb, tmp, px * 3, cudaMemcpyDeviceToHost, stream_));
+  CK(cudaFreeAsync(tmp, stream_));
+  CK(cudaStreamSynchronize(stream_));
+}
+
+// ---------------------------------------------------------------------------
 void Engine::trace_closest(int scene_id, const float* rays, std::uint64_t n, bool brute, float* t, std::int32_t* prim,
                            std::int32_t* is_plane, float* bary) {
   CK(cudaSetDevice(device_));

@@ -1,16 +1,28 @@
 #pragma once
-// GPU render engine: resident scenes, the wavefront path pool, framebuffers and
-// the progressive pass loop.
+// GPU render engine: resident scenes, the continuous wavefront, framebuffers and
+// the progressive pass schedule.
+//
+// Every render is a job; every pass of a job is a segment. Segments of any number
+// of jobs share one persistent pool of path slots: the host appends segments (and
+// jobs) between iterations and the device hands free slots to them in priority
+// order, so the pool stays full across pass boundaries, between the jobs of a
+// batch and between requests that arrive while others render. A job's finished
+// segments are folded into its framebuffer strictly in pass order, so results are
+// bit-identical whatever else shares the wavefront.
 //
 // The pass schedule, progress record and callback contract are the reference
 // Renderer's (src/rendering/renderer.cpp:58-105, include/raytracer/rendering/renderer.hpp:25-56):
 // pass sizes min(remaining, max(1, done), max_pass_spp) => 1, 1, 2, 4, 8, ...;
-// the callback runs on the calling thread between passes with no kernel of this
-// render in flight; cancellation is checked between wavefront iterations and a
-// cancelled pass is dropped whole, so every pixel keeps the same sample count.
+// the callback runs on the calling thread after each pass, when the framebuffer
+// holds exactly the passes reported so far (later passes may be tracing, but they
+// touch only their own radiance slots); cancellation is checked between
+// wavefront iterations and unfinished passes are dropped whole, so every pixel
+// keeps the same sample count.
 #include <chrono>
 #include <cstdint>
+#include <deque>
 #include <functional>
+#include <map>
 #include <memory>
 #include <string>
 #include <unordered_map>
@@ -48,7 +60,7 @@ struct RenderStats {
   double elapsed_ms = 0;
   double device_ms = 0;  // CUDA events on the engine stream around the whole render
   // Summed CUDA-event time of each kernel family (when kernel timing is on).
-  double extend_ms = 0, shade_ms = 0, shadow_ms = 0, accumulate_ms = 0, direct_ms = 0;
+  double extend_ms = 0, shade_ms = 0, shadow_ms = 0, accumulate_ms = 0, direct_ms = 0, plan_ms = 0;
   std::uint64_t extend_launches = 0;
 };
 
@@ -68,26 +80,36 @@ struct GpuScene {
   double* prims64 = nullptr;   // ray-query refinement geometry (lazily uploaded)
   double* planes64 = nullptr;
   std::size_t device_bytes = 0;
+  int jobs_open = 0;           // jobs in the wavefront that use this scene
 };
 
-// Per-render device framebuffer.
+// Per-job device framebuffer.
 struct GpuFrame {
   int width = 0, height = 0;
   double* sum = nullptr;
   double* sumsq = nullptr;
   std::uint32_t* count = nullptr;
   std::uint64_t* stats = nullptr;
-  std::size_t bytes() const { return std::size_t(width) * height * (64 + 4) + 8; }
+  std::size_t bytes() const { return std::size_t(width) * height * (64 + 4) + 32; }
 };
 
 using PassCallback = std::function<void(const RenderProgress&)>;
 
 struct EngineConfig {
-  std::uint32_t pool_paths = 1u << 20;     // wavefront path slots
-  std::uint64_t max_pass_samples = 1ull << 27;  // radiance slots per pass
+  std::uint32_t pool_paths = 1u << 20;          // wavefront path slots (<= 2^23)
+  std::uint64_t max_pass_samples = 1ull << 27;  // radiance slots shared by the open segments
+  std::uint32_t backlog_pools = 3;              // keep this many pools of samples open for generation
   LaunchShape shape;
-  bool time_kernels = false;               // CUDA events around every launch
-  bool count_traversal = false;            // node / primitive counters
+  bool time_kernels = false;                    // CUDA events around every launch
+  bool count_traversal = false;                 // node / primitive counters
+};
+
+// A render request for the scheduler.
+struct JobSpec {
+  int scene_id = 0;
+  RenderSettings settings;
+  RenderOptions opts;
+  int priority = 0;  // lower is served first (previews before finals)
 };
 
 class Engine {
@@ -99,6 +121,7 @@ class Engine {
 
   int device() const { return device_; }
   // Frees the wavefront pool so the next render allocates it with the current config.
+  // Requires an idle wavefront.
   void reset_wave();
   cudaStream_t stream() const { return stream_; }
   EngineConfig& config() { return cfg_; }
@@ -108,25 +131,49 @@ class Engine {
   GpuScene& scene(int id);
   bool has_scene(int id) const { return scenes_.count(id) != 0; }
 
-  // Plain renderer: one scene per launch sequence.
+  // Plain renderer: one job; its passes overlap in the wavefront.
   RenderProgress render(int scene_id, const RenderSettings& settings, const RenderOptions& opts,
                         const PassCallback& on_pass, const volatile std::int32_t* cancel);
 
-  // Batched renderer: every job's passes share one persistent wavefront; pass p of
-  // all jobs that still need samples runs as one pass.
+  // Batched renderer: every job's passes share the wavefront.
   struct BatchJob {
     int scene_id;
     RenderSettings settings;
   };
   std::vector<RenderProgress> render_batch(const std::vector<BatchJob>& jobs, const RenderOptions& opts,
-                                           const volatile std::int32_t* cancel);
+                                           const volatile std::int32_t* cancel, const PassCallback& on_pass = {});
 
   // Results of the last render (plain) or of job `j` of the last batch.
   const GpuFrame& frame(int job = -1) const;
   void read_mean(int job, double* rgb) const;
   void read_moments(int job, double* sum, double* sumsq, std::uint32_t* count) const;
   void read_image(int job, ToneMap op, double exposure, std::uint8_t* rgb) const;
+  void read_mean_frame(const GpuFrame& f, double* rgb) const;
+  void read_image_frame(const GpuFrame& f, ToneMap op, double exposure, std::uint8_t* rgb) const;
   const RenderStats& stats() const { return stats_; }
+
+  // ---- serving: requests live in the wavefront across calls ----
+  // Opens a request; it starts tracing on the next pump. Returns its handle (> 0).
+  int submit(const JobSpec& spec);
+  struct PassEvent {
+    int request;
+    RenderProgress progress;
+  };
+  // Runs wavefront iterations until `budget_ms` of host time has passed, an event
+  // is ready and `return_on_event` is set, or no request has work left. Appends
+  // the pass events (in completion order) to `events`.
+  void pump(double budget_ms, bool return_on_event, std::vector<PassEvent>& events);
+  void cancel_request(int request);
+  // Frees a finished or cancelled request's framebuffer.
+  void release_request(int request);
+  bool request_exists(int request) const { return jobs_.count(request) != 0; }
+  const GpuFrame& request_frame(int request) const;
+  const RenderProgress& request_progress(int request) const;
+  // Footprint a request adds on the device (framebuffer + radiance of one pass).
+  std::size_t request_bytes(const JobSpec& spec) const;
+  std::size_t open_requests() const { return serve_open_; }
+  std::size_t requests_rendering() const;
+  bool wave_idle() const { return jobs_.empty() || all_jobs_drained(); }
 
   // Ray queries against one scene: rays = n x 8 floats (o, tmin, d, tmax).
   void trace_closest(int scene_id, const float* rays, std::uint64_t n, bool brute, float* t, std::int32_t* prim,
@@ -137,14 +184,63 @@ class Engine {
 
  private:
   struct Wave;
-  void ensure_wave(std::uint64_t pass_samples);
+  struct Job {
+    int handle = 0;
+    int desc_slot = -1;
+    int scene_id = 0;
+    RenderSettings settings;
+    RenderOptions opts;
+    int priority = 0;
+    std::uint64_t seq = 0;          // submission order
+    GpuFrame frame;
+    std::uint64_t pixels = 0;
+    std::uint32_t target = 0, issued = 0, done = 0;
+    int passes_issued = 0;
+    RenderProgress prog;
+    std::deque<int> segs;           // issued segment slots, pass order
+    bool cancelled = false;
+    bool direct = false;
+    bool serving = false;           // owned by the serving API (else by a render call)
+    PassCallback on_pass;
+    std::chrono::steady_clock::time_point t0;
+    bool drained() const { return segs.empty() && (cancelled || done >= target); }
+  };
+  struct Seg {
+    bool used = false;
+    int job = 0;                    // job handle
+    DevSegment d{};
+    std::uint64_t rad_begin = 0;
+    bool in_gen = false;
+    bool complete = false;
+    bool abandoned = false;         // its job was cancelled: drop the result
+    std::uint64_t done = 0, generated = 0;  // last snapshot
+    std::uint64_t assigned_at = 0;  // first iteration whose plan sees the slot's records
+    std::uint64_t closed_at = 0;    // first iteration whose plan no longer lists it (cancelled)
+  };
+
+  void ensure_wave();
   GpuFrame make_frame(int w, int h);
   void free_frame(GpuFrame& f);
   RtgSceneDev job_descriptor(const GpuScene& sc, const RenderSettings& s, const GpuFrame& f) const;
-  // Runs one pass over the jobs in `table_host` (already staged); returns false if cancelled.
-  bool run_pass(std::vector<RtgSceneDev>& jobs, const std::vector<std::uint32_t>& ids, std::uint64_t total,
-                bool direct, const volatile std::int32_t* cancel);
 
+  // Scheduler.
+  int open_job(const JobSpec& spec, bool serving, PassCallback cb);
+  void close_job(Job& j);
+  bool all_jobs_drained() const;
+  std::uint32_t next_pass_size(const Job& j) const;
+  bool issue_pass(Job& j);          // false if no radiance space or slot is free now
+  void refill();
+  bool run_direct_pass(Job& j);     // false if no radiance space is free now
+  void process_snapshot(std::uint64_t iter, std::vector<PassEvent>* events);
+  void retire_segments(Job& j, std::vector<PassEvent>* events);
+  void launch_one_iteration();
+  void drain(const volatile std::int32_t* cancel, std::vector<PassEvent>* events, double budget_ms,
+             bool return_on_event);
+  void abort_all();                 // drop every open segment (after a cancel) and reset the pool
+  void stage(void* dst, const void* src, std::size_t n);
+  void write_gen_table();
+  void begin_stats();
+  void end_stats();
   void finish_timing();  // records the end event and fills stats_.device_ms
 
   int device_;
@@ -155,7 +251,17 @@ class Engine {
   int next_scene_ = 1;
   std::unique_ptr<Wave> wave_;
   std::vector<GpuFrame> frames_;  // frames of the last render / batch
+  std::vector<int> rendering_;    // handles of the render / batch in progress (pass callbacks read these)
+  std::vector<RenderSettings> frame_settings_;
   RenderStats stats_;
+  std::map<int, Job> jobs_;        // open jobs by handle
+  std::vector<Seg> segs_;          // by segment slot
+  int next_job_ = 1;
+  std::uint64_t job_seq_ = 0;
+  std::size_t serve_open_ = 0;
+  bool gen_dirty_ = false;
+  WaveCounters last_counters_{};   // from the latest snapshot
+  WaveCounters base_counters_{};   // at the start of the current render
 };
 
 }  // namespace rtg

@@ -77,7 +77,7 @@ class _Stats(C.Structure):
         "iterations", "node_visits", "prim_tests", "sphere_tests", "extend_launches", "shadow_node_visits",
         "shadow_prim_tests", "shadow_sphere_tests", "kernel_launches")] + [
         (n, C.c_double) for n in ("elapsed_ms", "device_ms", "extend_ms", "shade_ms", "shadow_ms", "accumulate_ms",
-                                  "direct_ms")]
+                                  "direct_ms", "plan_ms")]
 
 
 class _SceneInfo(C.Structure):
@@ -102,8 +102,13 @@ class _Tuning(C.Structure):
     _fields_ = [
         ("pool_paths", C.c_uint32), ("block", C.c_uint32), ("max_pass_samples", C.c_uint64),
         ("extend_blocks", C.c_int32), ("shade_blocks", C.c_int32), ("shadow_blocks", C.c_int32),
-        ("time_kernels", C.c_int32), ("count_traversal", C.c_int32),
+        ("time_kernels", C.c_int32), ("count_traversal", C.c_int32), ("backlog_pools", C.c_uint32),
+        ("reserved", C.c_uint32), ("serve_budget_bytes", C.c_uint64), ("serve_reserve_bytes", C.c_uint64),
     ]
+
+
+class _RequestEvent(C.Structure):
+    _fields_ = [("request", C.c_int32), ("reserved", C.c_int32), ("progress", _Progress)]
 
 
 PASS_FN = C.CFUNCTYPE(None, C.c_void_p, C.POINTER(_Progress))
@@ -144,6 +149,17 @@ _SIGNATURES = {
                                             C.POINTER(C.c_float)]),
     "rtg_get_tuning": (C.c_int, [C.c_void_p, C.POINTER(_Tuning)]),
     "rtg_set_tuning": (C.c_int, [C.c_void_p, C.POINTER(_Tuning)]),
+    "rtg_request_submit": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(_Settings), C.POINTER(_Options), C.c_int32,
+                                     C.POINTER(C.c_int32)]),
+    "rtg_serve_pump": (C.c_int, [C.c_void_p, C.c_double, C.c_int32, C.POINTER(_RequestEvent), C.c_int32,
+                                 C.POINTER(C.c_int32)]),
+    "rtg_request_cancel": (C.c_int, [C.c_void_p, C.c_int32]),
+    "rtg_request_release": (C.c_int, [C.c_void_p, C.c_int32]),
+    "rtg_request_progress": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(_Progress)]),
+    "rtg_request_mean": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double)]),
+    "rtg_request_image_rgb8": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_double, C.POINTER(C.c_uint8)]),
+    "rtg_serve_footprint": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_int32),
+                                      C.POINTER(C.c_int32)]),
     "rtg_encode_png": (C.c_int64, [C.POINTER(C.c_uint8), C.c_int32, C.c_int32, C.POINTER(C.c_uint8), C.c_size_t]),
 }
 
@@ -475,6 +491,57 @@ class Context:
         occ = np.zeros(n, np.uint8)
         self._check(lib().rtg_trace_any(self._h, scene_id, _ptr(rays, C.c_float), n, int(brute), _ptr(occ, C.c_uint8)))
         return occ
+
+    # serving
+    def submit(self, scene_id: int, settings: Optional[RenderSettings] = None,
+               options: Optional[RenderOptions] = None, priority: int = 0) -> Optional[int]:
+        """Opens a request; None when admission by footprint turns it away."""
+        s = settings.to_c() if settings else None
+        o = _Options(int(options.progressive), options.max_pass_spp) if options else None
+        rid = C.c_int32()
+        rc = lib().rtg_request_submit(self._h, scene_id, C.byref(s) if s else None, C.byref(o) if o else None,
+                                      priority, C.byref(rid))
+        if rc == RTG_ERR_LIMIT:
+            return None
+        self._check(rc)
+        return rid.value
+
+    def pump(self, budget_ms: float, return_on_event: bool = False, cap: int = 256) -> list[tuple[int, RenderProgress]]:
+        ev = (_RequestEvent * cap)()
+        n = C.c_int32()
+        self._check(lib().rtg_serve_pump(self._h, budget_ms, int(return_on_event), ev, cap, C.byref(n)))
+        return [(ev[k].request, RenderProgress.from_c(ev[k].progress)) for k in range(n.value)]
+
+    def cancel_request(self, rid: int):
+        self._check(lib().rtg_request_cancel(self._h, rid))
+
+    def release_request(self, rid: int):
+        self._check(lib().rtg_request_release(self._h, rid))
+
+    def request_progress(self, rid: int) -> RenderProgress:
+        p = _Progress()
+        self._check(lib().rtg_request_progress(self._h, rid, C.byref(p)))
+        return RenderProgress.from_c(p)
+
+    def request_mean(self, rid: int, width: int, height: int) -> np.ndarray:
+        out = np.zeros((height, width, 3), dtype=np.float64)
+        self._check(lib().rtg_request_mean(self._h, rid, _ptr(out, C.c_double)))
+        return out
+
+    def request_image(self, rid: int, width: int, height: int, tone_map: Optional[str] = None,
+                      exposure: float = 1.0) -> np.ndarray:
+        out = np.zeros((height, width, 3), dtype=np.uint8)
+        op = -1 if tone_map is None else TONE_MAPS[tone_map]
+        self._check(lib().rtg_request_image_rgb8(self._h, rid, op, exposure, _ptr(out, C.c_uint8)))
+        return out
+
+    def serve_footprint(self) -> tuple[int, int, int]:
+        """(device bytes held against the admission budget, open requests, requests still rendering)."""
+        b = C.c_uint64()
+        n = C.c_int32()
+        r = C.c_int32()
+        self._check(lib().rtg_serve_footprint(self._h, C.byref(b), C.byref(n), C.byref(r)))
+        return b.value, n.value, r.value
 
 
 class Renderer:

@@ -14,6 +14,8 @@ GOLDEN = os.path.join(ROOT, "tests", "golden")
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200); runs the sm_100a kernels through the C ABI")
+    # An assertion inside a ctypes callback is otherwise swallowed; make it fail the test.
+    config.addinivalue_line("filterwarnings", "error::pytest.PytestUnraisableExceptionWarning")
 
 
 @pytest.fixture(scope="session")
