@@ -49,6 +49,7 @@ def args():
     p.add_argument("--serve-seconds", type=float, default=10.0,
                    help="length of the serving run (Poisson arrivals over 32 resident scenes of the mix)")
     p.add_argument("--no-serve", action="store_true", help="skip the serving run")
+    p.add_argument("--no-autotune", action="store_true", help="keep the default pool and block size")
     return p.parse_args()
 
 
@@ -253,6 +254,9 @@ def run_rtg(a, dist, scenes, desc):
     settings = [ctx.scene_settings(i) for i in sids]
     scene_bytes = sum(ctx.scene_info(i)["device_bytes"] for i in sids)
     batched = len(sids) > 1
+    tuned = None
+    if not a.no_autotune:
+        tuned = ctx.autotune(sids, settings, opts, use_cache=True)
 
     def step():
         if batched:
@@ -369,7 +373,8 @@ def run_rtg(a, dist, scenes, desc):
             "config": {"workload": desc, "scenes": len(scenes), "samples_per_step": samples_of(scenes),
                        "primitives": int(sum(len(h.view()["prims"]) for h in hosts)) if len(hosts) <= 64 else None,
                        "progressive": not a.single_pass, "max_pass_spp": 32,
-                       "pool_paths": ctx.tuning()["pool_paths"],
+                       "pool_paths": ctx.tuning()["pool_paths"], "block": ctx.tuning()["block"],
+                       "autotune": tuned,
                        "mode": ("batched: every scene's passes in one continuous wavefront" if batched
                                 else "plain: one scene, its passes overlapping in the wavefront"),
                        "parallelism": f"replicas x{dist.world}",

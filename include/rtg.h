@@ -230,12 +230,20 @@ typedef struct rtg_tuning {
   int32_t time_kernels;      /* CUDA events around each kernel (rtg_stats.*_ms) */
   int32_t count_traversal;   /* node / primitive counters (rtg_stats.node_visits, prim_tests) */
   uint32_t backlog_pools;    /* samples kept open for generation, in pools (default 3) */
-  uint32_t reserved;
+  uint32_t chained;          /* programmatic dependent launch between wavefront kernels (default 1) */
   uint64_t serve_budget_bytes; /* admission limit of the open requests' device footprint */
   uint64_t serve_reserve_bytes; /* part of that budget only priority-0 requests (previews) may use */
 } rtg_tuning;
 int rtg_get_tuning(rtg_context* ctx, rtg_tuning* out);
 int rtg_set_tuning(rtg_context* ctx, const rtg_tuning* in);
+/* Picks pool_paths and block for a batch of renders (settings = NULL: each
+ * scene's own) by timing a reduced copy of it (1/16 of the samples) under each
+ * candidate, and applies the winner. Cached per GPU and workload signature in
+ * $RTG_TUNE_CACHE (default $HOME/.cache/rtg/tuning.txt) when use_cache is set.
+ * chosen, msamples_per_s and from_cache may be NULL. */
+int rtg_autotune(rtg_context* ctx, int32_t n, const rtg_scene_id* scenes, const rtg_settings* settings,
+                 const rtg_render_options* opts, int32_t use_cache, rtg_tuning* chosen, double* msamples_per_s,
+                 int32_t* from_cache);
 
 /* ---- serving (no reference counterpart: the reference renders one scene per
  * Renderer). Requests on resident scenes share one continuous wavefront with each

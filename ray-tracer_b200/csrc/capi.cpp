@@ -17,6 +17,7 @@
 #include <string>
 
 #include "device/noalloc.h"
+#include "host/autotune.hpp"
 #include "host/engine.hpp"
 #include "host/scene_io.hpp"
 
@@ -580,6 +581,7 @@ int rtg_get_tuning(rtg_context* ctx, rtg_tuning* out) {
     out->time_kernels = c.time_kernels ? 1 : 0;
     out->count_traversal = c.count_traversal ? 1 : 0;
     out->backlog_pools = c.backlog_pools;
+    out->chained = c.shape.chained ? 1 : 0;
     out->serve_budget_bytes = ctx->serve_budget;
     out->serve_reserve_bytes = ctx->serve_reserve;
     return RTG_OK;
@@ -609,10 +611,44 @@ int rtg_set_tuning(rtg_context* ctx, const rtg_tuning* in) {
     c.time_kernels = in->time_kernels != 0;
     c.count_traversal = in->count_traversal != 0;
     c.backlog_pools = in->backlog_pools;
+    c.shape.chained = in->chained != 0;
     if (in->serve_budget_bytes) ctx->serve_budget = in->serve_budget_bytes;
     if (in->serve_reserve_bytes > ctx->serve_budget) throw std::invalid_argument("serve_reserve_bytes exceeds the budget");
     ctx->serve_reserve = in->serve_reserve_bytes;
     if (realloc) ctx->engine->reset_wave();
+    return RTG_OK;
+  });
+}
+
+int rtg_autotune(rtg_context* ctx, int32_t n, const rtg_scene_id* scenes, const rtg_settings* settings,
+                 const rtg_render_options* opts, int32_t use_cache, rtg_tuning* chosen, double* msamples_per_s,
+                 int32_t* from_cache) {
+  return guarded(ctx, [&]() {
+    if (ctx->busy) return RTG_ERR_BUSY;
+    if (n <= 0 || n > 65535 || !scenes) throw std::invalid_argument("autotune needs 1..65535 jobs");
+    if (ctx->engine->open_requests() > 0) {
+      ctx->error = "rtg_autotune: serving requests are open on this context";
+      return RTG_ERR_BUSY;
+    }
+    std::vector<rtg::Engine::BatchJob> jobs;
+    for (int32_t j = 0; j < n; ++j) {
+      if (settings)
+        if (const char* bad = settings_problem(settings[j])) throw rtg::SceneError(bad);
+      const rtg::RenderSettings s = settings ? from_c(settings[j]) : ctx->engine->scene(scenes[j]).host.settings;
+      if (const char* bad = settings_problem(s)) throw rtg::SceneError(bad);
+      jobs.push_back({scenes[j], s});
+    }
+    rtg::RenderOptions o;
+    if (opts) {
+      o.progressive = opts->progressive != 0;
+      o.max_pass_spp = opts->max_pass_spp;
+    }
+    BusyGuard guard(ctx);
+    const rtg::AutotuneResult r = rtg::autotune(*ctx->engine, jobs, o, use_cache != 0);
+    if (msamples_per_s) *msamples_per_s = r.msamples_per_s;
+    if (from_cache) *from_cache = r.from_cache ? 1 : 0;
+    ctx->last_settings.clear();  // the probe renders replaced the last frames
+    if (chosen) return rtg_get_tuning(ctx, chosen);
     return RTG_OK;
   });
 }

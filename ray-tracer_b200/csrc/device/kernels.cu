@@ -60,6 +60,14 @@ __device__ __forceinline__ void warp_add_u64(std::uint64_t v, std::uint64_t* dst
   if ((threadIdx.x & 31) == 0 && v) atomicAdd(reinterpret_cast<unsigned long long*>(dst), static_cast<unsigned long long>(v));
 }
 
+// Programmatic dependent launch: each wavefront kernel lets the next one be
+// scheduled at once (its blocks take SM slots as this grid's blocks exit) and
+// waits for the previous grid's completion and memory before touching any data.
+__device__ __forceinline__ void chain_to_previous_grid() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // Warp-wide fetch of the next 32 work items from `cursor`.
 __device__ __forceinline__ std::uint32_t warp_fetch(std::uint32_t* cursor) {
   std::uint32_t base = 0;
@@ -102,6 +110,7 @@ __device__ __forceinline__ CameraSample camera_sample(const RtgSceneDev& J, cons
 __global__ void __launch_bounds__(kMaxGen) k_plan(WaveBuffers wb, int par) {
   __shared__ std::uint32_t scan[kMaxGen];
   __shared__ std::uint32_t fscan[kMaxGen];
+  chain_to_previous_grid();
   WaveCounters* C = wb.cnt;
   const int t = threadIdx.x;
   const std::uint32_t live = C->live[par];
@@ -174,6 +183,7 @@ __global__ void __launch_bounds__(kMaxGen) k_plan(WaveBuffers wb, int par) {
 template <int kBlock, bool kCount>
 __global__ void __launch_bounds__(kBlock) k_extend(WaveBuffers wb, int par) {
   __shared__ int stack[kStackSmem * kBlock];
+  chain_to_previous_grid();
   WaveCounters* C = wb.cnt;
   const std::uint32_t live = C->live[par];
   const std::uint32_t n = C->n_extend;
@@ -236,6 +246,7 @@ __global__ void __launch_bounds__(kBlock) k_extend(WaveBuffers wb, int par) {
 // ---------------------------------------------------------------------------
 template <int kBlock>
 __global__ void __launch_bounds__(kBlock) k_shade(WaveBuffers wb, int par) {
+  chain_to_previous_grid();
   WaveCounters* C = wb.cnt;
   const std::uint32_t n = C->n_extend;
   const float4* const A = wb.st_a[par];
@@ -355,6 +366,7 @@ __global__ void __launch_bounds__(kBlock) k_shade(WaveBuffers wb, int par) {
 template <int kBlock, bool kCount>
 __global__ void __launch_bounds__(kBlock) k_shadow(WaveBuffers wb) {
   __shared__ int stack[kStackSmem * kBlock];
+  chain_to_previous_grid();
   WaveCounters* C = wb.cnt;
   const std::uint32_t n = C->n_shadow;
   TraceCount tc;
@@ -612,33 +624,48 @@ const BlockCounts& block_counts() {
   return bc;
 }
 
+// Launch with programmatic stream serialization (when enabled) so the kernel's
+// blocks are scheduled while the previous wavefront kernel drains.
+template <class... KArgs, class... Args>
+cudaError_t launch_chained(void (*kernel)(KArgs...), int grid, int block, bool pdl, cudaStream_t stream,
+                           Args... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(static_cast<unsigned>(grid));
+  cfg.blockDim = dim3(static_cast<unsigned>(block));
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 template <int kBlock>
 cudaError_t stage_impl(Stage stage, const WaveBuffers& wb, int par, const LaunchShape& shape, bool count,
                        cudaStream_t stream) {
   const BlockCounts& bc = block_counts<kBlock>();
+  const bool pdl = shape.chained;
   switch (stage) {
     case Stage::Plan:
-      k_plan<<<1, kMaxGen, 0, stream>>>(wb, par);
-      break;
+      return launch_chained(k_plan, 1, kMaxGen, pdl, stream, wb, par);
     case Stage::Extend: {
       const int blocks = shape.extend_blocks ? shape.extend_blocks : (count ? bc.extend_counting : bc.extend);
-      if (count) k_extend<kBlock, true><<<blocks, kBlock, 0, stream>>>(wb, par);
-      else k_extend<kBlock, false><<<blocks, kBlock, 0, stream>>>(wb, par);
-      break;
+      return count ? launch_chained(k_extend<kBlock, true>, blocks, kBlock, pdl, stream, wb, par)
+                   : launch_chained(k_extend<kBlock, false>, blocks, kBlock, pdl, stream, wb, par);
     }
     case Stage::Shade: {
       const int blocks = shape.shade_blocks ? shape.shade_blocks : bc.shade;
-      k_shade<kBlock><<<blocks, kBlock, 0, stream>>>(wb, par);
-      break;
+      return launch_chained(k_shade<kBlock>, blocks, kBlock, pdl, stream, wb, par);
     }
     case Stage::Shadow: {
       const int blocks = shape.shadow_blocks ? shape.shadow_blocks : (count ? bc.shadow_counting : bc.shadow);
-      if (count) k_shadow<kBlock, true><<<blocks, kBlock, 0, stream>>>(wb);
-      else k_shadow<kBlock, false><<<blocks, kBlock, 0, stream>>>(wb);
-      break;
+      return count ? launch_chained(k_shadow<kBlock, true>, blocks, kBlock, pdl, stream, wb)
+                   : launch_chained(k_shadow<kBlock, false>, blocks, kBlock, pdl, stream, wb);
     }
   }
-  return cudaGetLastError();
+  return cudaErrorInvalidValue;
 }
 
 }  // namespace

@@ -35,6 +35,7 @@ struct WaveBuffers {
 struct LaunchShape {
   int extend_blocks = 0, shade_blocks = 0, shadow_blocks = 0;  // 0 = derived from the SM count
   int extend_block = 128;  // 64, 128 or 256
+  bool chained = true;     // programmatic dependent launch between the wavefront kernels
 };
 
 enum class Stage { Plan, Extend, Shade, Shadow };

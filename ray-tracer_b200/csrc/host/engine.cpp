@@ -24,11 +24,12 @@ T* dev_alloc(std::size_t n) {
   return static_cast<T*>(p);
 }
 
-// Stream-ordered allocation: never synchronises with kernels in flight.
+// Stream-ordered allocation from the engine's own pool: never synchronises with
+// kernels in flight, and freed blocks stay mapped for reuse.
 template <class T>
-T* dev_alloc_async(std::size_t n, cudaStream_t s) {
+T* dev_alloc_async(std::size_t n, cudaMemPool_t pool, cudaStream_t s) {
   void* p = nullptr;
-  CK(cudaMallocAsync(&p, std::max<std::size_t>(n, 1) * sizeof(T), s));
+  CK(cudaMallocFromPoolAsync(&p, std::max<std::size_t>(n, 1) * sizeof(T), pool, s));
   return static_cast<T*>(p);
 }
 
@@ -82,6 +83,7 @@ struct Engine::Wave {
   std::uint64_t stall = 0;             // snapshots without a finished sample while work is open
   std::uint64_t last_done_sum = 0;
 
+  std::uint64_t rad_in_free = 0;       // radiance slots in rad_free
   bool rad_alloc(std::uint64_t n, std::uint64_t& at) {
     for (auto itr = rad_free.begin(); itr != rad_free.end(); ++itr) {
       if (itr->second < n) continue;
@@ -89,11 +91,13 @@ struct Engine::Wave {
       const std::uint64_t rest = itr->second - n;
       rad_free.erase(itr);
       if (rest) rad_free.emplace(at + n, rest);
+      rad_in_free -= n;
       return true;
     }
     return false;
   }
   void rad_release(std::uint64_t at, std::uint64_t n) {
+    rad_in_free += n;
     auto nx = rad_free.lower_bound(at);
     if (nx != rad_free.end() && at + n == nx->first) {
       n += nx->second;
@@ -115,6 +119,14 @@ Engine::Engine(int device) : device_(device) {
   CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
   CK(cudaEventCreate(&ev_begin_));
   CK(cudaEventCreate(&ev_end_));
+  cudaMemPoolProps props{};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = device;
+  CK(cudaMemPoolCreate(&pool_, &props));
+  // Keep freed framebuffers mapped: requests come and go at hundreds per second.
+  std::uint64_t keep = ~0ull;
+  CK(cudaMemPoolSetAttribute(pool_, cudaMemPoolAttrReleaseThreshold, &keep));
 }
 
 void Engine::finish_timing() {
@@ -137,6 +149,7 @@ Engine::~Engine() {
   cudaEventDestroy(ev_begin_);
   cudaEventDestroy(ev_end_);
   cudaStreamDestroy(stream_);
+  cudaMemPoolDestroy(pool_);
 }
 
 void Engine::reset_wave() {
@@ -219,6 +232,7 @@ void Engine::ensure_wave() {
   W.rad_cap = std::max<std::uint64_t>(1, std::min<std::uint64_t>(cfg_.max_pass_samples, 0xFFFFFFFFull));
   b.radiance = dev_alloc<float4>(W.rad_cap);
   W.rad_free.emplace(0, W.rad_cap);
+  W.rad_in_free = W.rad_cap;
   b.cnt = dev_alloc<WaveCounters>(1);
   W.jobs_dev = dev_alloc<RtgSceneDev>(kJobSlots);
   W.segs_dev = dev_alloc<DevSegment>(kMaxSegments);
@@ -253,10 +267,10 @@ GpuFrame Engine::make_frame(int w, int h) {
   f.width = w;
   f.height = h;
   const std::size_t px = std::size_t(w) * std::size_t(h);
-  f.sum = dev_alloc_async<double>(px * 4, stream_);
-  f.sumsq = dev_alloc_async<double>(px * 4, stream_);
-  f.count = dev_alloc_async<std::uint32_t>(px, stream_);
-  f.stats = dev_alloc_async<std::uint64_t>(4, stream_);
+  f.sum = dev_alloc_async<double>(px * 4, pool_, stream_);
+  f.sumsq = dev_alloc_async<double>(px * 4, pool_, stream_);
+  f.count = dev_alloc_async<std::uint32_t>(px, pool_, stream_);
+  f.stats = dev_alloc_async<std::uint64_t>(4, pool_, stream_);
   CK(cudaMemsetAsync(f.sum, 0, px * 4 * sizeof(double), stream_));
   CK(cudaMemsetAsync(f.sumsq, 0, px * 4 * sizeof(double), stream_));
   CK(cudaMemsetAsync(f.count, 0, px * sizeof(std::uint32_t), stream_));
@@ -412,6 +426,8 @@ bool Engine::issue_pass(Job& j) {
   const std::uint32_t k = next_pass_size(j);
   const std::uint64_t count = j.pixels * k;
   if (W.free_segs.empty()) return false;
+  // Lower-priority work leaves an eighth of the radiance slots to priority 0.
+  if (j.priority > 0 && W.rad_in_free < count + W.rad_cap / 8) return false;
   std::uint64_t at = 0;
   if (!W.rad_alloc(count, at)) return false;
   const int slot = W.free_segs.back();
@@ -507,10 +523,12 @@ void Engine::refill() {
       if (run_direct_pass(*best) && best->on_pass) best->on_pass(best->prog);
       return;
     }
+    // Enough samples are open ahead of this job: wait. A priority-0 job (a plain
+    // or batched render, a preview) gets its first pass at once regardless.
     std::uint64_t ahead = 0;
     for (const auto& kv : backlog)
       if (kv.first <= best->priority) ahead += kv.second;
-    if (ahead >= target && !best->segs.empty()) return;
+    if (ahead >= target && !(best->priority == 0 && best->segs.empty())) return;
     const std::uint64_t before = best->issued;
     if (!issue_pass(*best)) return;
     backlog[best->priority] += best->pixels * (best->issued - before);
@@ -622,11 +640,11 @@ void Engine::launch_one_iteration() {
     if (timed) CK(cudaEventRecord(W.tev[2 * k], stream_));
     CK(launch_stage(stages[k], W.wb, par, cfg_.shape, count, stream_));
     if (timed) CK(cudaEventRecord(W.tev[2 * k + 1], stream_));
-    if (k == 0) {
-      CK(cudaEventRecord(W.plan_ev[r], stream_));
-      W.plan_recorded[r] = true;
-    }
   }
+  // After the whole iteration, so no event sits between chained kernels; the
+  // plan's snapshot and this slot's staged copies are complete once it fires.
+  CK(cudaEventRecord(W.plan_ev[r], stream_));
+  W.plan_recorded[r] = true;
   if (timed) {
     CK(cudaEventSynchronize(W.tev[7]));
     float ms[4] = {0, 0, 0, 0};
@@ -675,6 +693,7 @@ void Engine::abort_all() {
     }
   W.rad_free.clear();
   W.rad_free.emplace(0, W.rad_cap);
+  W.rad_in_free = W.rad_cap;
   for (auto& kv : jobs_) kv.second.segs.clear();
   W.seen = W.it;
   W.stall = 0;
@@ -880,7 +899,7 @@ void Engine::read_image(int job, ToneMap op, double exposure, std::uint8_t* rgb)
 
 void Engine::read_mean_frame(const GpuFrame& f, double* rgb) const {
   const std::uint64_t px = std::uint64_t(f.width) * f.height;
-  double* tmp = dev_alloc_async<double>(px * 3, stream_);
+  double* tmp = dev_alloc_async<double>(px * 3, pool_, stream_);
   CK(launch_resolve(f.sum, f.count, px, 0, 1.0, nullptr, tmp, stream_));
   CK(cudaMemcpyAsync(rgb, tmp, px * 3 * sizeof(double), cudaMemcpyDeviceToHost, stream_));
   CK(cudaFreeAsync(tmp, stream_));
@@ -889,7 +908,7 @@ void Engine::read_mean_frame(const GpuFrame& f, double* rgb) const {
 
 void Engine::read_image_frame(const GpuFrame& f, ToneMap op, double exposure, std::uint8_t* rgb) const {
   const std::uint64_t px = std::uint64_t(f.width) * f.height;
-  std::uint8_t* tmp = dev_alloc_async<std::uint8_t>(px * 3, stream_);
+  std::uint8_t* tmp = dev_alloc_async<std::uint8_t>(px * 3, pool_, stream_);
   CK(launch_resolve(f.sum, f.count, px, static_cast<int>(op), exposure, tmp, nullptr, stream_));
   CK(cudaMemcpyAsync(rgb, tmp, px * 3, cudaMemcpyDeviceToHost, stream_));
   CK(cudaFreeAsync(tmp, stream_));

@@ -245,6 +245,7 @@ class Engine {
 
   int device_;
   cudaStream_t stream_ = nullptr;
+  cudaMemPool_t pool_ = nullptr;  // framebuffers and read-back staging
   cudaEvent_t ev_begin_ = nullptr, ev_end_ = nullptr;
   EngineConfig cfg_;
   std::unordered_map<int, std::unique_ptr<GpuScene>> scenes_;

@@ -103,7 +103,7 @@ class _Tuning(C.Structure):
         ("pool_paths", C.c_uint32), ("block", C.c_uint32), ("max_pass_samples", C.c_uint64),
         ("extend_blocks", C.c_int32), ("shade_blocks", C.c_int32), ("shadow_blocks", C.c_int32),
         ("time_kernels", C.c_int32), ("count_traversal", C.c_int32), ("backlog_pools", C.c_uint32),
-        ("reserved", C.c_uint32), ("serve_budget_bytes", C.c_uint64), ("serve_reserve_bytes", C.c_uint64),
+        ("chained", C.c_uint32), ("serve_budget_bytes", C.c_uint64), ("serve_reserve_bytes", C.c_uint64),
     ]
 
 
@@ -160,6 +160,8 @@ _SIGNATURES = {
     "rtg_request_image_rgb8": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_double, C.POINTER(C.c_uint8)]),
     "rtg_serve_footprint": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_int32),
                                       C.POINTER(C.c_int32)]),
+    "rtg_autotune": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(_Settings), C.POINTER(_Options),
+                               C.c_int32, C.POINTER(_Tuning), C.POINTER(C.c_double), C.POINTER(C.c_int32)]),
     "rtg_encode_png": (C.c_int64, [C.POINTER(C.c_uint8), C.c_int32, C.c_int32, C.POINTER(C.c_uint8), C.c_size_t]),
 }
 
@@ -491,6 +493,21 @@ class Context:
         occ = np.zeros(n, np.uint8)
         self._check(lib().rtg_trace_any(self._h, scene_id, _ptr(rays, C.c_float), n, int(brute), _ptr(occ, C.c_uint8)))
         return occ
+
+    def autotune(self, scene_ids: list[int], settings: Optional[list[RenderSettings]] = None,
+                 options: Optional[RenderOptions] = None, use_cache: bool = True) -> dict:
+        """Picks pool size and block size for this batch and applies them."""
+        n = len(scene_ids)
+        ids = (C.c_int32 * n)(*scene_ids)
+        ss = (_Settings * n)(*[s.to_c() for s in settings]) if settings else None
+        o = _Options(int(options.progressive), options.max_pass_spp) if options else None
+        t = _Tuning()
+        rate = C.c_double()
+        cached = C.c_int32()
+        self._check(lib().rtg_autotune(self._h, n, ids, ss, C.byref(o) if o else None, int(use_cache), C.byref(t),
+                                       C.byref(rate), C.byref(cached)))
+        return {"pool_paths": t.pool_paths, "block": t.block, "probe_msamples_per_s": rate.value,
+                "from_cache": bool(cached.value)}
 
     # serving
     def submit(self, scene_id: int, settings: Optional[RenderSettings] = None,

@@ -39,6 +39,7 @@ class Request:
     arrival: float                 # seconds after the loop starts
     rid: Optional[int] = None
     submitted: Optional[float] = None
+    first_event: Optional[float] = None
     first_pass: Optional[float] = None
     finished: Optional[float] = None
     spp_done: int = 0
@@ -75,17 +76,29 @@ def serve(ctx: rtg.Context, scene_ids, seconds: float = 10.0, rate: float = 200.
     settings = {}
     rejected = 0
     t0 = time.perf_counter()
+    calls = collections.defaultdict(lambda: [0, 0.0, 0.0, 0])  # name -> [count, total s, max s, over 20 ms]
 
     def now():
         return time.perf_counter() - t0
+
+    def timed(name, fn, *args, **kw):
+        c0 = time.perf_counter()
+        out = fn(*args, **kw)
+        dt = time.perf_counter() - c0
+        rec = calls[name]
+        rec[0] += 1
+        rec[1] += dt
+        rec[2] = max(rec[2], dt)
+        rec[3] += dt > 0.02
+        return out
 
     def admit(q) -> bool:
         """Submits the head of q; False when the footprint budget turns it away."""
         r = q[0]
         st = settings.get((r.scene, r.kind.name)) or settings_for(ctx, r)
         settings[(r.scene, r.kind.name)] = st
-        rid = ctx.submit(r.scene, st, rtg.RenderOptions(progressive=r.kind.progressive, max_pass_spp=32),
-                         r.kind.priority)
+        rid = timed("submit", ctx.submit, r.scene, st,
+                    rtg.RenderOptions(progressive=r.kind.progressive, max_pass_spp=32), r.kind.priority)
         if rid is None:
             return False
         r.rid, r.submitted = rid, now()
@@ -116,18 +129,19 @@ def serve(ctx: rtg.Context, scene_ids, seconds: float = 10.0, rate: float = 200.
             if pending:
                 time.sleep(max(0.0, min(pending[0].arrival - now(), 0.002)))
             continue
-        for rid, p in ctx.pump(2.0, return_on_event=True):
+        for rid, p in timed("pump", ctx.pump, 2.0, return_on_event=True):
             r = live.get(rid)
             if r is None:
                 continue
             r.spp_done = p.spp_done
             if r.first_pass is None:
+                r.first_event = now()
                 if read_images:
-                    ctx.request_image(rid, r.kind.width, r.kind.height)
+                    timed("image", ctx.request_image, rid, r.kind.width, r.kind.height)
                 r.first_pass = now()
             if p.finished:
                 r.finished = now()
-                ctx.release_request(rid)
+                timed("release", ctx.release_request, rid)
                 del live[rid]
     window = now()
     # Stop what is still rendering (finals that outlast the window).
@@ -146,13 +160,20 @@ def serve(ctx: rtg.Context, scene_ids, seconds: float = 10.0, rate: float = 200.
 
     out = {"seconds": window, "arrival_rate_per_s": rate, "requests": len(reqs), "admission_retries": rejected,
            "msamples_per_s": sum(r.samples for r in reqs) / window / 1e6,
+           "host_calls": {k: {"count": v[0], "total_ms": v[1] * 1e3, "max_ms": v[2] * 1e3, "over_20ms": v[3]}
+                          for k, v in calls.items()},
            "policy": "previews priority 0 (may use the reserve), finals priority 1; finals still waiting for "
                      "footprint at the end of the arrival window are not admitted; finals still rendering are "
                      "cancelled after the last preview"}
     for kind in (PREVIEW, FINAL):
         rs = [r for r in reqs if r.kind is kind]
         ttfp = [r.first_pass - r.arrival for r in rs if r.first_pass is not None]
+        served = [r for r in rs if r.first_pass is not None]
+        phases = {"queue": [r.submitted - r.arrival for r in served],
+                  "trace": [r.first_event - r.submitted for r in served],
+                  "read": [r.first_pass - r.first_event for r in served]}
         out[kind.name] = {
+            "phase_ms_p50_p99": {k: [pct(v, 50), pct(v, 99)] for k, v in phases.items()},
             "count": len(rs), "admitted": sum(1 for r in rs if r.rid is not None), "first_pass_on_host": len(ttfp),
             "finished": sum(1 for r in rs if r.finished is not None),
             "ttfp_ms_p50": pct(ttfp, 50), "ttfp_ms_p99": pct(ttfp, 99), "ttfp_ms_max": pct(ttfp, 100),
