@@ -50,6 +50,8 @@ def args():
                    help="length of the serving run (Poisson arrivals over 32 resident scenes of the mix)")
     p.add_argument("--no-serve", action="store_true", help="skip the serving run")
     p.add_argument("--no-autotune", action="store_true", help="keep the default pool and block size")
+    p.add_argument("--pool", type=int, default=0, help="path slots (implies --no-autotune)")
+    p.add_argument("--block", type=int, default=0, help="threads per block: 64, 128, 256 (implies --no-autotune)")
     return p.parse_args()
 
 
@@ -255,7 +257,9 @@ def run_rtg(a, dist, scenes, desc):
     scene_bytes = sum(ctx.scene_info(i)["device_bytes"] for i in sids)
     batched = len(sids) > 1
     tuned = None
-    if not a.no_autotune:
+    if a.pool or a.block:
+        ctx.set_tuning(**({"pool_paths": a.pool} if a.pool else {}), **({"block": a.block} if a.block else {}))
+    elif not a.no_autotune:
         tuned = ctx.autotune(sids, settings, opts, use_cache=True)
 
     def step():

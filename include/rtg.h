@@ -280,6 +280,10 @@ int rtg_request_progress(rtg_context* ctx, rtg_request_id request, rtg_progress*
  * image (tone_map < 0: the request's own settings, as rtg_image_rgb8). */
 int rtg_request_mean(rtg_context* ctx, rtg_request_id request, double* rgb);
 int rtg_request_image_rgb8(rtg_context* ctx, rtg_request_id request, int32_t tone_map, double exposure, uint8_t* rgb);
+/* Maps the admission budget's worth of device memory into the context's pool
+ * (rtg_request_submit does it on first use otherwise): a server calls it once at
+ * start-up so no request's first allocation waits for the driver. */
+int rtg_serve_prepare(rtg_context* ctx);
 /* Device bytes the open requests hold against the admission budget, the number
  * of open requests, and how many of them still have passes to render or in flight. */
 int rtg_serve_footprint(rtg_context* ctx, uint64_t* bytes, int32_t* open_requests, int32_t* rendering);

@@ -677,6 +677,9 @@ int rtg_request_submit(rtg_context* ctx, rtg_scene_id scene, const rtg_settings*
                    std::to_string(priority) + ")";
       return RTG_ERR_LIMIT;
     }
+    // Map the whole admission budget into the pool before the first request, so
+    // later framebuffer allocations are suballocations and never stall on the driver.
+    ctx->engine->reserve_pool(static_cast<std::size_t>(ctx->serve_budget));
     const int h = ctx->engine->submit(spec);
     ctx->footprint[h] = bytes;
     ctx->serve_used += bytes;
@@ -773,6 +776,13 @@ int rtg_request_image_rgb8(rtg_context* ctx, rtg_request_id request, int32_t ton
       op = static_cast<rtg::ToneMap>(tone_map);
     }
     ctx->engine->read_image_frame(f, op, ex, rgb);
+    return RTG_OK;
+  });
+}
+
+int rtg_serve_prepare(rtg_context* ctx) {
+  return guarded(ctx, [&]() {
+    ctx->engine->reserve_pool(static_cast<std::size_t>(ctx->serve_budget));
     return RTG_OK;
   });
 }

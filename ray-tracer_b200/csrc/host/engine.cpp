@@ -852,6 +852,16 @@ void Engine::release_request(int request) {
   serve_open_--;
 }
 
+void Engine::reserve_pool(std::size_t bytes) {
+  if (bytes <= pool_reserved_) return;
+  CK(cudaSetDevice(device_));
+  void* p = nullptr;
+  CK(cudaMallocFromPoolAsync(&p, bytes, pool_, stream_));
+  CK(cudaFreeAsync(p, stream_));
+  CK(cudaStreamSynchronize(stream_));
+  pool_reserved_ = bytes;
+}
+
 std::size_t Engine::requests_rendering() const {
   std::size_t n = 0;
   for (const auto& kv : jobs_)

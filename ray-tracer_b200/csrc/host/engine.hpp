@@ -172,6 +172,9 @@ class Engine {
   // Footprint a request adds on the device (framebuffer + radiance of one pass).
   std::size_t request_bytes(const JobSpec& spec) const;
   std::size_t open_requests() const { return serve_open_; }
+  // Maps `bytes` of device memory into the engine's pool ahead of time, so
+  // framebuffer allocations of arriving requests never wait for the driver.
+  void reserve_pool(std::size_t bytes);
   std::size_t requests_rendering() const;
   bool wave_idle() const { return jobs_.empty() || all_jobs_drained(); }
 
@@ -246,6 +249,7 @@ class Engine {
   int device_;
   cudaStream_t stream_ = nullptr;
   cudaMemPool_t pool_ = nullptr;  // framebuffers and read-back staging
+  std::size_t pool_reserved_ = 0;
   cudaEvent_t ev_begin_ = nullptr, ev_end_ = nullptr;
   EngineConfig cfg_;
   std::unordered_map<int, std::unique_ptr<GpuScene>> scenes_;

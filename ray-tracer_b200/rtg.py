@@ -25,7 +25,7 @@ from typing import Callable, Optional
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "librtg.so")
+LIB_PATH = os.environ.get("RTG_LIBRARY") or os.path.join(_HERE, "librtg.so")  # override: another build
 
 RTG_OK = 0
 RTG_ERR_INVALID = -1
@@ -158,6 +158,7 @@ _SIGNATURES = {
     "rtg_request_progress": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(_Progress)]),
     "rtg_request_mean": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double)]),
     "rtg_request_image_rgb8": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_double, C.POINTER(C.c_uint8)]),
+    "rtg_serve_prepare": (C.c_int, [C.c_void_p]),
     "rtg_serve_footprint": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_int32),
                                       C.POINTER(C.c_int32)]),
     "rtg_autotune": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(_Settings), C.POINTER(_Options),
@@ -551,6 +552,10 @@ class Context:
         op = -1 if tone_map is None else TONE_MAPS[tone_map]
         self._check(lib().rtg_request_image_rgb8(self._h, rid, op, exposure, _ptr(out, C.c_uint8)))
         return out
+
+    def serve_prepare(self):
+        """Maps the admission budget into the device pool up front."""
+        self._check(lib().rtg_serve_prepare(self._h))
 
     def serve_footprint(self) -> tuple[int, int, int]:
         """(device bytes held against the admission budget, open requests, requests still rendering)."""

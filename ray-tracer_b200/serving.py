@@ -70,6 +70,7 @@ def serve(ctx: rtg.Context, scene_ids, seconds: float = 10.0, rate: float = 200.
     served, then cancels what is still rendering. Returns latency percentiles and
     throughput."""
     reqs = poisson_arrivals(scene_ids, seconds, rate, preview_share, seed)
+    ctx.serve_prepare()  # start-up, outside the timed loop
     pending = collections.deque(reqs)
     waiting = {PREVIEW.name: collections.deque(), FINAL.name: collections.deque()}
     live = {}
