@@ -245,6 +245,20 @@ def peaks():
     return 6650.0, "fallback 6.65 TB/s"
 
 
+def extend_traffic(pool_paths: int, rays_per_launch: float):
+    """DRAM bytes per k_extend launch from the committed ncu capture of the mix
+    (profiles/k_extend_mix_dram.json, taken with a full pool), scaled to this run's
+    rays per launch; None when no capture matches this pool size."""
+    p = os.path.join(ROOT, "profiles", "k_extend_mix_dram.json")
+    if not os.path.exists(p):
+        return None, None
+    d = json.load(open(p))
+    if int(d.get("pool_paths", 0)) != int(pool_paths):
+        return None, None
+    per_ray = d["dram_bytes_per_launch"] / d["rays_per_launch"]
+    return per_ray * rays_per_launch, f"ncu capture, {d['launches_captured']} launches ({os.path.basename(p)})"
+
+
 def run_rtg(a, dist, scenes, desc):
     import rtg
 
@@ -297,17 +311,25 @@ def run_rtg(a, dist, scenes, desc):
     dist.barrier()
     t0 = time.perf_counter()
     e2e_samples = 0
+    phase = {"upload_s": 0.0, "render_s": 0.0, "images_s": 0.0, "release_s": 0.0}
     for _ in range(max(1, a.steps)):
+        c0 = time.perf_counter()
         ids = [ctx.upload(h) for h in hosts]
+        c1 = time.perf_counter()
         if batched:
             ctx.render_batch(ids, settings, opts)
         else:
             ctx.render(ids[0], settings[0], opts)
         e2e_samples += ctx.stats()["camera_samples"]
+        c2 = time.perf_counter()
         for j, s in enumerate(settings):
             ctx.image(j if batched else -1, s.width, s.height)
+        c3 = time.perf_counter()
         for i in ids:
             ctx.release(i)
+        c4 = time.perf_counter()
+        for k, dt in zip(phase, (c1 - c0, c2 - c1, c3 - c2, c4 - c3)):
+            phase[k] += dt / max(1, a.steps)
     e2e_s = dist.max(time.perf_counter() - t0)
     e2e_value = dist.sum(e2e_samples) / e2e_s / 1e6
     sids = [ctx.upload(h) for h in hosts]
@@ -342,11 +364,12 @@ def run_rtg(a, dist, scenes, desc):
     avg_ms = t_st["extend_ms"] / launches_ext
     achieved = ext_bytes / launches_ext / (avg_ms / 1e3) / 1e9
     peak, peak_src = peaks()
+    traffic, traffic_src = extend_traffic(ctx.tuning()["pool_paths"], c_st["rays"] / launches_ext)
     kernel_total = t_st["extend_ms"] + t_st["shade_ms"] + t_st["shadow_ms"] + t_st["accumulate_ms"] + t_st["plan_ms"]
     roofline = {
         "kernel": "k_extend (closest-hit BVH traversal + camera-path generation)",
         "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-        "traffic": None, "peak_source": peak_src,
+        "traffic": traffic, "traffic_source": traffic_src, "peak_source": peak_src,
         "bytes_per_launch": ext_bytes / launches_ext, "avg_launch_ms": avg_ms, "launches": launches_ext,
         "share_of_kernel_time": t_st["extend_ms"] / kernel_total if kernel_total else None,
         "per_ray": {"nodes": c_st["node_visits"] / max(1, c_st["rays"]),
@@ -385,7 +408,7 @@ def run_rtg(a, dist, scenes, desc):
                        "l2": f"inputs larger than L2: {scene_bytes / 2**20:.0f} MiB of scenes + GBs of per-pass "
                              "radiance and path state rewritten every step (L2 126 MiB)"},
             "e2e": {"value": e2e_value, "unit": "Msamples/s", "h2d_bytes_per_step": scene_bytes,
-                    "d2h_bytes_per_step": d2h},
+                    "d2h_bytes_per_step": d2h, "phases_per_step": phase},
             "gpu_launches": launches,
             "clocks": clk,
             "roofline": roofline,

@@ -4,9 +4,12 @@
 // Semantics follow the reference's Scene::intersect / intersect_brute / occluded
 // (src/core/scene.cpp:152-234) and Bvh::closest / Bvh::any
 // (include/raytracer/geometry/bvh.hpp:75-132): planes are tested linearly first and
-// shrink t_max; the BVH is walked depth first, nearer child first by the sign of
-// the ray direction on the parent's split axis; a primitive is accepted only if
+// shrink t_max; the BVH is walked depth first; a primitive is accepted only if
 // t_min < t < t_max (strict), so among equal distances the first tested wins.
+// The closest-hit walk visits the child whose box the ray enters first (the
+// reference orders by the sign of the direction on the split axis); that visits
+// fewer nodes, and only changes which of two primitives at exactly the same
+// distance is reported.
 //
 // Traversal stack: the top kStackSmem entries of each thread's stack live in
 // shared memory (laid out [entry][thread] so a warp's pushes hit 32 distinct
@@ -49,8 +52,9 @@ struct SlabRay {
 };
 
 // Both children's slab tests from one node; returns entry distances.
+// `second_first` (when given) is set when child 1's box is entered before child 0's.
 __device__ __forceinline__ void node_boxes(const DevNode* __restrict__ node, const SlabRay& r, float tmin, float tmax,
-                                           bool& hit0, bool& hit1, int4& link) {
+                                           bool& hit0, bool& hit1, int4& link, bool* second_first = nullptr) {
   const float4 a = __ldg(&node->xy0);
   const float4 b = __ldg(&node->xy1);
   const float4 c = __ldg(&node->zz);
@@ -67,6 +71,7 @@ __device__ __forceinline__ void node_boxes(const DevNode* __restrict__ node, con
   const float b_out = fminf(fminf(fmaxf(bx0, bx1), fmaxf(by0, by1)), fminf(fmaxf(bz0, bz1), tmax));
   hit0 = a_in <= a_out;
   hit1 = b_in <= b_out;
+  if (second_first) *second_first = b_in < a_in;
 }
 
 // Möller-Trumbore, two-sided (include/raytracer/geometry/shapes.hpp:110-127).
@@ -187,12 +192,10 @@ __device__ __forceinline__ RayHit closest_hit(const RtgSceneDev& sc, float3 o, f
   while (true) {
     if (cur >= 0) {
       if (kCount) cnt.nodes++;
-      bool h0, h1;
+      bool h0, h1, right_first;
       int4 link;
-      node_boxes(sc.nodes + cur, sr, tmin, best.t, h0, h1, link);
+      node_boxes(sc.nodes + cur, sr, tmin, best.t, h0, h1, link, &right_first);
       if (h0 && h1) {
-        const int axis = (link.z >> 16) & 3;
-        const bool right_first = sr.neg[axis];
         st.push(right_first ? link.x : link.y);
         cur = right_first ? link.y : link.x;
         continue;

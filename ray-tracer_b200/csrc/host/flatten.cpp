@@ -1,8 +1,11 @@
 #include "host/flatten.hpp"
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <limits>
 #include <stdexcept>
+#include <thread>
 
 namespace rtg {
 
@@ -19,20 +22,51 @@ float float_of(std::uint32_t u) {
   return f;
 }
 
+// One float step toward -inf / +inf (std::nextafterf for finite f, by bits).
+float step_down(float f) {
+  if (f == 0.f) return -std::numeric_limits<float>::denorm_min();
+  return float_of(f > 0.f ? bits_of(f) - 1u : bits_of(f) + 1u);
+}
+float step_up(float f) {
+  if (f == 0.f) return std::numeric_limits<float>::denorm_min();
+  return float_of(f > 0.f ? bits_of(f) + 1u : bits_of(f) - 1u);
+}
+
 // Round a double down / up to the nearest float, then widen by a few float ulps
 // so the fp32 slab test (whose FMA form rounds once per plane) never culls a box
 // that a primitive inside it would have been hit in.
 float down(double v) {
   float f = static_cast<float>(v);
-  if (static_cast<double>(f) > v) f = std::nextafterf(f, -INFINITY);
+  if (static_cast<double>(f) > v) f = step_down(f);
   f -= std::fabs(f) * 0x1p-22f;
-  return std::nextafterf(f, -INFINITY);
+  return step_down(f);
 }
 float up(double v) {
   float f = static_cast<float>(v);
-  if (static_cast<double>(f) < v) f = std::nextafterf(f, INFINITY);
+  if (static_cast<double>(f) < v) f = step_up(f);
   f += std::fabs(f) * 0x1p-22f;
-  return std::nextafterf(f, INFINITY);
+  return step_up(f);
+}
+
+// Runs body(begin, end) over [0, n) in contiguous chunks on up to 16 threads
+// (one chunk inline when n is small). Used for the per-slot and per-node loops,
+// whose iterations write disjoint records.
+template <class F>
+void parallel_chunks(std::size_t n, F&& body) {
+  const std::size_t hw = std::max(1u, std::thread::hardware_concurrency());
+  const std::size_t workers = std::min<std::size_t>({hw, 16, (n + 32767) / 32768});
+  if (workers <= 1) {
+    body(std::size_t(0), n);
+    return;
+  }
+  std::vector<std::thread> pool;
+  const std::size_t chunk = (n + workers - 1) / workers;
+  for (std::size_t w = 1; w < workers; ++w) {
+    const std::size_t b = std::min(n, w * chunk), e = std::min(n, b + chunk);
+    pool.emplace_back([&body, b, e] { body(b, e); });
+  }
+  body(std::size_t(0), std::min(n, chunk));
+  for (auto& t : pool) t.join();
 }
 
 float4 f4(D3 v, float w = 0.f) { return make_float4(float(v.x), float(v.y), float(v.z), w); }
@@ -67,16 +101,17 @@ FlatScene flatten(const CompiledScene& s) {
 
   // Primitive slots in leaf order; mark the last slot of every leaf.
   const std::size_t nslots = bvh.order.size();
-  std::vector<bool> last(nslots, false);
+  if (s.prims.size() > kIdMask) throw std::runtime_error("too many primitives for the device layout");
+  std::vector<std::uint8_t> last(nslots, 0);
   for (const BinaryNode& n : bvh.nodes)
-    if (n.leaf()) last[n.first + n.count - 1] = true;
+    if (n.leaf()) last[n.first + n.count - 1] = 1;
   f.prims.resize(nslots * 3);
   f.slot_material.resize(nslots);
   f.slot_normals.resize(nslots * 3, make_float4(0.f, 0.f, 0.f, 0.f));
   f.slot_prim.resize(nslots);
-  for (std::size_t k = 0; k < nslots; ++k) {
+  parallel_chunks(nslots, [&](std::size_t k0, std::size_t k1) {
+  for (std::size_t k = k0; k < k1; ++k) {
     const std::uint32_t id = bvh.order[k];
-    if (id > kIdMask) throw std::runtime_error("too many primitives for the device layout");
     const Prim& p = s.prims[id];
     std::uint32_t word = id | (last[k] ? kLastInLeaf : 0u);
     if (p.kind == Prim::kSphere) {
@@ -97,6 +132,7 @@ FlatScene flatten(const CompiledScene& s) {
     f.slot_material[k] = p.material | ((p.kind == Prim::kTriangle && p.smooth) ? 0x80000000u : 0u);
     f.slot_prim[k] = id;
   }
+  });
 
   // Interior nodes in depth-first order -> DevNode indices.
   std::vector<std::int32_t> dev_index(bvh.nodes.size(), -1);
@@ -108,7 +144,8 @@ FlatScene flatten(const CompiledScene& s) {
     return c.leaf() ? ~static_cast<std::int32_t>(c.first) : dev_index[child];
   };
   f.nodes.resize(static_cast<std::size_t>(ninterior));
-  for (std::size_t i = 0; i < bvh.nodes.size(); ++i) {
+  parallel_chunks(bvh.nodes.size(), [&](std::size_t i0, std::size_t i1) {
+  for (std::size_t i = i0; i < i1; ++i) {
     const BinaryNode& n = bvh.nodes[i];
     if (n.leaf()) continue;
     const Box& L = bvh.nodes[i + 1].box;
@@ -119,6 +156,7 @@ FlatScene flatten(const CompiledScene& s) {
     d.zz = make_float4(down(L.lo.z), up(L.hi.z), down(R.lo.z), up(R.hi.z));
     d.link = make_int4(link_of(i + 1), link_of(n.first), static_cast<int>(n.axis) << 16, 0);
   }
+  });
   if (!bvh.nodes.empty()) f.root = link_of(0);
 
   for (const PlanePrim& pl : s.planes) {
