@@ -246,18 +246,21 @@ __global__ void __launch_bounds__(kBlock) k_extend(WaveBuffers wb, int par) {
 // ---------------------------------------------------------------------------
 template <int kBlock>
 __global__ void __launch_bounds__(kBlock) k_shade(WaveBuffers wb, int par) {
+  constexpr int kWarps = kBlock / 32;
+  __shared__ std::uint32_t s_cnt[2][kWarps];
+  __shared__ std::uint32_t s_base[2];
   chain_to_previous_grid();
   WaveCounters* C = wb.cnt;
   const std::uint32_t n = C->n_extend;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const float4* const A = wb.st_a[par];
   const float4* const B = wb.st_b[par];
   const float4* const Cc = wb.st_c[par];
   const uint4* const D = wb.st_d[par];
   std::uint64_t rr_killed = 0;
-  while (true) {
-    const std::uint32_t base = warp_fetch(&C->fetch[1]);
-    if (base >= n) break;
-    const std::uint32_t i = base + (threadIdx.x & 31);
+  // Uniform work per path: blocks stride over the hits in order (no fetch atomics).
+  for (std::uint32_t base = blockIdx.x * kBlock; base < n; base += gridDim.x * kBlock) {
+    const std::uint32_t i = base + threadIdx.x;
     bool cont = false, shadow = false;
     float3 o_next = f3(0.f, 0.f, 0.f), d_next = o_next, beta = o_next, sh_o = o_next, sh_d = o_next, sh_c = o_next;
     float sh_tmax = 0.f;
@@ -304,10 +307,10 @@ __global__ void __launch_bounds__(kBlock) k_shade(WaveBuffers wb, int par) {
         if (scatter(m, d, s, rng, sr)) {
           if (J.light_sampling && !sr.specular && J.n_lights > 0) {
             const std::uint32_t nl = static_cast<std::uint32_t>(J.n_lights);
-            const DevLight L = J.lights[rng.below(nl)];
-            const LightSample ls = sample_light(L, s, rng);
+            const LightSample ls = sample_light(J.lights + rng.below(nl), s, rng);
             if (ls.valid) {
-              const float3 f = brdf_cos(m, s, ls.wi);
+              // Only a Lambertian scatter is non-specular: its weight is the albedo.
+              const float3 f = lambert_cos(sr.weight, s, ls.wi);
               if (!is_zero3(f) && !is_zero3(ls.li_over_pdf)) {
                 const ShadowRay sray = shadow_ray(s, ls);
                 sh_o = sray.o;
@@ -338,8 +341,27 @@ __global__ void __launch_bounds__(kBlock) k_shade(WaveBuffers wb, int par) {
         }
       }
     }
-    const std::uint32_t cpos = warp_append(cont, &C->live[par ^ 1]);
-    const std::uint32_t spos = warp_append(shadow, &C->n_shadow);
+    // Appends aggregated per block: one atomic per queue per 256 paths.
+    const unsigned mc = __ballot_sync(kFull, cont), ms = __ballot_sync(kFull, shadow);
+    if (lane == 0) {
+      s_cnt[0][warp] = __popc(mc);
+      s_cnt[1][warp] = __popc(ms);
+    }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+      std::uint32_t total = 0;
+      for (int w = 0; w < kWarps; ++w) {
+        const std::uint32_t c = s_cnt[threadIdx.x][w];
+        s_cnt[threadIdx.x][w] = total;
+        total += c;
+      }
+      s_base[threadIdx.x] = total ? atomicAdd(threadIdx.x == 0 ? &C->live[par ^ 1] : &C->n_shadow, total) : 0u;
+    }
+    __syncthreads();
+    const unsigned below = (1u << lane) - 1u;
+    const std::uint32_t cpos = s_base[0] + s_cnt[0][warp] + __popc(mc & below);
+    const std::uint32_t spos = s_base[1] + s_cnt[1][warp] + __popc(ms & below);
+    __syncthreads();  // s_cnt / s_base are rewritten next round
     // A path that ends here is done once this iteration's shadow stage has run:
     // count it in its segment (one atomic per segment present in the warp).
     const bool fin = i < n && !cont;
@@ -413,7 +435,7 @@ __device__ __forceinline__ float3 direct_light_all(const RtgSceneDev& J, const D
                                                    Pcg& rng, int* stack, TraceCount& tc, std::uint64_t& shadow_rays) {
   float3 sum = f3(0.f, 0.f, 0.f);
   for (int li = 0; li < J.n_lights; ++li) {
-    const LightSample ls = sample_light(J.lights[li], s, rng);
+    const LightSample ls = sample_light(J.lights + li, s, rng);
     if (!ls.valid) continue;
     const float3 f = brdf_cos(m, s, ls.wi);
     if (is_zero3(f) || is_zero3(ls.li_over_pdf)) continue;

@@ -151,6 +151,14 @@ __device__ __forceinline__ float3 brdf_cos(const DevMaterial& m, const Surface& 
   return albedo_at(m, s.p) * (c * kInvPiF);
 }
 
+// brdf_cos for a Lambertian surface of albedo `albedo` (the only non-specular
+// scatter), from the scatter weight instead of the material record.
+__device__ __forceinline__ float3 lambert_cos(float3 albedo, const Surface& s, float3 wi) {
+  const float c = dot3(s.n, wi);
+  if (c <= 0.f || dot3(s.gn, wi) <= 0.f) return f3(0.f, 0.f, 0.f);
+  return albedo * (c * kInvPiF);
+}
+
 struct LightSample {
   float3 wi;
   float dist;
@@ -178,27 +186,30 @@ __device__ __forceinline__ ShadowRay shadow_ray(const Surface& s, const LightSam
   return r;
 }
 
-// One sample of one light as seen from s.p (no shadow test).
-__device__ __forceinline__ LightSample sample_light(const DevLight& L, const Surface& s, Pcg& rng) {
+// One sample of one light as seen from s.p (no shadow test). The record's
+// fields are read only for the light's kind, which keeps registers free.
+__device__ __forceinline__ LightSample sample_light(const DevLight* __restrict__ Lp, const Surface& s, Pcg& rng) {
   LightSample out{};
   out.valid = false;
-  const std::uint32_t kind = __float_as_uint(L.q0.w);
+  const float4 q0 = __ldg(&Lp->q0);
+  const std::uint32_t kind = __float_as_uint(q0.w);
   const float3 p = s.p;
   if (kind == kLightPoint) {
-    const float3 dv = f3(L.q0) - p;
+    const float3 dv = f3(q0) - p;
     const float d2 = dot3(dv, dv);
     if (d2 < 1e-16f) return out;
     out.dist = sqrtf(d2);
     out.wi = dv * (1.f / out.dist);
-    out.li_over_pdf = f3(L.q1) * (1.f / d2);
+    out.li_over_pdf = f3(__ldg(&Lp->q1)) * (1.f / d2);
     out.valid = true;
     return out;
   }
   if (kind == kLightSphere) {
-    const float3 c = f3(L.q0);
-    const float r = L.q1.x, r2 = L.q1.y, area = L.q1.z;
-    const bool two_sided = L.q1.w != 0.f;
-    const float3 emit = f3(L.q2);
+    const float4 q1 = __ldg(&Lp->q1);
+    const float3 c = f3(q0);
+    const float r = q1.x, r2 = q1.y, area = q1.z;
+    const bool two_sided = q1.w != 0.f;
+    const float3 emit = f3(__ldg(&Lp->q2));
     const float3 oc = c - p;
     const float d2 = dot3(oc, oc);
     if (d2 <= r2) {
@@ -229,9 +240,10 @@ __device__ __forceinline__ LightSample sample_light(const DevLight& L, const Sur
     return out;
   }
   // Triangle: uniform area sample converted to solid angle.
-  const float3 v0 = f3(L.q0), v1 = f3(L.q1), v2 = f3(L.q2);
-  const float area = L.q1.w;
-  const bool two_sided = L.q2.w != 0.f;
+  const float4 q1 = __ldg(&Lp->q1), q2 = __ldg(&Lp->q2);
+  const float3 v0 = f3(q0), v1 = f3(q1), v2 = f3(q2);
+  const float area = q1.w;
+  const bool two_sided = q2.w != 0.f;
   const float2 b = uniform_triangle(rng);
   const float3 q = (1.f - b.x - b.y) * v0 + b.x * v1 + b.y * v2;
   const float3 dv = q - p;
@@ -239,11 +251,11 @@ __device__ __forceinline__ LightSample sample_light(const DevLight& L, const Sur
   if (d2 < 1e-16f) return out;
   out.dist = sqrtf(d2);
   out.wi = dv * (1.f / out.dist);
-  const float cos_signed = -dot3(f3(L.q3), out.wi);
+  const float cos_signed = -dot3(f3(__ldg(&Lp->q3)), out.wi);
   if (cos_signed <= 0.f && !two_sided) return out;
   const float cos_l = fabsf(cos_signed);
   if (cos_l < 1e-9f) return out;
-  out.li_over_pdf = f3(L.q4) * (cos_l * area / d2);
+  out.li_over_pdf = f3(__ldg(&Lp->q4)) * (cos_l * area / d2);
   out.valid = true;
   return out;
 }
