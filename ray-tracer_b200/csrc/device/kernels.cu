@@ -41,20 +41,6 @@ __device__ __forceinline__ std::uint64_t ld_u64(std::uint32_t lo, std::uint32_t 
   return static_cast<std::uint64_t>(lo) | (static_cast<std::uint64_t>(hi) << 32);
 }
 
-// Appends flagged lanes to a queue with one atomic per warp; returns this lane's
-// position (meaningful only where flag is set). All 32 lanes must call it.
-__device__ __forceinline__ std::uint32_t warp_append(bool flag, std::uint32_t* counter) {
-  const std::uint32_t mask = __ballot_sync(kFull, flag);
-  const int lane = threadIdx.x & 31;
-  std::uint32_t base = 0;
-  if (mask != 0) {
-    const int leader = __ffs(mask) - 1;
-    if (lane == leader) base = atomicAdd(counter, static_cast<std::uint32_t>(__popc(mask)));
-    base = __shfl_sync(kFull, base, leader);
-  }
-  return base + static_cast<std::uint32_t>(__popc(mask & ((1u << lane) - 1u)));
-}
-
 __device__ __forceinline__ void warp_add_u64(std::uint64_t v, std::uint64_t* dst) {
   for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(kFull, v, off);
   if ((threadIdx.x & 31) == 0 && v) atomicAdd(reinterpret_cast<unsigned long long*>(dst), static_cast<unsigned long long>(v));
@@ -401,7 +387,7 @@ __global__ void __launch_bounds__(kBlock) k_shadow(WaveBuffers wb) {
     const float4 a = wb.sh_a[i], b = wb.sh_b[i], c = wb.sh_c[i];
     const RtgSceneDev& J = wb.jobs[__float_as_uint(c.w)];
     const float3 o = f3(a), d = f3(b);
-    const bool blocked = J.use_bvh ? any_hit<kStackSmem, kBlock, kCount>(J, o, d, kRayTMin, b.w, stack, tc)
+    const bool blocked = J.use_bvh ? any_hit4<kStackSmem, kBlock, kCount>(J, o, d, kRayTMin, b.w, stack, tc)
                                    : any_brute(J, o, d, kRayTMin, b.w);
     ++rays;
     if (!blocked) {
@@ -441,7 +427,7 @@ __device__ __forceinline__ float3 direct_light_all(const RtgSceneDev& J, const D
     if (is_zero3(f) || is_zero3(ls.li_over_pdf)) continue;
     const ShadowRay sr = shadow_ray(s, ls);
     ++shadow_rays;
-    const bool blocked = J.use_bvh ? any_hit<kStackSmem, kBlock, false>(J, sr.o, sr.d, kRayTMin, sr.tmax, stack, tc)
+    const bool blocked = J.use_bvh ? any_hit4<kStackSmem, kBlock, false>(J, sr.o, sr.d, kRayTMin, sr.tmax, stack, tc)
                                    : any_brute(J, sr.o, sr.d, kRayTMin, sr.tmax);
     if (!blocked) sum = sum + f * ls.li_over_pdf;
   }
@@ -613,7 +599,7 @@ __global__ void __launch_bounds__(kBlock) k_ray_any(const RtgSceneDev* __restric
   const float4 a = rays[2 * i], b = rays[2 * i + 1];
   TraceCount tc;
   const bool hit = brute ? any_brute(*job, f3(a), f3(b), a.w, b.w)
-                         : any_hit<kStackSmem, kBlock, false>(*job, f3(a), f3(b), a.w, b.w, stack, tc);
+                         : any_hit4<kStackSmem, kBlock, false>(*job, f3(a), f3(b), a.w, b.w, stack, tc);
   out[i] = hit ? 1u : 0u;
 }
 

@@ -29,6 +29,22 @@ struct alignas(16) DevNode {
   int4 link;    // x: child 0 link, y: child 1 link, z: split axis << 16, w: unused
 };
 
+// Four-child BVH node, collapsed from the binary tree (same leaves): the four
+// children's boxes as SoA float4s (component k is child k), then their links with
+// the same meaning as DevNode's; an unused child has kNoChild. One 128-byte node
+// replaces up to three binary nodes. Any-hit (shadow) queries walk this tree: they
+// stop at the first hit, so a wide node's four tests pay off; closest-hit queries
+// walk the binary tree, which measured faster for them.
+struct alignas(16) DevNode4 {
+  float4 lo_x, hi_x, lo_y, hi_y, lo_z, hi_z;
+  int4 link;
+  int4 pad;
+};
+constexpr std::int32_t kNoChild = INT32_MIN;
+// Traversal stack entries a 4-wide walk may need: 3 per level (the binary tree's
+// depth cap of 60 bounds the four-wide depth) plus the current one.
+constexpr int kWideStackDepth = 3 * 61 + 1;
+
 // Primitive slot (leaf order): three float4.
 //  triangle: p0 = (v0, id), p1 = (e1 = v1 - v0, 0), p2 = (e2 = v2 - v0, 0)
 //  sphere:   p0 = (centre, id | kSphereBit), p1 = (radius, radius^2, 0, 0), p2 = 0
@@ -104,6 +120,10 @@ struct alignas(16) RtgSceneDev {
   // (sphere: centre, radius; triangle: v0, v1, v2); per plane 6 (point, normal).
   const double* prims64;
   const double* planes64;
+  // 4-wide copy of the same tree (any-hit queries).
+  const DevNode4* nodes4;
+  std::int32_t root4;         // as root, for nodes4
+  std::int32_t pad1;
 };
 
 // A segment is one pass of one render: samples [pass_s0, pass_s0 + pass_spp) of every

@@ -154,10 +154,10 @@ __device__ __forceinline__ std::uint32_t prim_slot_test(const float4* __restrict
   return id;
 }
 
-template <int kStackSmem, int kBlock>
+template <int kStackSmem, int kBlock, int kDepth = kStackDepth>
 struct TraversalStack {
   int* smem;  // this thread's column: entry k at smem[k * kBlock]
-  int spill[kStackDepth - kStackSmem];
+  int spill[kDepth - kStackSmem];
   int sp = 0;
   __device__ __forceinline__ explicit TraversalStack(int* base) : smem(base + threadIdx.x) {}
   __device__ __forceinline__ void push(int v) {
@@ -214,6 +214,142 @@ __device__ __forceinline__ RayHit closest_hit(const RtgSceneDev& sc, float3 o, f
     if (!st.pop(cur)) break;
   }
   return best;
+}
+
+// Slab tests of a four-wide node's children: entry distances and hit flags.
+__device__ __forceinline__ void node4_boxes(const DevNode4* __restrict__ nd, const SlabRay& r, float tmin, float tmax,
+                                            float in[4], bool hit[4], int link[4]) {
+  const float4 lx = __ldg(&nd->lo_x), hx = __ldg(&nd->hi_x);
+  const float4 ly = __ldg(&nd->lo_y), hy = __ldg(&nd->hi_y);
+  const float4 lz = __ldg(&nd->lo_z), hz = __ldg(&nd->hi_z);
+  const int4 lk = __ldg(&nd->link);
+  const float lox[4] = {lx.x, lx.y, lx.z, lx.w}, hix[4] = {hx.x, hx.y, hx.z, hx.w};
+  const float loy[4] = {ly.x, ly.y, ly.z, ly.w}, hiy[4] = {hy.x, hy.y, hy.z, hy.w};
+  const float loz[4] = {lz.x, lz.y, lz.z, lz.w}, hiz[4] = {hz.x, hz.y, hz.z, hz.w};
+  link[0] = lk.x;
+  link[1] = lk.y;
+  link[2] = lk.z;
+  link[3] = lk.w;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const float x0 = fmaf(lox[k], r.inv.x, -r.ooi.x), x1 = fmaf(hix[k], r.inv.x, -r.ooi.x);
+    const float y0 = fmaf(loy[k], r.inv.y, -r.ooi.y), y1 = fmaf(hiy[k], r.inv.y, -r.ooi.y);
+    const float z0 = fmaf(loz[k], r.inv.z, -r.ooi.z), z1 = fmaf(hiz[k], r.inv.z, -r.ooi.z);
+    in[k] = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), tmin));
+    const float out = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fminf(fmaxf(z0, z1), tmax));
+    hit[k] = in[k] <= out && link[k] != kNoChild;
+  }
+}
+
+__device__ __forceinline__ int pick4(const int v[4], std::uint32_t k) {
+  return k == 0 ? v[0] : (k == 1 ? v[1] : (k == 2 ? v[2] : v[3]));
+}
+
+__device__ __forceinline__ void cswap(std::uint32_t& a, std::uint32_t& b) {
+  const std::uint32_t lo = min(a, b), hi = max(a, b);
+  a = lo;
+  b = hi;
+}
+
+// Closest hit over planes then the four-wide BVH: hit children are visited
+// nearest entry first (keys = entry distance bits with the child index in the
+// low two bits, sorted by a five-exchange network).
+template <int kStackSmem, int kBlock, bool kCount>
+__device__ __forceinline__ RayHit closest_hit4(const RtgSceneDev& sc, float3 o, float3 d, float tmin, float tmax,
+                                               int* stack_base, TraceCount& cnt) {
+  RayHit best{tmax, kHitMiss, 0.f, 0.f};
+  for (int i = 0; i < sc.n_planes; ++i) {
+    float t;
+    if (plane_test(sc.planes[i], o, d, tmin, best.t, t)) {
+      best.t = t;
+      best.word = kHitPlaneBit | static_cast<std::uint32_t>(i);
+    }
+  }
+  if (sc.root4 == INT32_MIN) return best;
+  const SlabRay sr(o, d);
+  TraversalStack<kStackSmem, kBlock, kWideStackDepth> st(stack_base);
+  int cur = sc.root4;
+  while (true) {
+    if (cur >= 0) {
+      if (kCount) cnt.nodes++;
+      float in[4];
+      bool hit[4];
+      int link[4];
+      node4_boxes(sc.nodes4 + cur, sr, tmin, best.t, in, hit, link);
+      std::uint32_t key[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        key[k] = hit[k] ? ((__float_as_uint(fmaxf(in[k], 0.f)) & ~3u) | static_cast<std::uint32_t>(k)) : 0xFFFFFFFFu;
+      cswap(key[0], key[1]);
+      cswap(key[2], key[3]);
+      cswap(key[0], key[2]);
+      cswap(key[1], key[3]);
+      cswap(key[1], key[2]);
+      if (key[0] != 0xFFFFFFFFu) {
+        if (key[3] != 0xFFFFFFFFu) st.push(pick4(link, key[3] & 3u));
+        if (key[2] != 0xFFFFFFFFu) st.push(pick4(link, key[2] & 3u));
+        if (key[1] != 0xFFFFFFFFu) st.push(pick4(link, key[1] & 3u));
+        cur = pick4(link, key[0] & 3u);
+        continue;
+      }
+    } else {
+      int slot = ~cur;
+      while (true) {
+        const std::uint32_t id = prim_slot_test(sc.prims, slot, o, d, tmin, best);
+        if (kCount) cnt.add_prim(id);
+        if (id & kLastInLeaf) break;
+        ++slot;
+      }
+    }
+    if (!st.pop(cur)) break;
+  }
+  return best;
+}
+
+// Any hit over planes then the four-wide BVH (order does not matter: first hit wins).
+template <int kStackSmem, int kBlock, bool kCount>
+__device__ __forceinline__ bool any_hit4(const RtgSceneDev& sc, float3 o, float3 d, float tmin, float tmax,
+                                         int* stack_base, TraceCount& cnt) {
+  for (int i = 0; i < sc.n_planes; ++i) {
+    float t;
+    if (plane_test(sc.planes[i], o, d, tmin, tmax, t)) return true;
+  }
+  if (sc.root4 == INT32_MIN) return false;
+  const SlabRay sr(o, d);
+  TraversalStack<kStackSmem, kBlock, kWideStackDepth> st(stack_base);
+  int cur = sc.root4;
+  RayHit probe{tmax, kHitMiss, 0.f, 0.f};
+  while (true) {
+    if (cur >= 0) {
+      if (kCount) cnt.nodes++;
+      float in[4];
+      bool hit[4];
+      int link[4];
+      node4_boxes(sc.nodes4 + cur, sr, tmin, tmax, in, hit, link);
+      int next = INT32_MIN;
+#pragma unroll
+      for (int k = 3; k >= 0; --k) {
+        if (!hit[k]) continue;
+        if (next != INT32_MIN) st.push(next);
+        next = link[k];
+      }
+      if (next != INT32_MIN) {
+        cur = next;
+        continue;
+      }
+    } else {
+      int slot = ~cur;
+      while (true) {
+        const std::uint32_t id = prim_slot_test(sc.prims, slot, o, d, tmin, probe);
+        if (kCount) cnt.add_prim(id);
+        if (probe.word != kHitMiss) return true;
+        if (id & kLastInLeaf) break;
+        ++slot;
+      }
+    }
+    if (!st.pop(cur)) break;
+  }
+  return false;
 }
 
 // Any hit in (tmin, tmax): planes, then BVH with early exit.

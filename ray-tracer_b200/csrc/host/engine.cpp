@@ -46,7 +46,7 @@ void dev_free(void* p) {
 }
 
 void free_scene_arrays(GpuScene& s) {
-  dev_free(s.nodes); dev_free(s.prims); dev_free(s.slot_material); dev_free(s.slot_normals);
+  dev_free(s.nodes); dev_free(s.nodes4); dev_free(s.prims); dev_free(s.slot_material); dev_free(s.slot_normals);
   dev_free(s.planes); dev_free(s.materials); dev_free(s.lights);
   dev_free(s.prims64); dev_free(s.planes64);
 }
@@ -180,6 +180,8 @@ int Engine::add_scene(CompiledScene scene) {
   gs->n_lights = static_cast<std::int32_t>(flat.lights.size());
   std::size_t bytes = 0;
   gs->nodes = dev_upload(flat.nodes, stream_, bytes);
+  gs->nodes4 = dev_upload(flat.nodes4, stream_, bytes);
+  gs->root4 = flat.root4;
   gs->prims = dev_upload(flat.prims, stream_, bytes);
   gs->slot_material = dev_upload(flat.slot_material, stream_, bytes);
   gs->slot_normals = dev_upload(flat.slot_normals, stream_, bytes);
@@ -296,6 +298,8 @@ RtgSceneDev Engine::job_descriptor(const GpuScene& sc, const RenderSettings& s, 
   d.materials = sc.materials;
   d.lights = sc.lights;
   d.root = sc.root;
+  d.nodes4 = sc.nodes4;
+  d.root4 = sc.root4;
   d.n_planes = sc.n_planes;
   d.n_lights = sc.n_lights;
   d.slot_begin = 0;

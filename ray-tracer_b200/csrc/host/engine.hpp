@@ -71,6 +71,8 @@ struct GpuScene {
   std::int32_t root = kNoRoot;
   std::int32_t n_slots = 0, n_planes = 0, n_lights = 0;
   DevNode* nodes = nullptr;
+  DevNode4* nodes4 = nullptr;  // four-wide copy of the tree (any-hit queries)
+  std::int32_t root4 = kNoRoot;
   float4* prims = nullptr;
   std::uint32_t* slot_material = nullptr;
   float4* slot_normals = nullptr;

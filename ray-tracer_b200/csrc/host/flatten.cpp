@@ -93,6 +93,88 @@ DevMaterial material_record(const Material& m) {
   return r;
 }
 
+// Collapses the binary tree into four-child nodes: starting from an interior
+// node's two children, the interior child with the largest surface area is
+// replaced by its own children until there are four (or only leaves). Leaves
+// keep their slot ranges. Nodes are numbered in creation order from the root.
+void build_wide(const BinaryBvh& bvh, FlatScene& f) {
+  f.nodes4.clear();
+  f.depth4 = 0;
+  if (bvh.nodes.empty()) {
+    f.root4 = kNoRoot;
+    return;
+  }
+  if (bvh.nodes[0].leaf()) {
+    f.root4 = ~static_cast<std::int32_t>(bvh.nodes[0].first);
+    return;
+  }
+  struct Item {
+    std::size_t bin;   // binary interior node
+    std::size_t slot;  // its four-wide node
+    int depth;
+  };
+  std::vector<Item> work{{0, 0, 1}};
+  f.nodes4.emplace_back();
+  while (!work.empty()) {
+    const Item it = work.back();
+    work.pop_back();
+    f.depth4 = std::max(f.depth4, it.depth);
+    std::size_t kids[4];
+    int nk = 0;
+    kids[nk++] = it.bin + 1;
+    kids[nk++] = bvh.nodes[it.bin].first;
+    while (nk < 4) {
+      int pick = -1;
+      double pick_area = -1;
+      for (int k = 0; k < nk; ++k) {
+        const BinaryNode& c = bvh.nodes[kids[k]];
+        if (c.leaf()) continue;
+        const double a = c.box.area();
+        if (a > pick_area) {
+          pick_area = a;
+          pick = k;
+        }
+      }
+      if (pick < 0) break;
+      const std::size_t b = kids[pick];
+      kids[pick] = b + 1;
+      kids[nk++] = bvh.nodes[b].first;
+    }
+    float lo[3][4], hi[3][4];
+    int link[4];
+    for (int k = 0; k < 4; ++k) {
+      if (k >= nk) {
+        for (int a = 0; a < 3; ++a) lo[a][k] = hi[a][k] = 0.f;
+        link[k] = kNoChild;
+        continue;
+      }
+      const BinaryNode& c = bvh.nodes[kids[k]];
+      lo[0][k] = down(c.box.lo.x); hi[0][k] = up(c.box.hi.x);
+      lo[1][k] = down(c.box.lo.y); hi[1][k] = up(c.box.hi.y);
+      lo[2][k] = down(c.box.lo.z); hi[2][k] = up(c.box.hi.z);
+      if (c.leaf()) {
+        link[k] = ~static_cast<std::int32_t>(c.first);
+      } else {
+        link[k] = static_cast<std::int32_t>(f.nodes4.size());
+        work.push_back({kids[k], f.nodes4.size(), it.depth + 1});
+        f.nodes4.emplace_back();
+      }
+    }
+    DevNode4& d = f.nodes4[it.slot];
+    d.lo_x = make_float4(lo[0][0], lo[0][1], lo[0][2], lo[0][3]);
+    d.hi_x = make_float4(hi[0][0], hi[0][1], hi[0][2], hi[0][3]);
+    d.lo_y = make_float4(lo[1][0], lo[1][1], lo[1][2], lo[1][3]);
+    d.hi_y = make_float4(hi[1][0], hi[1][1], hi[1][2], hi[1][3]);
+    d.lo_z = make_float4(lo[2][0], lo[2][1], lo[2][2], lo[2][3]);
+    d.hi_z = make_float4(hi[2][0], hi[2][1], hi[2][2], hi[2][3]);
+    d.link = make_int4(link[0], link[1], link[2], link[3]);
+    d.pad = make_int4(0, 0, 0, 0);
+  }
+  f.root4 = 0;
+  if (3 * f.depth4 + 1 > kWideStackDepth)
+    throw std::runtime_error("BVH deeper than the traversal stack allows");
+}
+
 }  // namespace
 
 FlatScene flatten(const CompiledScene& s) {
@@ -158,6 +240,7 @@ FlatScene flatten(const CompiledScene& s) {
   }
   });
   if (!bvh.nodes.empty()) f.root = link_of(0);
+  build_wide(bvh, f);
 
   for (const PlanePrim& pl : s.planes) {
     DevPlane dp;

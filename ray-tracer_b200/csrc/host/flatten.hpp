@@ -26,6 +26,10 @@ struct FlatScene {
   std::vector<DevMaterial> materials;
   std::vector<DevLight> lights;
   std::int32_t root = kNoRoot;              // >= 0 node; < 0: ~slot of a root leaf; kNoRoot: none
+  // The same tree collapsed to four children per node (any-hit queries).
+  std::vector<DevNode4> nodes4;
+  std::int32_t root4 = kNoRoot;
+  int depth4 = 0;
 };
 
 FlatScene flatten(const CompiledScene& s);
