@@ -67,13 +67,17 @@ struct CameraSample {
   std::uint32_t sample;  // radiance slot
 };
 
-// Camera ray for local sample `local` of a segment (pixel-major, then sample):
-// jitter (2 draws), then the lens (2 draws).
+// Camera ray for local sample `local` of a segment, numbered pixel-major
+// (local = pixel * pass_spp + (s - pass_s0)): a warp's new paths are samples of
+// the same few pixels, which keeps their walks (and their later bounces) coherent;
+// numbering sample-major measured 17% slower in the closest-hit stage.
+// Jitter (2 draws), then the lens (2 draws). A segment holds fewer than 2^32 samples.
 __device__ __forceinline__ CameraSample camera_sample(const RtgSceneDev& J, const DevSegment& S, std::uint64_t local) {
   CameraSample cs;
   const std::uint32_t spp = S.pass_spp;
-  const std::uint64_t pixel = local / spp;
-  const std::uint32_t s = S.pass_s0 + static_cast<std::uint32_t>(local - pixel * spp);
+  const std::uint32_t l32 = static_cast<std::uint32_t>(local);
+  const std::uint32_t pixel = l32 / spp;
+  const std::uint32_t s = S.pass_s0 + (l32 - pixel * spp);
   const std::uint32_t px = static_cast<std::uint32_t>(pixel % static_cast<std::uint32_t>(J.width));
   const std::uint32_t py = static_cast<std::uint32_t>(pixel / static_cast<std::uint32_t>(J.width));
   cs.rng = Pcg::for_sample(J.seed, pixel, s);
@@ -91,11 +95,36 @@ __device__ __forceinline__ CameraSample camera_sample(const RtgSceneDev& J, cons
 }
 
 // ---------------------------------------------------------------------------
+// Inclusive scan over one block of kMaxGen threads (warp shuffles, then the warp
+// totals); `tot` is a kMaxGen / 32 scratch array and receives the block total.
+__device__ __forceinline__ std::uint32_t plan_scan(std::uint32_t v, std::uint32_t* tot, std::uint32_t& total) {
+  constexpr int kWarps = kMaxGen / 32;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const std::uint32_t y = __shfl_up_sync(kFull, v, off);
+    if (lane >= off) v += y;
+  }
+  if (lane == 31) tot[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    std::uint32_t x = lane < kWarps ? tot[lane] : 0u;
+#pragma unroll
+    for (int off = 1; off < kWarps; off <<= 1) {
+      const std::uint32_t y = __shfl_up_sync(kFull, x, off);
+      if (lane >= off) x += y;
+    }
+    if (lane < kWarps) tot[lane] = x;
+  }
+  __syncthreads();
+  total = tot[kWarps - 1];
+  return v + (w > 0 ? tot[w - 1] : 0u);
+}
+
 // Generation plan: free slots go to the open segments greedily in the host's
 // order. One block of kMaxGen threads, one table entry each.
 __global__ void __launch_bounds__(kMaxGen) k_plan(WaveBuffers wb, int par) {
-  __shared__ std::uint32_t scan[kMaxGen];
-  __shared__ std::uint32_t fscan[kMaxGen];
+  __shared__ std::uint32_t tot_rem[kMaxGen / 32], tot_flag[kMaxGen / 32];
   chain_to_previous_grid();
   WaveCounters* C = wb.cnt;
   const int t = threadIdx.x;
@@ -123,28 +152,13 @@ __global__ void __launch_bounds__(kMaxGen) k_plan(WaveBuffers wb, int par) {
     }
   }
   // Inclusive scan of rem (each <= room <= 2^23, so the sum fits 32 bits).
-  scan[t] = rem;
-  __syncthreads();
-  for (int off = 1; off < kMaxGen; off <<= 1) {
-    const std::uint32_t v = t >= off ? scan[t - off] : 0u;
-    __syncthreads();
-    scan[t] += v;
-    __syncthreads();
-  }
-  const std::uint32_t excl = scan[t] - rem;
-  const std::uint32_t total = scan[kMaxGen - 1];
+  std::uint32_t total = 0, n_plan = 0;
+  const std::uint32_t excl = plan_scan(rem, tot_rem, total) - rem;
   const std::uint32_t take = excl >= room ? 0u : min(rem, room - excl);
   const std::uint32_t flag = take > 0 ? 1u : 0u;
-  fscan[t] = flag;
-  __syncthreads();
-  for (int off = 1; off < kMaxGen; off <<= 1) {
-    const std::uint32_t v = t >= off ? fscan[t - off] : 0u;
-    __syncthreads();
-    fscan[t] += v;
-    __syncthreads();
-  }
+  const std::uint32_t fpos = plan_scan(flag, tot_flag, n_plan);
   if (flag) {
-    const std::uint32_t k = fscan[t] - 1;
+    const std::uint32_t k = fpos - 1;
     wb.plan->end[k] = excl + take;
     wb.plan->seg[k] = slot;
     wb.plan->start[k] = gen0;
@@ -152,7 +166,7 @@ __global__ void __launch_bounds__(kMaxGen) k_plan(WaveBuffers wb, int par) {
   }
   if (t == 0) {
     const std::uint32_t n_new = total < room ? total : room;
-    wb.plan->n = fscan[kMaxGen - 1];
+    wb.plan->n = n_plan;
     wb.plan->n_new = n_new;
     C->n_extend = live + n_new;
     C->live[par ^ 1] = 0;

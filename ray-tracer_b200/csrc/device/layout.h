@@ -135,7 +135,8 @@ struct alignas(16) DevSegment {
   std::uint32_t pass_spp;     // samples per pixel in this pass
   std::uint32_t pad;
   std::uint64_t count;        // pixels * pass_spp camera samples
-  std::uint64_t sample_base;  // radiance slot of (pixel 0, sample pass_s0)
+  std::uint64_t sample_base;  // radiance slot of (pixel 0, sample pass_s0); sample s of pixel p
+                              // is at sample_base + p * pass_spp + (s - pass_s0)
 };
 
 // Device-side progress of one segment slot (zeroed when the slot is assigned).

@@ -45,9 +45,11 @@ void dev_free(void* p) {
   if (p) cudaFree(p);
 }
 
-void free_scene_arrays(GpuScene& s) {
-  dev_free(s.nodes); dev_free(s.nodes4); dev_free(s.prims); dev_free(s.slot_material); dev_free(s.slot_normals);
-  dev_free(s.planes); dev_free(s.materials); dev_free(s.lights);
+// Returns a scene's device memory; the flattened arrays are one stream-ordered
+// allocation from the engine's pool, freed in stream order (no device sync).
+void free_scene_arrays(GpuScene& s, cudaStream_t stream) {
+  if (s.block) cudaFreeAsync(s.block, stream);
+  s.block = nullptr;
   dev_free(s.prims64); dev_free(s.planes64);
 }
 
@@ -119,6 +121,7 @@ Engine::Engine(int device) : device_(device) {
   CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
   CK(cudaEventCreate(&ev_begin_));
   CK(cudaEventCreate(&ev_end_));
+  for (auto& e : upload_ev_) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   cudaMemPoolProps props{};
   props.allocType = cudaMemAllocationTypePinned;
   props.location.type = cudaMemLocationTypeDevice;
@@ -143,11 +146,16 @@ Engine::~Engine() {
   for (auto& f : frames_) free_frame(f);
   for (auto& kv : jobs_) free_frame(kv.second.frame);
   cudaStreamSynchronize(stream_);
-  for (auto& kv : scenes_) free_scene_arrays(*kv.second);
+  for (auto& kv : scenes_) free_scene_arrays(*kv.second, stream_);
+  cudaStreamSynchronize(stream_);
   jobs_.clear();
   reset_wave();
   cudaEventDestroy(ev_begin_);
   cudaEventDestroy(ev_end_);
+  for (int b = 0; b < 2; ++b) {
+    cudaEventDestroy(upload_ev_[b]);
+    if (upload_host_[b]) cudaFreeHost(upload_host_[b]);
+  }
   cudaStreamDestroy(stream_);
   cudaMemPoolDestroy(pool_);
 }
@@ -178,20 +186,52 @@ int Engine::add_scene(CompiledScene scene) {
   gs->n_slots = static_cast<std::int32_t>(flat.slot_prim.size());
   gs->n_planes = static_cast<std::int32_t>(flat.planes.size());
   gs->n_lights = static_cast<std::int32_t>(flat.lights.size());
-  std::size_t bytes = 0;
-  gs->nodes = dev_upload(flat.nodes, stream_, bytes);
-  gs->nodes4 = dev_upload(flat.nodes4, stream_, bytes);
   gs->root4 = flat.root4;
-  gs->prims = dev_upload(flat.prims, stream_, bytes);
-  gs->slot_material = dev_upload(flat.slot_material, stream_, bytes);
-  gs->slot_normals = dev_upload(flat.slot_normals, stream_, bytes);
-  gs->planes = dev_upload(flat.planes, stream_, bytes);
-  gs->materials = dev_upload(flat.materials, stream_, bytes);
-  gs->lights = dev_upload(flat.lights, stream_, bytes);
-  gs->device_bytes = bytes;
+  // One device allocation and one copy per scene, through a pinned staging
+  // buffer: the copy runs while the caller flattens the next scene (two buffers
+  // alternate), and the flattened vectors can go at once.
+  struct Part {
+    const void* src;
+    std::size_t bytes;
+    std::size_t at;
+  };
+  auto part = [](const auto& v) { return Part{v.data(), v.size() * sizeof(v[0]), 0}; };
+  Part parts[8] = {part(flat.nodes), part(flat.nodes4), part(flat.prims), part(flat.slot_material),
+                   part(flat.slot_normals), part(flat.planes), part(flat.materials), part(flat.lights)};
+  std::size_t total = 0;
+  for (Part& p : parts) {
+    p.at = total;
+    total += (std::max<std::size_t>(p.bytes, 1) + 255) & ~std::size_t(255);
+  }
+  void* block = nullptr;
+  CK(cudaMallocFromPoolAsync(&block, total, pool_, stream_));
+  const int b = upload_next_;
+  upload_next_ ^= 1;
+  if (upload_pending_[b]) CK(cudaEventSynchronize(upload_ev_[b]));
+  if (upload_cap_[b] < total) {
+    if (upload_host_[b]) CK(cudaFreeHost(upload_host_[b]));
+    upload_host_[b] = nullptr;
+    CK(cudaMallocHost(reinterpret_cast<void**>(&upload_host_[b]), total));
+    upload_cap_[b] = total;
+  }
+  for (const Part& p : parts)
+    if (p.bytes) std::memcpy(upload_host_[b] + p.at, p.src, p.bytes);
+  CK(cudaMemcpyAsync(block, upload_host_[b], total, cudaMemcpyHostToDevice, stream_));
+  CK(cudaEventRecord(upload_ev_[b], stream_));
+  upload_pending_[b] = true;
+  auto at = [&](int k) { return static_cast<void*>(static_cast<unsigned char*>(block) + parts[k].at); };
+  gs->block = block;
+  gs->nodes = static_cast<DevNode*>(at(0));
+  gs->nodes4 = static_cast<DevNode4*>(at(1));
+  gs->prims = static_cast<float4*>(at(2));
+  gs->slot_material = static_cast<std::uint32_t*>(at(3));
+  gs->slot_normals = static_cast<float4*>(at(4));
+  gs->planes = static_cast<DevPlane*>(at(5));
+  gs->materials = static_cast<DevMaterial*>(at(6));
+  gs->lights = static_cast<DevLight*>(at(7));
+  gs->device_bytes = total;
   gs->slot_prim = std::move(flat.slot_prim);
   gs->host = std::move(scene);
-  CK(cudaStreamSynchronize(stream_));  // the host vectors die with `flat`
   const int id = next_scene_++;
   scenes_[id] = std::move(gs);
   return id;
@@ -201,8 +241,7 @@ void Engine::release_scene(int id) {
   auto it = scenes_.find(id);
   if (it == scenes_.end()) throw std::invalid_argument("unknown scene id " + std::to_string(id));
   if (it->second->jobs_open > 0) throw std::logic_error("scene " + std::to_string(id) + " is used by an open request");
-  cudaStreamSynchronize(stream_);
-  free_scene_arrays(*it->second);
+  free_scene_arrays(*it->second, stream_);
   scenes_.erase(it);
 }
 

@@ -70,6 +70,7 @@ struct GpuScene {
   std::vector<std::uint32_t> slot_prim;  // slot -> primitive id (ray API)
   std::int32_t root = kNoRoot;
   std::int32_t n_slots = 0, n_planes = 0, n_lights = 0;
+  void* block = nullptr;       // one device allocation holding the arrays below
   DevNode* nodes = nullptr;
   DevNode4* nodes4 = nullptr;  // four-wide copy of the tree (any-hit queries)
   std::int32_t root4 = kNoRoot;
@@ -251,6 +252,12 @@ class Engine {
   int device_;
   cudaStream_t stream_ = nullptr;
   cudaMemPool_t pool_ = nullptr;  // framebuffers and read-back staging
+  // Pinned staging for scene uploads (two alternating buffers).
+  unsigned char* upload_host_[2] = {nullptr, nullptr};
+  std::size_t upload_cap_[2] = {0, 0};
+  cudaEvent_t upload_ev_[2] = {nullptr, nullptr};
+  bool upload_pending_[2] = {false, false};
+  int upload_next_ = 0;
   std::size_t pool_reserved_ = 0;
   cudaEvent_t ev_begin_ = nullptr, ev_end_ = nullptr;
   EngineConfig cfg_;

@@ -69,6 +69,14 @@ void parallel_chunks(std::size_t n, F&& body) {
   for (auto& t : pool) t.join();
 }
 
+// A node box rounded outward to fp32 (lo down, hi up).
+struct FBox {
+  float lo[3], hi[3];
+};
+FBox outward(const Box& b) {
+  return FBox{{down(b.lo.x), down(b.lo.y), down(b.lo.z)}, {up(b.hi.x), up(b.hi.y), up(b.hi.z)}};
+}
+
 float4 f4(D3 v, float w = 0.f) { return make_float4(float(v.x), float(v.y), float(v.z), w); }
 float3 f3h(D3 v) { return make_float3(float(v.x), float(v.y), float(v.z)); }
 
@@ -97,7 +105,7 @@ DevMaterial material_record(const Material& m) {
 // node's two children, the interior child with the largest surface area is
 // replaced by its own children until there are four (or only leaves). Leaves
 // keep their slot ranges. Nodes are numbered in creation order from the root.
-void build_wide(const BinaryBvh& bvh, FlatScene& f) {
+void build_wide(const BinaryBvh& bvh, const std::vector<FBox>& fbox, FlatScene& f) {
   f.nodes4.clear();
   f.depth4 = 0;
   if (bvh.nodes.empty()) {
@@ -108,68 +116,86 @@ void build_wide(const BinaryBvh& bvh, FlatScene& f) {
     f.root4 = ~static_cast<std::int32_t>(bvh.nodes[0].first);
     return;
   }
+  // Topology first (serial, indices only), then the boxes in parallel.
   struct Item {
     std::size_t bin;   // binary interior node
     std::size_t slot;  // its four-wide node
     int depth;
   };
+  struct Kids {
+    std::uint32_t bin[4];
+    std::int32_t link[4];
+    int n;
+  };
+  std::vector<Kids> kids_of(1);
   std::vector<Item> work{{0, 0, 1}};
-  f.nodes4.emplace_back();
   while (!work.empty()) {
     const Item it = work.back();
     work.pop_back();
     f.depth4 = std::max(f.depth4, it.depth);
-    std::size_t kids[4];
-    int nk = 0;
-    kids[nk++] = it.bin + 1;
-    kids[nk++] = bvh.nodes[it.bin].first;
-    while (nk < 4) {
+    Kids k{};
+    k.bin[k.n++] = static_cast<std::uint32_t>(it.bin + 1);
+    k.bin[k.n++] = bvh.nodes[it.bin].first;
+    while (k.n < 4) {
       int pick = -1;
       double pick_area = -1;
-      for (int k = 0; k < nk; ++k) {
-        const BinaryNode& c = bvh.nodes[kids[k]];
+      for (int q = 0; q < k.n; ++q) {
+        const BinaryNode& c = bvh.nodes[k.bin[q]];
         if (c.leaf()) continue;
         const double a = c.box.area();
         if (a > pick_area) {
           pick_area = a;
-          pick = k;
+          pick = q;
         }
       }
       if (pick < 0) break;
-      const std::size_t b = kids[pick];
-      kids[pick] = b + 1;
-      kids[nk++] = bvh.nodes[b].first;
+      const std::uint32_t b = k.bin[pick];
+      k.bin[pick] = b + 1;
+      k.bin[k.n++] = bvh.nodes[b].first;
     }
-    float lo[3][4], hi[3][4];
-    int link[4];
-    for (int k = 0; k < 4; ++k) {
-      if (k >= nk) {
-        for (int a = 0; a < 3; ++a) lo[a][k] = hi[a][k] = 0.f;
-        link[k] = kNoChild;
+    for (int q = 0; q < 4; ++q) {
+      if (q >= k.n) {
+        k.link[q] = kNoChild;
         continue;
       }
-      const BinaryNode& c = bvh.nodes[kids[k]];
-      lo[0][k] = down(c.box.lo.x); hi[0][k] = up(c.box.hi.x);
-      lo[1][k] = down(c.box.lo.y); hi[1][k] = up(c.box.hi.y);
-      lo[2][k] = down(c.box.lo.z); hi[2][k] = up(c.box.hi.z);
+      const BinaryNode& c = bvh.nodes[k.bin[q]];
       if (c.leaf()) {
-        link[k] = ~static_cast<std::int32_t>(c.first);
+        k.link[q] = ~static_cast<std::int32_t>(c.first);
       } else {
-        link[k] = static_cast<std::int32_t>(f.nodes4.size());
-        work.push_back({kids[k], f.nodes4.size(), it.depth + 1});
-        f.nodes4.emplace_back();
+        k.link[q] = static_cast<std::int32_t>(kids_of.size());
+        work.push_back({k.bin[q], kids_of.size(), it.depth + 1});
+        kids_of.emplace_back();
       }
     }
-    DevNode4& d = f.nodes4[it.slot];
-    d.lo_x = make_float4(lo[0][0], lo[0][1], lo[0][2], lo[0][3]);
-    d.hi_x = make_float4(hi[0][0], hi[0][1], hi[0][2], hi[0][3]);
-    d.lo_y = make_float4(lo[1][0], lo[1][1], lo[1][2], lo[1][3]);
-    d.hi_y = make_float4(hi[1][0], hi[1][1], hi[1][2], hi[1][3]);
-    d.lo_z = make_float4(lo[2][0], lo[2][1], lo[2][2], lo[2][3]);
-    d.hi_z = make_float4(hi[2][0], hi[2][1], hi[2][2], hi[2][3]);
-    d.link = make_int4(link[0], link[1], link[2], link[3]);
-    d.pad = make_int4(0, 0, 0, 0);
+    kids_of[it.slot] = k;
   }
+  f.nodes4.resize(kids_of.size());
+  parallel_chunks(kids_of.size(), [&](std::size_t i0, std::size_t i1) {
+    for (std::size_t i = i0; i < i1; ++i) {
+      const Kids& k = kids_of[i];
+      float lo[3][4], hi[3][4];
+      for (int q = 0; q < 4; ++q) {
+        if (q >= k.n) {
+          for (int a = 0; a < 3; ++a) lo[a][q] = hi[a][q] = 0.f;
+          continue;
+        }
+        const FBox& b = fbox[k.bin[q]];
+        for (int a = 0; a < 3; ++a) {
+          lo[a][q] = b.lo[a];
+          hi[a][q] = b.hi[a];
+        }
+      }
+      DevNode4& d = f.nodes4[i];
+      d.lo_x = make_float4(lo[0][0], lo[0][1], lo[0][2], lo[0][3]);
+      d.hi_x = make_float4(hi[0][0], hi[0][1], hi[0][2], hi[0][3]);
+      d.lo_y = make_float4(lo[1][0], lo[1][1], lo[1][2], lo[1][3]);
+      d.hi_y = make_float4(hi[1][0], hi[1][1], hi[1][2], hi[1][3]);
+      d.lo_z = make_float4(lo[2][0], lo[2][1], lo[2][2], lo[2][3]);
+      d.hi_z = make_float4(hi[2][0], hi[2][1], hi[2][2], hi[2][3]);
+      d.link = make_int4(k.link[0], k.link[1], k.link[2], k.link[3]);
+      d.pad = make_int4(0, 0, 0, 0);
+    }
+  });
   f.root4 = 0;
   if (3 * f.depth4 + 1 > kWideStackDepth)
     throw std::runtime_error("BVH deeper than the traversal stack allows");
@@ -225,22 +251,27 @@ FlatScene flatten(const CompiledScene& s) {
     const BinaryNode& c = bvh.nodes[child];
     return c.leaf() ? ~static_cast<std::int32_t>(c.first) : dev_index[child];
   };
+  // Every node's box rounded outward once; both device trees copy from here.
+  std::vector<FBox> fbox(bvh.nodes.size());
+  parallel_chunks(bvh.nodes.size(), [&](std::size_t i0, std::size_t i1) {
+    for (std::size_t i = i0; i < i1; ++i) fbox[i] = outward(bvh.nodes[i].box);
+  });
   f.nodes.resize(static_cast<std::size_t>(ninterior));
   parallel_chunks(bvh.nodes.size(), [&](std::size_t i0, std::size_t i1) {
   for (std::size_t i = i0; i < i1; ++i) {
     const BinaryNode& n = bvh.nodes[i];
     if (n.leaf()) continue;
-    const Box& L = bvh.nodes[i + 1].box;
-    const Box& R = bvh.nodes[n.first].box;
+    const FBox& L = fbox[i + 1];
+    const FBox& R = fbox[n.first];
     DevNode& d = f.nodes[static_cast<std::size_t>(dev_index[i])];
-    d.xy0 = make_float4(down(L.lo.x), up(L.hi.x), down(L.lo.y), up(L.hi.y));
-    d.xy1 = make_float4(down(R.lo.x), up(R.hi.x), down(R.lo.y), up(R.hi.y));
-    d.zz = make_float4(down(L.lo.z), up(L.hi.z), down(R.lo.z), up(R.hi.z));
+    d.xy0 = make_float4(L.lo[0], L.hi[0], L.lo[1], L.hi[1]);
+    d.xy1 = make_float4(R.lo[0], R.hi[0], R.lo[1], R.hi[1]);
+    d.zz = make_float4(L.lo[2], L.hi[2], R.lo[2], R.hi[2]);
     d.link = make_int4(link_of(i + 1), link_of(n.first), static_cast<int>(n.axis) << 16, 0);
   }
   });
   if (!bvh.nodes.empty()) f.root = link_of(0);
-  build_wide(bvh, f);
+  build_wide(bvh, fbox, f);
 
   for (const PlanePrim& pl : s.planes) {
     DevPlane dp;
