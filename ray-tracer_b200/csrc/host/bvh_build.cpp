@@ -3,7 +3,9 @@
 #include <algorithm>
 #include <array>
 #include <chrono>
+#include <future>
 #include <stdexcept>
+#include <thread>
 
 namespace rtg {
 
@@ -24,23 +26,66 @@ int bin_index(double c, double lo, double inv_width) {
   return std::clamp(b, 0, kBinCount - 1);
 }
 
+// Large nodes bin on several threads and their two subtrees build concurrently.
+// Box unions (min/max) and counts do not depend on the order they are taken in,
+// and each subtree's nodes are numbered locally and spliced into the depth-first
+// order afterwards, so the tree is the same as a single-threaded build's.
+constexpr std::size_t kParallelItems = 16384;   // subtrees at least this big may build concurrently
+constexpr std::size_t kParallelBinItems = 65536; // nodes at least this big bin on several threads
+constexpr std::size_t kMaxTasks = 16;
+
+struct Subtree {
+  std::vector<BinaryNode> nodes;
+  BvhStats stats;
+};
+
+// Runs body(t, begin, end) on `parts` contiguous chunks of [lo, hi) concurrently.
+template <class F>
+void chunked(std::size_t lo, std::size_t hi, std::size_t parts, F&& body) {
+  std::vector<std::thread> pool;
+  const std::size_t n = hi - lo, step = (n + parts - 1) / parts;
+  for (std::size_t t = 1; t < parts; ++t) {
+    const std::size_t b = std::min(hi, lo + t * step), e = std::min(hi, b + step);
+    pool.emplace_back([&body, t, b, e] { body(t, b, e); });
+  }
+  body(std::size_t(0), lo, std::min(hi, lo + step));
+  for (auto& th : pool) th.join();
+}
+
 class SahBuilder {
  public:
-  SahBuilder(std::vector<Item>& items, BinaryBvh& out, std::size_t leaf_cap)
-      : items_(items), out_(out), leaf_cap_(leaf_cap) {}
+  SahBuilder(std::vector<Item>& items, std::size_t leaf_cap) : items_(items), leaf_cap_(leaf_cap) {
+    workers_ = std::min<std::size_t>(kMaxTasks, std::max(1u, std::thread::hardware_concurrency()));
+  }
 
-  void node(std::size_t lo, std::size_t hi, std::size_t depth) {
-    const std::size_t me = out_.nodes.size();
-    out_.nodes.emplace_back();
-    Box box, cbox;
-    for (std::size_t i = lo; i < hi; ++i) {
-      box.grow(items_[i].box);
-      cbox.grow(items_[i].centre);
-    }
-    out_.nodes[me].box = box;
-    out_.stats.max_depth = std::max(out_.stats.max_depth, depth);
+  // Builds the subtree over items [lo, hi) into `out` (indices local to `out`).
+  void node(std::size_t lo, std::size_t hi, std::size_t depth, Subtree& out, std::size_t tasks) {
+    const std::size_t me = out.nodes.size();
+    out.nodes.emplace_back();
     const std::size_t n = hi - lo;
-    if (n <= leaf_cap_ || depth >= kDepthCap) return leaf(me, lo, n);
+    const std::size_t parts = (n >= kParallelBinItems && tasks > 1) ? std::min<std::size_t>(tasks, 16) : 1;
+    Box box, cbox;
+    if (parts > 1) {
+      std::vector<Box> pb(parts), pc(parts);
+      chunked(lo, hi, parts, [&](std::size_t t, std::size_t b, std::size_t e) {
+        for (std::size_t i = b; i < e; ++i) {
+          pb[t].grow(items_[i].box);
+          pc[t].grow(items_[i].centre);
+        }
+      });
+      for (std::size_t t = 0; t < parts; ++t) {
+        box.grow(pb[t]);
+        cbox.grow(pc[t]);
+      }
+    } else {
+      for (std::size_t i = lo; i < hi; ++i) {
+        box.grow(items_[i].box);
+        cbox.grow(items_[i].centre);
+      }
+    }
+    out.nodes[me].box = box;
+    out.stats.max_depth = std::max(out.stats.max_depth, depth);
+    if (n <= leaf_cap_ || depth >= kDepthCap) return leaf(out, me, lo, n);
 
     // Evaluate the kBinCount - 1 bin boundaries on every axis.
     int split_axis = -1, split_bin = -1;
@@ -52,10 +97,28 @@ class SahBuilder {
       std::array<Box, kBinCount> bin_box{};
       std::array<std::size_t, kBinCount> bin_n{};
       const double inv_width = kBinCount / (chi - clo);
-      for (std::size_t i = lo; i < hi; ++i) {
-        const auto b = static_cast<std::size_t>(bin_index(items_[i].centre[axis], clo, inv_width));
-        bin_n[b]++;
-        bin_box[b].grow(items_[i].box);
+      if (parts > 1) {
+        std::vector<std::array<Box, kBinCount>> pbox(parts);
+        std::vector<std::array<std::size_t, kBinCount>> pn(parts);
+        chunked(lo, hi, parts, [&](std::size_t t, std::size_t b, std::size_t e) {
+          pn[t].fill(0);
+          for (std::size_t i = b; i < e; ++i) {
+            const auto k = static_cast<std::size_t>(bin_index(items_[i].centre[axis], clo, inv_width));
+            pn[t][k]++;
+            pbox[t][k].grow(items_[i].box);
+          }
+        });
+        for (std::size_t t = 0; t < parts; ++t)
+          for (std::size_t k = 0; k < kBinCount; ++k) {
+            bin_n[k] += pn[t][k];
+            bin_box[k].grow(pbox[t][k]);
+          }
+      } else {
+        for (std::size_t i = lo; i < hi; ++i) {
+          const auto b = static_cast<std::size_t>(bin_index(items_[i].centre[axis], clo, inv_width));
+          bin_n[b]++;
+          bin_box[b].grow(items_[i].box);
+        }
       }
       // Suffix (right-side) areas and counts, then a prefix sweep.
       std::array<double, kBinCount> right_area{};
@@ -93,7 +156,7 @@ class SahBuilder {
       mid = lo + n / 2;
       split_axis = cbox.widest_axis();
     } else {
-      if (split_cost >= double(n) && n <= 16) return leaf(me, lo, n);
+      if (split_cost >= double(n) && n <= 16) return leaf(out, me, lo, n);
       const double clo = cbox.lo[split_axis];
       const double inv_width = kBinCount / (cbox.hi[split_axis] - clo);
       const auto first = items_.begin() + static_cast<std::ptrdiff_t>(lo);
@@ -105,26 +168,52 @@ class SahBuilder {
       if (mid == lo || mid == hi) mid = lo + n / 2;  // rounding put everything on one side
     }
 
-    out_.nodes[me].axis = static_cast<std::uint8_t>(split_axis);
-    node(lo, mid, depth + 1);
-    const std::size_t right = out_.nodes.size();
-    node(mid, hi, depth + 1);
-    out_.nodes[me].first = static_cast<std::uint32_t>(right);
-    out_.nodes[me].count = 0;
+    out.nodes[me].axis = static_cast<std::uint8_t>(split_axis);
+    out.nodes[me].count = 0;
+    if (tasks > 1 && mid - lo >= kParallelItems && hi - mid >= kParallelItems) {
+      // Both halves concurrently, each into its own list, then spliced in order.
+      Subtree left, right;
+      const std::size_t lt = tasks / 2, rt = tasks - lt;
+      auto done = std::async(std::launch::async, [&] { node(lo, mid, depth + 1, left, lt); });
+      node(mid, hi, depth + 1, right, rt);
+      done.get();
+      splice(out, left);
+      out.nodes[me].first = static_cast<std::uint32_t>(out.nodes.size());
+      splice(out, right);
+      return;
+    }
+    node(lo, mid, depth + 1, out, tasks);
+    const std::size_t right = out.nodes.size();
+    node(mid, hi, depth + 1, out, tasks);
+    out.nodes[me].first = static_cast<std::uint32_t>(right);
   }
 
+  std::size_t workers() const { return workers_; }
+
  private:
-  void leaf(std::size_t me, std::size_t lo, std::size_t n) {
+  void leaf(Subtree& out, std::size_t me, std::size_t lo, std::size_t n) {
     if (n > 0xFFFF) throw std::runtime_error("BVH leaf too large");
-    out_.nodes[me].first = static_cast<std::uint32_t>(lo);
-    out_.nodes[me].count = static_cast<std::uint32_t>(n);
-    out_.stats.leaves++;
-    out_.stats.max_leaf = std::max(out_.stats.max_leaf, n);
+    out.nodes[me].first = static_cast<std::uint32_t>(lo);
+    out.nodes[me].count = static_cast<std::uint32_t>(n);
+    out.stats.leaves++;
+    out.stats.max_leaf = std::max(out.stats.max_leaf, n);
+  }
+
+  // Appends a subtree built with local indices; its interior links move by the offset.
+  static void splice(Subtree& out, const Subtree& sub) {
+    const auto base = static_cast<std::uint32_t>(out.nodes.size());
+    for (BinaryNode nd : sub.nodes) {
+      if (!nd.leaf()) nd.first += base;
+      out.nodes.push_back(nd);
+    }
+    out.stats.leaves += sub.stats.leaves;
+    out.stats.max_leaf = std::max(out.stats.max_leaf, sub.stats.max_leaf);
+    out.stats.max_depth = std::max(out.stats.max_depth, sub.stats.max_depth);
   }
 
   std::vector<Item>& items_;
-  BinaryBvh& out_;
   std::size_t leaf_cap_;
+  std::size_t workers_ = 1;
 };
 
 }  // namespace
@@ -143,8 +232,14 @@ void BinaryBvh::build(const std::vector<Box>& prim_boxes, int max_leaf) {
   }
   if (items.empty()) return;
   const std::size_t cap = static_cast<std::size_t>(std::max(1, max_leaf));
-  nodes.reserve(2 * items.size() / cap + 1);
-  SahBuilder(items, *this, cap).node(0, items.size(), 0);
+  SahBuilder builder(items, cap);
+  Subtree tree;
+  tree.nodes.reserve(2 * items.size() / cap + 1);
+  builder.node(0, items.size(), 0, tree, builder.workers());
+  nodes = std::move(tree.nodes);
+  stats.leaves = tree.stats.leaves;
+  stats.max_leaf = tree.stats.max_leaf;
+  stats.max_depth = tree.stats.max_depth;
   order.resize(items.size());
   for (std::size_t i = 0; i < items.size(); ++i) order[i] = items[i].id;
 
