@@ -134,15 +134,17 @@ __device__ __forceinline__ bool plane_test(const DevPlane& pl, float3 o, float3 
 // Tests one primitive slot; updates the best hit when closer.
 __device__ __forceinline__ std::uint32_t prim_slot_test(const float4* __restrict__ prims, int slot, float3 o, float3 d,
                                                         float tmin, RayHit& best) {
+  // All three rows at once: waiting for the kind bit before fetching the third
+  // row put a second memory round trip on every triangle test.
   const float4 p0 = __ldg(&prims[3 * slot]);
   const float4 p1 = __ldg(&prims[3 * slot + 1]);
+  const float4 p2 = __ldg(&prims[3 * slot + 2]);
   const std::uint32_t id = __float_as_uint(p0.w);
   float t, b1 = 0.f, b2 = 0.f;
   bool hit;
   if (id & kSphereBit) {
     hit = sphere_test(o, d, f3(p0), p1.x, tmin, best.t, t);
   } else {
-    const float4 p2 = __ldg(&prims[3 * slot + 2]);
     hit = tri_test(o, d, f3(p0), f3(p1), f3(p2), tmin, best.t, t, b1, b2);
   }
   if (hit) {
