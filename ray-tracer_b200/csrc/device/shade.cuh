@@ -46,6 +46,7 @@ __device__ __forceinline__ Surface make_surface(const RtgSceneDev& sc, float3 o,
   const int slot = static_cast<int>(h.word);
   const float4 p0 = __ldg(&sc.prims[3 * slot]);
   const float4 p1 = __ldg(&sc.prims[3 * slot + 1]);
+  const float4 p2 = __ldg(&sc.prims[3 * slot + 2]);  // with the others, not after the kind test
   const std::uint32_t mword = __ldg(&sc.slot_material[slot]);
   s.material = mword & 0x7FFFFFFFu;
   if (__float_as_uint(p0.w) & kSphereBit) {
@@ -56,7 +57,6 @@ __device__ __forceinline__ Surface make_surface(const RtgSceneDev& sc, float3 o,
     s.n = s.gn;
     return s;
   }
-  const float4 p2 = __ldg(&sc.prims[3 * slot + 2]);
   s.p = f3(p0) + h.b1 * f3(p1) + h.b2 * f3(p2);
   const float3 ng = unit_or(cross3(f3(p1), f3(p2)), f3(0.f, 0.f, 0.f));
   s.front = dot3(d, ng) < 0.f;

@@ -99,7 +99,7 @@ AutotuneResult autotune(Engine& e, const std::vector<Engine::BatchJob>& jobs, co
   for (auto& j : probe) j.settings.spp = std::max(1, j.settings.spp / 16);
   const bool timed = cfg.time_kernels, counted = cfg.count_traversal;
   cfg.time_kernels = cfg.count_traversal = false;
-  const std::uint32_t pools[] = {1u << 20, 1u << 21, 1u << 22};
+  const std::uint32_t pools[] = {1u << 20, 1u << 21, 1u << 22, 6u << 20, 1u << 23};
   const int blocks[] = {128, 256};
   for (std::uint32_t pool : pools) {
     for (int block : blocks) {

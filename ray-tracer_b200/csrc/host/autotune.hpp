@@ -1,5 +1,5 @@
 #pragma once
-// Engine autotuner: picks the wavefront pool size and block size for a workload
+// Engine autotuner: picks the wavefront pool size (1M to 8M path slots) and block size for a workload
 // by rendering a reduced copy of it (every job at 1/16 of its samples) under each
 // candidate and keeping the fastest by device time. Results are cached per GPU
 // (name, SM count) and per workload signature (scene sizes, resolutions, sample
