@@ -243,71 +243,6 @@ __device__ __forceinline__ void node4_boxes(const DevNode4* __restrict__ nd, con
   }
 }
 
-__device__ __forceinline__ int pick4(const int v[4], std::uint32_t k) {
-  return k == 0 ? v[0] : (k == 1 ? v[1] : (k == 2 ? v[2] : v[3]));
-}
-
-__device__ __forceinline__ void cswap(std::uint32_t& a, std::uint32_t& b) {
-  const std::uint32_t lo = min(a, b), hi = max(a, b);
-  a = lo;
-  b = hi;
-}
-
-// Closest hit over planes then the four-wide BVH: hit children are visited
-// nearest entry first (keys = entry distance bits with the child index in the
-// low two bits, sorted by a five-exchange network).
-template <int kStackSmem, int kBlock, bool kCount>
-__device__ __forceinline__ RayHit closest_hit4(const RtgSceneDev& sc, float3 o, float3 d, float tmin, float tmax,
-                                               int* stack_base, TraceCount& cnt) {
-  RayHit best{tmax, kHitMiss, 0.f, 0.f};
-  for (int i = 0; i < sc.n_planes; ++i) {
-    float t;
-    if (plane_test(sc.planes[i], o, d, tmin, best.t, t)) {
-      best.t = t;
-      best.word = kHitPlaneBit | static_cast<std::uint32_t>(i);
-    }
-  }
-  if (sc.root4 == INT32_MIN) return best;
-  const SlabRay sr(o, d);
-  TraversalStack<kStackSmem, kBlock, kWideStackDepth> st(stack_base);
-  int cur = sc.root4;
-  while (true) {
-    if (cur >= 0) {
-      if (kCount) cnt.nodes++;
-      float in[4];
-      bool hit[4];
-      int link[4];
-      node4_boxes(sc.nodes4 + cur, sr, tmin, best.t, in, hit, link);
-      std::uint32_t key[4];
-#pragma unroll
-      for (int k = 0; k < 4; ++k)
-        key[k] = hit[k] ? ((__float_as_uint(fmaxf(in[k], 0.f)) & ~3u) | static_cast<std::uint32_t>(k)) : 0xFFFFFFFFu;
-      cswap(key[0], key[1]);
-      cswap(key[2], key[3]);
-      cswap(key[0], key[2]);
-      cswap(key[1], key[3]);
-      cswap(key[1], key[2]);
-      if (key[0] != 0xFFFFFFFFu) {
-        if (key[3] != 0xFFFFFFFFu) st.push(pick4(link, key[3] & 3u));
-        if (key[2] != 0xFFFFFFFFu) st.push(pick4(link, key[2] & 3u));
-        if (key[1] != 0xFFFFFFFFu) st.push(pick4(link, key[1] & 3u));
-        cur = pick4(link, key[0] & 3u);
-        continue;
-      }
-    } else {
-      int slot = ~cur;
-      while (true) {
-        const std::uint32_t id = prim_slot_test(sc.prims, slot, o, d, tmin, best);
-        if (kCount) cnt.add_prim(id);
-        if (id & kLastInLeaf) break;
-        ++slot;
-      }
-    }
-    if (!st.pop(cur)) break;
-  }
-  return best;
-}
-
 // Any hit over planes then the four-wide BVH (order does not matter: first hit wins).
 template <int kStackSmem, int kBlock, bool kCount>
 __device__ __forceinline__ bool any_hit4(const RtgSceneDev& sc, float3 o, float3 d, float tmin, float tmax,
@@ -339,47 +274,6 @@ __device__ __forceinline__ bool any_hit4(const RtgSceneDev& sc, float3 o, float3
         cur = next;
         continue;
       }
-    } else {
-      int slot = ~cur;
-      while (true) {
-        const std::uint32_t id = prim_slot_test(sc.prims, slot, o, d, tmin, probe);
-        if (kCount) cnt.add_prim(id);
-        if (probe.word != kHitMiss) return true;
-        if (id & kLastInLeaf) break;
-        ++slot;
-      }
-    }
-    if (!st.pop(cur)) break;
-  }
-  return false;
-}
-
-// Any hit in (tmin, tmax): planes, then BVH with early exit.
-template <int kStackSmem, int kBlock, bool kCount>
-__device__ __forceinline__ bool any_hit(const RtgSceneDev& sc, float3 o, float3 d, float tmin, float tmax,
-                                        int* stack_base, TraceCount& cnt) {
-  for (int i = 0; i < sc.n_planes; ++i) {
-    float t;
-    if (plane_test(sc.planes[i], o, d, tmin, tmax, t)) return true;
-  }
-  if (sc.root == INT32_MIN) return false;
-  const SlabRay sr(o, d);
-  TraversalStack<kStackSmem, kBlock> st(stack_base);
-  int cur = sc.root;
-  RayHit probe{tmax, kHitMiss, 0.f, 0.f};
-  while (true) {
-    if (cur >= 0) {
-      if (kCount) cnt.nodes++;
-      bool h0, h1;
-      int4 link;
-      node_boxes(sc.nodes + cur, sr, tmin, tmax, h0, h1, link);
-      if (h0 && h1) {
-        st.push(link.y);
-        cur = link.x;
-        continue;
-      }
-      if (h0) { cur = link.x; continue; }
-      if (h1) { cur = link.y; continue; }
     } else {
       int slot = ~cur;
       while (true) {
