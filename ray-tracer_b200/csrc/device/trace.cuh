@@ -74,6 +74,12 @@ __device__ __forceinline__ void node_boxes(const DevNode* __restrict__ node, con
   if (second_first) *second_first = b_in < a_in;
 }
 
+// Barycentric slack of the fp32 triangle test. Without it, a ray through the edge
+// two triangles share can round outside both and pass through the surface: with
+// the Cornell camera, pixel centres on the image diagonal met the back wall's
+// diagonal edge that way. The reference, in double, hits one of the two.
+constexpr float kEdgeSlack = 1e-6f;
+
 // Möller-Trumbore, two-sided (include/raytracer/geometry/shapes.hpp:110-127).
 __device__ __forceinline__ bool tri_test(float3 o, float3 d, float3 v0, float3 e1, float3 e2, float tmin, float tmax,
                                          float& t, float& b1, float& b2) {
@@ -83,10 +89,10 @@ __device__ __forceinline__ bool tri_test(float3 o, float3 d, float3 v0, float3 e
   const float inv_det = 1.f / det;
   const float3 tv = o - v0;
   const float u = dot3(tv, pv) * inv_det;
-  if (u < 0.f || u > 1.f) return false;
+  if (u < -kEdgeSlack || u > 1.f + kEdgeSlack) return false;
   const float3 qv = cross3(tv, e1);
   const float v = dot3(d, qv) * inv_det;
-  if (v < 0.f || u + v > 1.f) return false;
+  if (v < -kEdgeSlack || u + v > 1.f + kEdgeSlack) return false;
   const float tt = dot3(e2, qv) * inv_det;
   if (!(tmin < tt && tt < tmax)) return false;
   t = tt;
