@@ -314,7 +314,7 @@ def run_rtg(a, dist, scenes, desc):
     phase = {"upload_s": 0.0, "render_s": 0.0, "images_s": 0.0, "release_s": 0.0}
     for _ in range(max(1, a.steps)):
         c0 = time.perf_counter()
-        ids = [ctx.upload(h) for h in hosts]
+        ids = ctx.upload_many(hosts)
         c1 = time.perf_counter()
         if batched:
             ctx.render_batch(ids, settings, opts)

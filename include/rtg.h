@@ -164,6 +164,10 @@ int rtg_scene_load_file(rtg_context* ctx, const char* path, rtg_scene_id* out);
 /* Flatten a host-compiled scene to the device layout and copy it to HBM. The
  * host scene stays owned by the caller. */
 int rtg_scene_upload(rtg_context* ctx, const rtg_host_scene* scene, rtg_scene_id* out);
+/* Uploads n host scenes at once: they are flattened for the device in parallel
+ * on the host cores, then copied. out receives n ids (no counterpart in the
+ * reference: the batched form). */
+int rtg_scene_upload_batch(rtg_context* ctx, int32_t n, const rtg_host_scene* const* scenes, rtg_scene_id* out);
 /* The scene file's own render settings. */
 int rtg_scene_settings(rtg_context* ctx, rtg_scene_id scene, rtg_settings* out);
 int rtg_scene_get_info(rtg_context* ctx, rtg_scene_id scene, rtg_scene_info* out);

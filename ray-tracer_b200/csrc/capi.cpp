@@ -26,7 +26,7 @@ std::vector<std::uint8_t> encode_png(const std::uint8_t* rgb, int width, int hei
 }
 
 struct rtg_host_scene {
-  rtg::CompiledScene scene;
+  std::shared_ptr<const rtg::CompiledScene> scene;  // shared with every context it is uploaded to
   // Reference-layout arrays behind rtg_scene_view.
   std::vector<double> prims, planes, nodes, point_lights, materials;
   std::vector<std::uint32_t> lights;
@@ -200,8 +200,8 @@ int rtg_compile(const char* scene_json, const char* base_dir, rtg_host_scene** o
     rtg::SceneDesc d = rtg::parse_scene(scene_json);
     if (base_dir) d.base_dir = base_dir;
     auto hs = std::make_unique<rtg_host_scene>();
-    hs->scene = rtg::compile_scene(d);
-    const rtg::CompiledScene& s = hs->scene;
+    hs->scene = std::make_shared<const rtg::CompiledScene>(rtg::compile_scene(d));
+    const rtg::CompiledScene& s = *hs->scene;
     for (const rtg::Prim& p : s.prims) {
       const rtg::D3 v[6] = {p.a, p.b, p.c, p.n0, p.n1, p.n2};
       hs->prims.push_back(p.kind == rtg::Prim::kSphere ? 0.0 : 1.0);
@@ -267,7 +267,7 @@ void rtg_host_scene_free(rtg_host_scene* scene) { delete scene; }
 
 int rtg_host_scene_view(const rtg_host_scene* hs, rtg_scene_view* out) {
   if (!hs || !out) return RTG_ERR_INVALID;
-  const rtg::CompiledScene& s = hs->scene;
+  const rtg::CompiledScene& s = *hs->scene;
   *out = rtg_scene_view{};
   out->n_prims = s.prims.size();
   out->n_planes = s.planes.size();
@@ -312,6 +312,20 @@ int rtg_scene_upload(rtg_context* ctx, const rtg_host_scene* scene, rtg_scene_id
   });
 }
 
+int rtg_scene_upload_batch(rtg_context* ctx, int32_t n, const rtg_host_scene* const* scenes, rtg_scene_id* out) {
+  return guarded(ctx, [&]() {
+    if (n < 0 || (n > 0 && (!scenes || !out))) throw std::invalid_argument("null argument");
+    std::vector<std::shared_ptr<const rtg::CompiledScene>> list;
+    for (int32_t k = 0; k < n; ++k) {
+      if (!scenes[k]) throw std::invalid_argument("null scene in batch");
+      list.push_back(scenes[k]->scene);
+    }
+    const std::vector<int> ids = ctx->engine->add_scenes(list);
+    for (int32_t k = 0; k < n; ++k) out[k] = ids[static_cast<std::size_t>(k)];
+    return RTG_OK;
+  });
+}
+
 int rtg_device_count(void) {
   int n = 0;
   if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
@@ -343,7 +357,7 @@ int rtg_scene_load_json(rtg_context* ctx, const char* scene_json, const char* ba
     if (!scene_json || !out) throw std::invalid_argument("null argument");
     rtg::SceneDesc d = rtg::parse_scene(scene_json);
     if (base_dir) d.base_dir = base_dir;
-    *out = ctx->engine->add_scene(rtg::compile_scene(d));
+    *out = ctx->engine->add_scene(std::make_shared<const rtg::CompiledScene>(rtg::compile_scene(d)));
     return RTG_OK;
   });
 }
@@ -352,7 +366,7 @@ int rtg_scene_load_file(rtg_context* ctx, const char* path, rtg_scene_id* out) {
   return guarded(ctx, [&]() {
     if (!path || !out) throw std::invalid_argument("null argument");
     const rtg::SceneDesc d = rtg::load_scene(path);
-    *out = ctx->engine->add_scene(rtg::compile_scene(d));
+    *out = ctx->engine->add_scene(std::make_shared<const rtg::CompiledScene>(rtg::compile_scene(d)));
     return RTG_OK;
   });
 }
@@ -360,7 +374,7 @@ int rtg_scene_load_file(rtg_context* ctx, const char* path, rtg_scene_id* out) {
 int rtg_scene_settings(rtg_context* ctx, rtg_scene_id scene, rtg_settings* out) {
   return guarded(ctx, [&]() {
     if (!out) throw std::invalid_argument("null argument");
-    *out = to_c(ctx->engine->scene(scene).host.settings);
+    *out = to_c(ctx->engine->scene(scene).host->settings);
     return RTG_OK;
   });
 }
@@ -369,9 +383,9 @@ int rtg_scene_get_info(rtg_context* ctx, rtg_scene_id scene, rtg_scene_info* out
   return guarded(ctx, [&]() {
     if (!out) throw std::invalid_argument("null argument");
     const rtg::GpuScene& g = ctx->engine->scene(scene);
-    const rtg::BuildInfo& i = g.host.info;
+    const rtg::BuildInfo& i = g.host->info;
     *out = rtg_scene_info{};
-    out->primitives = g.host.prims.size();
+    out->primitives = g.host->prims.size();
     out->triangles = i.triangles;
     out->spheres = i.spheres;
     out->planes = i.planes;
@@ -402,7 +416,7 @@ int rtg_render(rtg_context* ctx, rtg_scene_id scene, const rtg_settings* setting
     if (ctx->busy) return RTG_ERR_BUSY;
     if (settings)
       if (const char* bad = settings_problem(*settings)) throw rtg::SceneError(bad);
-    const rtg::RenderSettings s = settings ? from_c(*settings) : ctx->engine->scene(scene).host.settings;
+    const rtg::RenderSettings s = settings ? from_c(*settings) : ctx->engine->scene(scene).host->settings;
     if (const char* bad = settings_problem(s)) throw rtg::SceneError(bad);
     rtg::RenderOptions o;
     if (opts) {
@@ -435,7 +449,7 @@ int rtg_render_batch(rtg_context* ctx, int32_t n, const rtg_scene_id* scenes, co
     for (int32_t j = 0; j < n; ++j) {
       if (settings)
         if (const char* bad = settings_problem(settings[j])) throw rtg::SceneError(bad);
-      const rtg::RenderSettings s = settings ? from_c(settings[j]) : ctx->engine->scene(scenes[j]).host.settings;
+      const rtg::RenderSettings s = settings ? from_c(settings[j]) : ctx->engine->scene(scenes[j]).host->settings;
       if (const char* bad = settings_problem(s)) throw rtg::SceneError(bad);
       jobs.push_back({scenes[j], s});
     }
@@ -634,7 +648,7 @@ int rtg_autotune(rtg_context* ctx, int32_t n, const rtg_scene_id* scenes, const 
     for (int32_t j = 0; j < n; ++j) {
       if (settings)
         if (const char* bad = settings_problem(settings[j])) throw rtg::SceneError(bad);
-      const rtg::RenderSettings s = settings ? from_c(settings[j]) : ctx->engine->scene(scenes[j]).host.settings;
+      const rtg::RenderSettings s = settings ? from_c(settings[j]) : ctx->engine->scene(scenes[j]).host->settings;
       if (const char* bad = settings_problem(s)) throw rtg::SceneError(bad);
       jobs.push_back({scenes[j], s});
     }
@@ -662,7 +676,7 @@ int rtg_request_submit(rtg_context* ctx, rtg_scene_id scene, const rtg_settings*
       if (const char* bad = settings_problem(*settings)) throw rtg::SceneError(bad);
     rtg::JobSpec spec;
     spec.scene_id = scene;
-    spec.settings = settings ? from_c(*settings) : ctx->engine->scene(scene).host.settings;
+    spec.settings = settings ? from_c(*settings) : ctx->engine->scene(scene).host->settings;
     if (const char* bad = settings_problem(spec.settings)) throw rtg::SceneError(bad);
     if (opts) {
       spec.opts.progressive = opts->progressive != 0;

@@ -3,10 +3,14 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
+#include <exception>
 #include <limits>
+#include <mutex>
 #include <stdexcept>
 #include <string>
+#include <thread>
 
 namespace rtg {
 
@@ -178,10 +182,42 @@ void Engine::reset_wave() {
   segs_.clear();
 }
 
-int Engine::add_scene(CompiledScene scene) {
+int Engine::add_scene(std::shared_ptr<const CompiledScene> scene) {
+  FlatScene flat = flatten(*scene);
+  return add_flat(std::move(scene), std::move(flat));
+}
+
+std::vector<int> Engine::add_scenes(const std::vector<std::shared_ptr<const CompiledScene>>& scenes) {
+  // Flatten on all host cores (one scene per task), then copy in order.
+  std::vector<FlatScene> flats(scenes.size());
+  std::atomic<std::size_t> next{0};
+  std::exception_ptr failed;
+  std::mutex failed_lock;
+  auto work = [&] {
+    for (std::size_t k; (k = next.fetch_add(1)) < scenes.size();) {
+      try {
+        flats[k] = flatten(*scenes[k]);
+      } catch (...) {
+        std::lock_guard<std::mutex> g(failed_lock);
+        if (!failed) failed = std::current_exception();
+      }
+    }
+  };
+  const std::size_t workers = std::min<std::size_t>(scenes.size(), std::max(1u, std::thread::hardware_concurrency()));
+  std::vector<std::thread> pool;
+  for (std::size_t w = 1; w < workers; ++w) pool.emplace_back(work);
+  work();
+  for (auto& t : pool) t.join();
+  if (failed) std::rethrow_exception(failed);
+  std::vector<int> ids;
+  ids.reserve(scenes.size());
+  for (std::size_t k = 0; k < scenes.size(); ++k) ids.push_back(add_flat(scenes[k], std::move(flats[k])));
+  return ids;
+}
+
+int Engine::add_flat(std::shared_ptr<const CompiledScene> scene, FlatScene flat) {
   CK(cudaSetDevice(device_));
   auto gs = std::make_unique<GpuScene>();
-  FlatScene flat = flatten(scene);
   gs->root = flat.root;
   gs->n_slots = static_cast<std::int32_t>(flat.slot_prim.size());
   gs->n_planes = static_cast<std::int32_t>(flat.planes.size());
@@ -328,7 +364,7 @@ void Engine::free_frame(GpuFrame& f) {
 
 RtgSceneDev Engine::job_descriptor(const GpuScene& sc, const RenderSettings& s, const GpuFrame& f) const {
   RtgSceneDev d{};
-  describe(sc.host, s, d);
+  describe(*sc.host, s, d);
   d.nodes = sc.nodes;
   d.prims = sc.prims;
   d.slot_material = sc.slot_material;
@@ -979,7 +1015,7 @@ void Engine::trace_closest(int scene_id, const float* rays, std::uint64_t n, boo
     // Double originals in slot order, for the reported distance only.
     std::vector<double> g(std::max<std::size_t>(1, sc.slot_prim.size()) * 9, 0.0);
     for (std::size_t k = 0; k < sc.slot_prim.size(); ++k) {
-      const Prim& p = sc.host.prims[sc.slot_prim[k]];
+      const Prim& p = sc.host->prims[sc.slot_prim[k]];
       const D3 v[3] = {p.a, p.kind == Prim::kSphere ? D3{p.b.x, 0, 0} : p.b, p.c};
       for (int j = 0; j < 3; ++j) {
         g[9 * k + 3 * j] = v[j].x;
@@ -987,9 +1023,9 @@ void Engine::trace_closest(int scene_id, const float* rays, std::uint64_t n, boo
         g[9 * k + 3 * j + 2] = v[j].z;
       }
     }
-    std::vector<double> pl(std::max<std::size_t>(1, sc.host.planes.size()) * 6, 0.0);
-    for (std::size_t k = 0; k < sc.host.planes.size(); ++k) {
-      const PlanePrim& q = sc.host.planes[k];
+    std::vector<double> pl(std::max<std::size_t>(1, sc.host->planes.size()) * 6, 0.0);
+    for (std::size_t k = 0; k < sc.host->planes.size(); ++k) {
+      const PlanePrim& q = sc.host->planes[k];
       const double r[6] = {q.point.x, q.point.y, q.point.z, q.normal.x, q.normal.y, q.normal.z};
       std::copy(r, r + 6, pl.begin() + 6 * k);
     }
@@ -998,7 +1034,7 @@ void Engine::trace_closest(int scene_id, const float* rays, std::uint64_t n, boo
     sc.planes64 = dev_upload(pl, stream_, bytes);
     CK(cudaStreamSynchronize(stream_));
   }
-  RenderSettings s = sc.host.settings;
+  RenderSettings s = sc.host->settings;
   s.use_bvh = !brute;
   const RtgSceneDev d = job_descriptor(sc, s, GpuFrame{});
   RtgSceneDev* dd = dev_alloc<RtgSceneDev>(1);
@@ -1033,7 +1069,7 @@ void Engine::trace_any(int scene_id, const float* rays, std::uint64_t n, bool br
   GpuScene& sc = scene(scene_id);
   if (n == 0) return;
   if (n > 0xFFFFFFFFull) throw std::invalid_argument("too many rays in one call");
-  RenderSettings s = sc.host.settings;
+  RenderSettings s = sc.host->settings;
   s.use_bvh = !brute;
   const RtgSceneDev d = job_descriptor(sc, s, GpuFrame{});
   RtgSceneDev* dd = dev_alloc<RtgSceneDev>(1);
@@ -1057,7 +1093,7 @@ namespace rtg {
 
 RtgSceneDev Engine::query_descriptor(int scene_id, bool brute) {
   GpuScene& sc = scene(scene_id);
-  RenderSettings s = sc.host.settings;
+  RenderSettings s = sc.host->settings;
   s.use_bvh = !brute;
   return job_descriptor(sc, s, GpuFrame{});
 }

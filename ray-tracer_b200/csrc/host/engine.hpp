@@ -66,7 +66,7 @@ struct RenderStats {
 
 // One uploaded scene: device copy of the flattened arrays plus the host compile.
 struct GpuScene {
-  CompiledScene host;
+  std::shared_ptr<const CompiledScene> host;  // shared with the caller's host scene (not copied)
   std::vector<std::uint32_t> slot_prim;  // slot -> primitive id (ray API)
   std::int32_t root = kNoRoot;
   std::int32_t n_slots = 0, n_planes = 0, n_lights = 0;
@@ -129,7 +129,9 @@ class Engine {
   cudaStream_t stream() const { return stream_; }
   EngineConfig& config() { return cfg_; }
 
-  int add_scene(CompiledScene scene);
+  int add_scene(std::shared_ptr<const CompiledScene> scene);
+  // Several scenes at once: flattened in parallel on the host, then copied.
+  std::vector<int> add_scenes(const std::vector<std::shared_ptr<const CompiledScene>>& scenes);
   void release_scene(int id);
   GpuScene& scene(int id);
   bool has_scene(int id) const { return scenes_.count(id) != 0; }
@@ -224,6 +226,7 @@ class Engine {
     std::uint64_t closed_at = 0;    // first iteration whose plan no longer lists it (cancelled)
   };
 
+  int add_flat(std::shared_ptr<const CompiledScene> scene, FlatScene flat);
   void ensure_wave();
   GpuFrame make_frame(int w, int h);
   void free_frame(GpuFrame& f);

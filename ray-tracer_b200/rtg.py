@@ -127,6 +127,7 @@ _SIGNATURES = {
     "rtg_scene_load_json": (C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.POINTER(C.c_int32)]),
     "rtg_scene_load_file": (C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_int32)]),
     "rtg_scene_upload": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int32)]),
+    "rtg_scene_upload_batch": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_void_p), C.POINTER(C.c_int32)]),
     "rtg_scene_settings": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(_Settings)]),
     "rtg_scene_get_info": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(_SceneInfo)]),
     "rtg_scene_release": (C.c_int, [C.c_void_p, C.c_int32]),
@@ -375,6 +376,14 @@ class Context:
         sid = C.c_int32()
         self._check(lib().rtg_scene_upload(self._h, scene.handle, C.byref(sid)))
         return sid.value
+
+    def upload_many(self, scenes: list[HostScene]) -> list[int]:
+        """Uploads several host scenes at once (flattened in parallel)."""
+        n = len(scenes)
+        handles = (C.c_void_p * n)(*[s.handle for s in scenes])
+        ids = (C.c_int32 * n)()
+        self._check(lib().rtg_scene_upload_batch(self._h, n, handles, ids))
+        return list(ids)
 
     def load_json(self, scene_json: str, base_dir: Optional[str] = None) -> int:
         sid = C.c_int32()

@@ -242,3 +242,23 @@ def test_workloads_render_with_no_invalid_samples(ctx, make):
     scene["render"].update(width=64, height=64, spp=8)
     prog, s, q, n, stats = render(ctx, scene)
     assert prog.finished and stats["invalid_samples"] == 0 and np.isfinite(s).all() and s.max() > 0
+
+
+def test_batch_upload_renders_like_single_uploads(ctx):
+    scenes = [workloads.cornell(width=24, height=24, spp=3), workloads.mesh_stress(width=16, height=16, spp=2),
+              workloads.mix_scene(5)]
+    scenes[2]["render"].update(width=16, height=16, spp=2)
+    hosts = [rtg.parse_scene(json.dumps(s)) for s in scenes]
+    single = [ctx.upload(h) for h in hosts]
+    many = ctx.upload_many(hosts)
+    assert len(set(single + many)) == 6
+    for a, b in zip(single, many):
+        st = ctx.scene_settings(a)
+        assert ctx.scene_info(a)["primitives"] == ctx.scene_info(b)["primitives"]
+        ctx.render(a, st)
+        ra = ctx.framebuffer_moments(-1, st.width, st.height)[0]
+        ctx.render(b, st)
+        rb = ctx.framebuffer_moments(-1, st.width, st.height)[0]
+        assert ra.tobytes() == rb.tobytes()
+    for i in single + many:
+        ctx.release(i)
