@@ -21,6 +21,10 @@
 // framebuffer in sample order (Framebuffer::add,
 // include/raytracer/rendering/framebuffer.hpp:31), passes of one render in order.
 //
+// Path state, hits and shadow rays are written and read once per iteration and
+// outgrow L2 at the pool sizes used, so they go through cache-streaming loads and
+// stores (__ldcs / __stcs) and leave L1/L2 to the BVH nodes and primitives.
+//
 // Work distribution: persistent warps fetch 32 items at a time from a cursor in
 // WaveCounters (Aila & Laine, "Understanding the Efficiency of Ray Traversal on
 // GPUs", HPG 2009), so uneven traversal costs balance across SMs.
@@ -215,16 +219,16 @@ __global__ void __launch_bounds__(kBlock) k_extend(WaveBuffers wb, int par) {
       const CameraSample cs = camera_sample(wb.jobs[job], S, local);
       o = cs.o;
       d = cs.d;
-      A[i] = make_float4(o.x, o.y, o.z, __uint_as_float(cs.sample));
+      __stcs(&A[i], make_float4(o.x, o.y, o.z, __uint_as_float(cs.sample)));
       // Camera rays count as a specular bounce (no NEE double-count guard).
-      B[i] = make_float4(d.x, d.y, d.z, __uint_as_float(kFlagSpecular | (job << kMetaSceneShift)));
-      wb.st_c[par][i] = make_float4(1.f, 1.f, 1.f, __uint_as_float(seg));
-      wb.st_d[par][i] = make_uint4(static_cast<std::uint32_t>(cs.rng.state), static_cast<std::uint32_t>(cs.rng.state >> 32),
-                                   static_cast<std::uint32_t>(cs.rng.inc), static_cast<std::uint32_t>(cs.rng.inc >> 32));
+      __stcs(&B[i], make_float4(d.x, d.y, d.z, __uint_as_float(kFlagSpecular | (job << kMetaSceneShift))));
+      __stcs(&wb.st_c[par][i], make_float4(1.f, 1.f, 1.f, __uint_as_float(seg)));
+      __stcs(&wb.st_d[par][i], make_uint4(static_cast<std::uint32_t>(cs.rng.state), static_cast<std::uint32_t>(cs.rng.state >> 32),
+                                   static_cast<std::uint32_t>(cs.rng.inc), static_cast<std::uint32_t>(cs.rng.inc >> 32)));
       wb.radiance[cs.sample] = make_float4(0.f, 0.f, 0.f, 0.f);
     } else {
-      const float4 a = A[i];
-      const float4 b = B[i];
+      const float4 a = __ldcs(&A[i]);
+      const float4 b = __ldcs(&B[i]);
       o = f3(a);
       d = f3(b);
       job = __float_as_uint(b.w) >> kMetaSceneShift;
@@ -232,7 +236,7 @@ __global__ void __launch_bounds__(kBlock) k_extend(WaveBuffers wb, int par) {
     const RtgSceneDev& J = wb.jobs[job];
     const RayHit h = J.use_bvh ? closest_hit<kStackSmem, kBlock, kCount>(J, o, d, kRayTMin, FLT_MAX, stack, tc)
                                : closest_brute<kCount>(J, o, d, kRayTMin, FLT_MAX, tc);
-    wb.hits[i] = make_float4(h.t, __uint_as_float(h.word), h.b1, h.b2);
+    __stcs(&wb.hits[i], make_float4(h.t, __uint_as_float(h.word), h.b1, h.b2));
     ++rays;
   }
   warp_add_u64(rays, &C->rays);
@@ -268,8 +272,8 @@ __global__ void __launch_bounds__(kBlock, 1024 / kBlock) k_shade(WaveBuffers wb,
     std::uint32_t sample = 0, meta_next = 0, job = 0, seg = 0;
     Pcg rng{0, 0};
     if (i < n) {
-      const float4 a = A[i], b = B[i], c = Cc[i], hv = wb.hits[i];
-      const uint4 r = D[i];
+      const float4 a = __ldcs(&A[i]), b = __ldcs(&B[i]), c = __ldcs(&Cc[i]), hv = __ldcs(&wb.hits[i]);
+      const uint4 r = __ldcs(&D[i]);
       const float3 o = f3(a), d = f3(b);
       sample = __float_as_uint(a.w);
       const std::uint32_t meta = __float_as_uint(b.w);
@@ -370,16 +374,16 @@ __global__ void __launch_bounds__(kBlock, 1024 / kBlock) k_shade(WaveBuffers wb,
     if (fin && (threadIdx.x & 31) == static_cast<unsigned>(__ffs(same) - 1))
       atomicAdd(&wb.seg_prog[seg].done, static_cast<std::uint32_t>(__popc(same)));
     if (cont) {
-      wb.st_a[par ^ 1][cpos] = make_float4(o_next.x, o_next.y, o_next.z, __uint_as_float(sample));
-      wb.st_b[par ^ 1][cpos] = make_float4(d_next.x, d_next.y, d_next.z, __uint_as_float(meta_next));
-      wb.st_c[par ^ 1][cpos] = make_float4(beta.x, beta.y, beta.z, __uint_as_float(seg));
-      wb.st_d[par ^ 1][cpos] = make_uint4(static_cast<std::uint32_t>(rng.state), static_cast<std::uint32_t>(rng.state >> 32),
-                                          static_cast<std::uint32_t>(rng.inc), static_cast<std::uint32_t>(rng.inc >> 32));
+      __stcs(&wb.st_a[par ^ 1][cpos], make_float4(o_next.x, o_next.y, o_next.z, __uint_as_float(sample)));
+      __stcs(&wb.st_b[par ^ 1][cpos], make_float4(d_next.x, d_next.y, d_next.z, __uint_as_float(meta_next)));
+      __stcs(&wb.st_c[par ^ 1][cpos], make_float4(beta.x, beta.y, beta.z, __uint_as_float(seg)));
+      __stcs(&wb.st_d[par ^ 1][cpos], make_uint4(static_cast<std::uint32_t>(rng.state), static_cast<std::uint32_t>(rng.state >> 32),
+                                          static_cast<std::uint32_t>(rng.inc), static_cast<std::uint32_t>(rng.inc >> 32)));
     }
     if (shadow) {
-      wb.sh_a[spos] = make_float4(sh_o.x, sh_o.y, sh_o.z, __uint_as_float(sample));
-      wb.sh_b[spos] = make_float4(sh_d.x, sh_d.y, sh_d.z, sh_tmax);
-      wb.sh_c[spos] = make_float4(sh_c.x, sh_c.y, sh_c.z, __uint_as_float(job));
+      __stcs(&wb.sh_a[spos], make_float4(sh_o.x, sh_o.y, sh_o.z, __uint_as_float(sample)));
+      __stcs(&wb.sh_b[spos], make_float4(sh_d.x, sh_d.y, sh_d.z, sh_tmax));
+      __stcs(&wb.sh_c[spos], make_float4(sh_c.x, sh_c.y, sh_c.z, __uint_as_float(job)));
     }
   }
   warp_add_u64(rr_killed, &C->rr_terminated);
@@ -399,7 +403,7 @@ __global__ void __launch_bounds__(kBlock) k_shadow(WaveBuffers wb) {
     if (base >= n) break;
     const std::uint32_t i = base + (threadIdx.x & 31);
     if (i >= n) continue;
-    const float4 a = wb.sh_a[i], b = wb.sh_b[i], c = wb.sh_c[i];
+    const float4 a = __ldcs(&wb.sh_a[i]), b = __ldcs(&wb.sh_b[i]), c = __ldcs(&wb.sh_c[i]);
     const RtgSceneDev& J = wb.jobs[__float_as_uint(c.w)];
     const float3 o = f3(a), d = f3(b);
     const bool blocked = J.use_bvh ? any_hit4<kStackSmem, kBlock, kCount>(J, o, d, kRayTMin, b.w, stack, tc)
