@@ -112,6 +112,12 @@ typedef struct rtg_host_scene rtg_host_scene;
 
 /* Parse + validate + compile. On RTG_ERR_SCENE the message goes to err (cap bytes). */
 int rtg_compile(const char* scene_json, const char* base_dir, rtg_host_scene** out, char* err, size_t err_cap);
+/* rtg_compile with flags. RTG_COMPILE_DEFER_BVH leaves the BVH out of the host
+ * compile (Bvh::build, src/geometry/bvh.cpp:133-163, is skipped; the view below
+ * then has no nodes): rtg_scene_upload builds the same tree on the GPU instead. */
+#define RTG_COMPILE_DEFER_BVH 1u
+int rtg_compile_flags(const char* scene_json, const char* base_dir, uint32_t flags, rtg_host_scene** out, char* err,
+                      size_t err_cap);
 void rtg_host_scene_free(rtg_host_scene* scene);
 
 /* Read-only view of a compiled scene in the reference's own layout and order
@@ -168,6 +174,29 @@ int rtg_scene_upload(rtg_context* ctx, const rtg_host_scene* scene, rtg_scene_id
  * on the host cores, then copied. out receives n ids (no counterpart in the
  * reference: the batched form). */
 int rtg_scene_upload_batch(rtg_context* ctx, int32_t n, const rtg_host_scene* const* scenes, rtg_scene_id* out);
+/* Uploads a host scene with its BVH built on the GPU: the binned-SAH tree of
+ * Bvh::build (src/geometry/bvh.cpp:28-163), node for node, and the device layout
+ * derived from it there (byte-identical to what rtg_scene_upload makes from a host
+ * build). Host scenes compiled with RTG_COMPILE_DEFER_BVH take this path in
+ * rtg_scene_upload too. It replaces the host build for scenes that are not
+ * resident yet, where that build dominates the time to the first pass. */
+int rtg_scene_upload_gpu_bvh(rtg_context* ctx, const rtg_host_scene* scene, rtg_scene_id* out);
+/* Reads back one part of a scene's device layout (tests and tools; no reference
+ * counterpart). Copies min(cap, size) bytes to out (out may be NULL) and returns
+ * the part's full size in bytes, or a negative error. */
+enum {
+  RTG_LAYOUT_NODES = 0,         /* DevNode, 64 B each (interior nodes, depth-first) */
+  RTG_LAYOUT_NODES4 = 1,        /* DevNode4, 128 B each */
+  RTG_LAYOUT_PRIMS = 2,         /* 3 float4 per slot */
+  RTG_LAYOUT_SLOT_MATERIAL = 3, /* uint32 per slot */
+  RTG_LAYOUT_SLOT_NORMALS = 4,  /* 3 float4 per slot */
+  RTG_LAYOUT_PLANES = 5,
+  RTG_LAYOUT_MATERIALS = 6,
+  RTG_LAYOUT_LIGHTS = 7,
+  RTG_LAYOUT_SLOT_PRIM = 8,     /* uint32 per slot: primitive id */
+  RTG_LAYOUT_ROOTS = 9          /* int32[4]: root link, four-wide root link, slots, built on the GPU */
+};
+int64_t rtg_scene_layout(rtg_context* ctx, rtg_scene_id scene, int32_t part, void* out, uint64_t cap);
 /* The scene file's own render settings. */
 int rtg_scene_settings(rtg_context* ctx, rtg_scene_id scene, rtg_settings* out);
 int rtg_scene_get_info(rtg_context* ctx, rtg_scene_id scene, rtg_scene_info* out);

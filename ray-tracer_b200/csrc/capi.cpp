@@ -187,7 +187,12 @@ int64_t rtg_scene_dump(const char* scene_json, char* out, size_t cap) {
 }
 
 int rtg_compile(const char* scene_json, const char* base_dir, rtg_host_scene** out, char* err, size_t err_cap) {
-  if (!scene_json || !out) return RTG_ERR_INVALID;
+  return rtg_compile_flags(scene_json, base_dir, 0, out, err, err_cap);
+}
+
+int rtg_compile_flags(const char* scene_json, const char* base_dir, uint32_t flags, rtg_host_scene** out, char* err,
+                      size_t err_cap) {
+  if (!scene_json || !out || (flags & ~uint32_t(RTG_COMPILE_DEFER_BVH))) return RTG_ERR_INVALID;
   *out = nullptr;
   auto fail = [&](const char* msg) {
     if (err && err_cap) {
@@ -200,7 +205,7 @@ int rtg_compile(const char* scene_json, const char* base_dir, rtg_host_scene** o
     rtg::SceneDesc d = rtg::parse_scene(scene_json);
     if (base_dir) d.base_dir = base_dir;
     auto hs = std::make_unique<rtg_host_scene>();
-    hs->scene = std::make_shared<const rtg::CompiledScene>(rtg::compile_scene(d));
+    hs->scene = std::make_shared<const rtg::CompiledScene>(rtg::compile_scene(d, !(flags & RTG_COMPILE_DEFER_BVH)));
     const rtg::CompiledScene& s = *hs->scene;
     for (const rtg::Prim& p : s.prims) {
       const rtg::D3 v[6] = {p.a, p.b, p.c, p.n0, p.n1, p.n2};
@@ -312,6 +317,64 @@ int rtg_scene_upload(rtg_context* ctx, const rtg_host_scene* scene, rtg_scene_id
   });
 }
 
+int rtg_scene_upload_gpu_bvh(rtg_context* ctx, const rtg_host_scene* scene, rtg_scene_id* out) {
+  return guarded(ctx, [&]() {
+    if (!scene || !out) throw std::invalid_argument("null argument");
+    *out = ctx->engine->add_scene_gpu_bvh(scene->scene);
+    return RTG_OK;
+  });
+}
+
+int64_t rtg_scene_layout(rtg_context* ctx, rtg_scene_id scene, int32_t part, void* out, uint64_t cap) {
+  int64_t bytes = 0;
+  const int rc = guarded(ctx, [&]() {
+    if (ctx->busy) return RTG_ERR_BUSY;
+    const rtg::GpuScene& g = ctx->engine->scene(scene);
+    const std::int32_t roots[4] = {g.root, g.root4, g.n_slots, g.device_built ? 1 : 0};
+    const void* src = nullptr;
+    bool on_device = true;
+    const int64_t slots = g.n_slots;
+    switch (part) {
+      case RTG_LAYOUT_NODES: src = g.nodes; bytes = int64_t(g.n_interior) * int64_t(sizeof(rtg::DevNode)); break;
+      case RTG_LAYOUT_NODES4: src = g.nodes4; bytes = int64_t(g.n_wide) * int64_t(sizeof(rtg::DevNode4)); break;
+      case RTG_LAYOUT_PRIMS: src = g.prims; bytes = slots * 3 * int64_t(sizeof(float4)); break;
+      case RTG_LAYOUT_SLOT_MATERIAL: src = g.slot_material; bytes = slots * int64_t(sizeof(uint32_t)); break;
+      case RTG_LAYOUT_SLOT_NORMALS: src = g.slot_normals; bytes = slots * 3 * int64_t(sizeof(float4)); break;
+      case RTG_LAYOUT_PLANES: src = g.planes; bytes = int64_t(g.n_planes) * int64_t(sizeof(rtg::DevPlane)); break;
+      case RTG_LAYOUT_MATERIALS:
+        src = g.materials;
+        bytes = int64_t(g.host->materials.size()) * int64_t(sizeof(rtg::DevMaterial));
+        break;
+      case RTG_LAYOUT_LIGHTS: src = g.lights; bytes = int64_t(g.n_lights) * int64_t(sizeof(rtg::DevLight)); break;
+      case RTG_LAYOUT_SLOT_PRIM:
+        src = g.slot_prim.data();
+        on_device = false;
+        bytes = slots * int64_t(sizeof(uint32_t));
+        break;
+      case RTG_LAYOUT_ROOTS:
+        src = roots;
+        on_device = false;
+        bytes = int64_t(sizeof(roots));
+        break;
+      default: throw std::invalid_argument("unknown layout part " + std::to_string(part));
+    }
+    const std::size_t n = static_cast<std::size_t>(std::min<uint64_t>(cap, uint64_t(bytes)));
+    if (out && n) {
+      if (on_device) {
+        cudaStream_t st = ctx->engine->stream();
+        const cudaError_t e1 = cudaMemcpyAsync(out, src, n, cudaMemcpyDeviceToHost, st);
+        const cudaError_t e2 = cudaStreamSynchronize(st);
+        if (e1 != cudaSuccess || e2 != cudaSuccess)
+          throw rtg::CudaFailure(std::string("layout read-back: ") + cudaGetErrorString(e1 != cudaSuccess ? e1 : e2));
+      } else {
+        std::memcpy(out, src, n);
+      }
+    }
+    return RTG_OK;
+  });
+  return rc < 0 ? rc : bytes;
+}
+
 int rtg_scene_upload_batch(rtg_context* ctx, int32_t n, const rtg_host_scene* const* scenes, rtg_scene_id* out) {
   return guarded(ctx, [&]() {
     if (n < 0 || (n > 0 && (!scenes || !out))) throw std::invalid_argument("null argument");
@@ -384,6 +447,7 @@ int rtg_scene_get_info(rtg_context* ctx, rtg_scene_id scene, rtg_scene_info* out
     if (!out) throw std::invalid_argument("null argument");
     const rtg::GpuScene& g = ctx->engine->scene(scene);
     const rtg::BuildInfo& i = g.host->info;
+    const rtg::BvhStats& b = g.bvh;
     *out = rtg_scene_info{};
     out->primitives = g.host->prims.size();
     out->triangles = i.triangles;
@@ -391,13 +455,13 @@ int rtg_scene_get_info(rtg_context* ctx, rtg_scene_id scene, rtg_scene_info* out
     out->planes = i.planes;
     out->degenerate_skipped = i.degenerate_skipped;
     out->lights = i.lights;
-    out->bvh_nodes = i.bvh.nodes;
-    out->bvh_leaves = i.bvh.leaves;
-    out->bvh_max_depth = i.bvh.max_depth;
-    out->bvh_max_leaf = i.bvh.max_leaf;
+    out->bvh_nodes = b.nodes;
+    out->bvh_leaves = b.leaves;
+    out->bvh_max_depth = b.max_depth;
+    out->bvh_max_leaf = b.max_leaf;
     out->device_bytes = g.device_bytes;
-    out->bvh_build_ms = i.bvh.build_ms;
-    out->bvh_sah_cost = i.bvh.sah_cost;
+    out->bvh_build_ms = b.build_ms;
+    out->bvh_sah_cost = b.sah_cost;
     return RTG_OK;
   });
 }

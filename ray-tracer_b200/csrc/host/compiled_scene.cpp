@@ -54,7 +54,7 @@ void CameraFrame::setup(const CameraDesc& d, int width, int height) {
   lens_radius = d.aperture / 2;
 }
 
-CompiledScene compile_scene(const SceneDesc& desc) {
+CompiledScene compile_scene(const SceneDesc& desc, bool build_bvh) {
   CompiledScene s;
   s.settings = desc.render;
   s.background = desc.background;
@@ -157,6 +157,10 @@ CompiledScene compile_scene(const SceneDesc& desc) {
       s.lights.push_back({LightEntry::kEmitter, static_cast<std::uint32_t>(i)});
   s.info.lights = s.lights.size();
 
+  if (!build_bvh) {
+    s.bvh_built = false;
+    return s;
+  }
   std::vector<Box> boxes;
   boxes.reserve(s.prims.size());
   for (const Prim& p : s.prims) boxes.push_back(p.bounds());

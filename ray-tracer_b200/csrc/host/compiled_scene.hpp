@@ -64,9 +64,12 @@ struct CompiledScene {
   std::vector<PointLight> point_lights;
   std::vector<LightEntry> lights;
   BinaryBvh bvh;
+  bool bvh_built = true;  // false: compiled without the BVH (built on the GPU at upload)
   BuildInfo info;
 };
 
-CompiledScene compile_scene(const SceneDesc& desc);
+// build_bvh = false leaves `bvh` empty: the device build (bvh_gpu.h) makes the
+// same tree on the GPU when the scene is uploaded.
+CompiledScene compile_scene(const SceneDesc& desc, bool build_bvh = true);
 
 }  // namespace rtg

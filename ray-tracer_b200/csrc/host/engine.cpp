@@ -1,5 +1,7 @@
 #include "host/engine.hpp"
 
+#include "device/bvh_gpu.h"
+
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -183,12 +185,21 @@ void Engine::reset_wave() {
 }
 
 int Engine::add_scene(std::shared_ptr<const CompiledScene> scene) {
+  if (!scene->bvh_built) return add_scene_gpu_bvh(std::move(scene));
   FlatScene flat = flatten(*scene);
   return add_flat(std::move(scene), std::move(flat));
 }
 
 std::vector<int> Engine::add_scenes(const std::vector<std::shared_ptr<const CompiledScene>>& scenes) {
   // Flatten on all host cores (one scene per task), then copy in order.
+  for (const auto& sc : scenes)
+    if (!sc->bvh_built) {
+      // Scenes without a host BVH are built on the GPU, one after another.
+      std::vector<int> ids;
+      ids.reserve(scenes.size());
+      for (const auto& x : scenes) ids.push_back(add_scene(x));
+      return ids;
+    }
   std::vector<FlatScene> flats(scenes.size());
   std::atomic<std::size_t> next{0};
   std::exception_ptr failed;
@@ -223,6 +234,8 @@ int Engine::add_flat(std::shared_ptr<const CompiledScene> scene, FlatScene flat)
   gs->n_planes = static_cast<std::int32_t>(flat.planes.size());
   gs->n_lights = static_cast<std::int32_t>(flat.lights.size());
   gs->root4 = flat.root4;
+  gs->n_interior = static_cast<std::int32_t>(flat.nodes.size());
+  gs->n_wide = static_cast<std::int32_t>(flat.nodes4.size());
   // One device allocation and one copy per scene, through a pinned staging
   // buffer: the copy runs while the caller flattens the next scene (two buffers
   // alternate), and the flattened vectors can go at once.
@@ -241,18 +254,11 @@ int Engine::add_flat(std::shared_ptr<const CompiledScene> scene, FlatScene flat)
   }
   void* block = nullptr;
   CK(cudaMallocFromPoolAsync(&block, total, pool_, stream_));
-  const int b = upload_next_;
-  upload_next_ ^= 1;
-  if (upload_pending_[b]) CK(cudaEventSynchronize(upload_ev_[b]));
-  if (upload_cap_[b] < total) {
-    if (upload_host_[b]) CK(cudaFreeHost(upload_host_[b]));
-    upload_host_[b] = nullptr;
-    CK(cudaMallocHost(reinterpret_cast<void**>(&upload_host_[b]), total));
-    upload_cap_[b] = total;
-  }
+  int b = 0;
+  unsigned char* host = upload_staging(total, b);
   for (const Part& p : parts)
-    if (p.bytes) std::memcpy(upload_host_[b] + p.at, p.src, p.bytes);
-  CK(cudaMemcpyAsync(block, upload_host_[b], total, cudaMemcpyHostToDevice, stream_));
+    if (p.bytes) std::memcpy(host + p.at, p.src, p.bytes);
+  CK(cudaMemcpyAsync(block, host, total, cudaMemcpyHostToDevice, stream_));
   CK(cudaEventRecord(upload_ev_[b], stream_));
   upload_pending_[b] = true;
   auto at = [&](int k) { return static_cast<void*>(static_cast<unsigned char*>(block) + parts[k].at); };
@@ -267,6 +273,153 @@ int Engine::add_flat(std::shared_ptr<const CompiledScene> scene, FlatScene flat)
   gs->lights = static_cast<DevLight*>(at(7));
   gs->device_bytes = total;
   gs->slot_prim = std::move(flat.slot_prim);
+  gs->bvh = scene->info.bvh;
+  gs->host = std::move(scene);
+  const int id = next_scene_++;
+  scenes_[id] = std::move(gs);
+  return id;
+}
+
+unsigned char* Engine::upload_staging(std::size_t bytes, int& b) {
+  b = upload_next_;
+  upload_next_ ^= 1;
+  if (upload_pending_[b]) CK(cudaEventSynchronize(upload_ev_[b]));
+  upload_pending_[b] = false;
+  if (upload_cap_[b] < bytes) {
+    if (upload_host_[b]) CK(cudaFreeHost(upload_host_[b]));
+    upload_host_[b] = nullptr;
+    upload_cap_[b] = 0;
+    CK(cudaMallocHost(reinterpret_cast<void**>(&upload_host_[b]), bytes));
+    upload_cap_[b] = bytes;
+  }
+  return upload_host_[b];
+}
+
+int Engine::add_scene_gpu_bvh(std::shared_ptr<const CompiledScene> scene) {
+  CK(cudaSetDevice(device_));
+  const CompiledScene& s = *scene;
+  if (s.prims.size() > kIdMask) throw std::runtime_error("too many primitives for the device layout");
+  const std::size_t np = s.prims.size();
+  FlatScene tables;
+  flatten_tables(s, tables);
+
+  // Inputs in primitive order, converted on the host cores into one pinned buffer:
+  // boxes (double), slot rows, normals, material words, the ids of primitives
+  // with a usable box, then the tables. One copy takes them all to the GPU.
+  auto pad = [](std::size_t bytes) { return (std::max<std::size_t>(bytes, 1) + 255) & ~std::size_t(255); };
+  const std::size_t in_bytes[8] = {np * 6 * sizeof(double), np * 3 * sizeof(float4), np * 3 * sizeof(float4),
+                                   np * sizeof(std::uint32_t), np * sizeof(std::uint32_t),
+                                   tables.planes.size() * sizeof(DevPlane),
+                                   tables.materials.size() * sizeof(DevMaterial),
+                                   tables.lights.size() * sizeof(DevLight)};
+  std::size_t in_at[9];
+  in_at[0] = 0;
+  for (int k = 0; k < 8; ++k) in_at[k + 1] = in_at[k] + pad(in_bytes[k]);
+  const std::size_t staged = in_at[8];
+  int b = 0;
+  unsigned char* host = upload_staging(staged, b);
+  auto* boxes = reinterpret_cast<double*>(host + in_at[0]);
+  auto* rows = reinterpret_cast<float4*>(host + in_at[1]);
+  auto* normals = reinterpret_cast<float4*>(host + in_at[2]);
+  auto* material = reinterpret_cast<std::uint32_t*>(host + in_at[3]);
+  auto* items = reinterpret_cast<std::uint32_t*>(host + in_at[4]);
+  std::vector<std::uint8_t> usable(np);
+  {
+    const std::size_t workers = std::min<std::size_t>({16, std::max(1u, std::thread::hardware_concurrency()),
+                                                       (np + 16383) / 16384});
+    auto body = [&](std::size_t i0, std::size_t i1) {
+      for (std::size_t i = i0; i < i1; ++i) {
+        const Prim& p = s.prims[i];
+        const Box bx = p.bounds();
+        double* d = boxes + 6 * i;
+        d[0] = bx.lo.x; d[1] = bx.lo.y; d[2] = bx.lo.z;
+        d[3] = bx.hi.x; d[4] = bx.hi.y; d[5] = bx.hi.z;
+        usable[i] = !(bx.empty() || !bx.lo.finite() || !bx.hi.finite());
+        slot_record(p, static_cast<std::uint32_t>(i), rows + 3 * i, normals + 3 * i, material[i]);
+      }
+    };
+    std::vector<std::thread> pool;
+    const std::size_t chunk = workers > 1 ? (np + workers - 1) / workers : np;
+    for (std::size_t w = 1; w < workers; ++w)
+      pool.emplace_back(body, std::min(np, w * chunk), std::min(np, (w + 1) * chunk));
+    body(0, std::min(np, chunk));
+    for (auto& t : pool) t.join();
+  }
+  std::uint32_t n_items = 0;
+  for (std::size_t i = 0; i < np; ++i)
+    if (usable[i]) items[n_items++] = static_cast<std::uint32_t>(i);
+  std::memcpy(host + in_at[5], tables.planes.data(), in_bytes[5]);
+  std::memcpy(host + in_at[6], tables.materials.data(), in_bytes[6]);
+  std::memcpy(host + in_at[7], tables.lights.data(), in_bytes[7]);
+
+  // Device copy of the inputs plus room for the slot -> primitive map.
+  void* in_block = nullptr;
+  CK(cudaMallocFromPoolAsync(&in_block, staged + pad(np * sizeof(std::uint32_t)), pool_, stream_));
+  struct FreeInput {
+    void* p;
+    cudaStream_t s;
+    ~FreeInput() { cudaFreeAsync(p, s); }
+  } free_input{in_block, stream_};
+  auto* dev_in = static_cast<unsigned char*>(in_block);
+  CK(cudaMemcpyAsync(dev_in, host, staged, cudaMemcpyHostToDevice, stream_));
+  CK(cudaEventRecord(upload_ev_[b], stream_));
+  upload_pending_[b] = true;
+  auto* order = reinterpret_cast<std::uint32_t*>(dev_in + staged);
+
+  GpuBvhInput in;
+  in.n_items = n_items;
+  in.boxes = reinterpret_cast<const double*>(dev_in + in_at[0]);
+  in.rows = reinterpret_cast<const float4*>(dev_in + in_at[1]);
+  in.normals = reinterpret_cast<const float4*>(dev_in + in_at[2]);
+  in.material = reinterpret_cast<const std::uint32_t*>(dev_in + in_at[3]);
+  in.items = reinterpret_cast<const std::uint32_t*>(dev_in + in_at[4]);
+  GpuBvhBuilder builder(stream_, pool_);
+  const GpuBvhCounts c = builder.build(in);
+
+  // The scene's arrays, in add_flat's order, in one allocation.
+  const std::size_t part_bytes[8] = {std::size_t(c.interior) * sizeof(DevNode), std::size_t(c.wide) * sizeof(DevNode4),
+                                     std::size_t(n_items) * 3 * sizeof(float4), std::size_t(n_items) * sizeof(std::uint32_t),
+                                     std::size_t(n_items) * 3 * sizeof(float4), in_bytes[5], in_bytes[6], in_bytes[7]};
+  std::size_t at[8], total = 0;
+  for (int k = 0; k < 8; ++k) {
+    at[k] = total;
+    total += pad(part_bytes[k]);
+  }
+  void* block = nullptr;
+  CK(cudaMallocFromPoolAsync(&block, total, pool_, stream_));
+  auto* dst = static_cast<unsigned char*>(block);
+  auto gs = std::make_unique<GpuScene>();
+  gs->block = block;
+  gs->nodes = reinterpret_cast<DevNode*>(dst + at[0]);
+  gs->nodes4 = reinterpret_cast<DevNode4*>(dst + at[1]);
+  gs->prims = reinterpret_cast<float4*>(dst + at[2]);
+  gs->slot_material = reinterpret_cast<std::uint32_t*>(dst + at[3]);
+  gs->slot_normals = reinterpret_cast<float4*>(dst + at[4]);
+  gs->planes = reinterpret_cast<DevPlane*>(dst + at[5]);
+  gs->materials = reinterpret_cast<DevMaterial*>(dst + at[6]);
+  gs->lights = reinterpret_cast<DevLight*>(dst + at[7]);
+  builder.emit(in, gs->nodes, gs->nodes4, gs->prims, gs->slot_material, gs->slot_normals, order);
+  for (int k = 5; k < 8; ++k)
+    if (part_bytes[k]) CK(cudaMemcpyAsync(dst + at[k], dev_in + in_at[k], part_bytes[k], cudaMemcpyDeviceToDevice, stream_));
+  gs->slot_prim.resize(n_items);
+  if (n_items)
+    CK(cudaMemcpyAsync(gs->slot_prim.data(), order, n_items * sizeof(std::uint32_t), cudaMemcpyDeviceToHost, stream_));
+  CK(cudaStreamSynchronize(stream_));
+
+  gs->root = n_items ? c.root : kNoRoot;
+  gs->root4 = n_items ? c.root4 : kNoRoot;
+  gs->n_slots = static_cast<std::int32_t>(n_items);
+  gs->n_interior = c.interior;
+  gs->n_wide = c.wide;
+  gs->n_planes = static_cast<std::int32_t>(tables.planes.size());
+  gs->n_lights = static_cast<std::int32_t>(tables.lights.size());
+  gs->device_bytes = total;
+  gs->bvh.nodes = static_cast<std::size_t>(c.nodes);
+  gs->bvh.leaves = static_cast<std::size_t>(c.leaves);
+  gs->bvh.max_depth = static_cast<std::size_t>(c.max_depth);
+  gs->bvh.max_leaf = static_cast<std::size_t>(c.max_leaf);
+  gs->bvh.build_ms = c.build_ms;
+  gs->device_built = true;
   gs->host = std::move(scene);
   const int id = next_scene_++;
   scenes_[id] = std::move(gs);

@@ -70,6 +70,7 @@ struct GpuScene {
   std::vector<std::uint32_t> slot_prim;  // slot -> primitive id (ray API)
   std::int32_t root = kNoRoot;
   std::int32_t n_slots = 0, n_planes = 0, n_lights = 0;
+  std::int32_t n_interior = 0, n_wide = 0;  // DevNode / DevNode4 records
   void* block = nullptr;       // one device allocation holding the arrays below
   DevNode* nodes = nullptr;
   DevNode4* nodes4 = nullptr;  // four-wide copy of the tree (any-hit queries)
@@ -84,6 +85,8 @@ struct GpuScene {
   double* planes64 = nullptr;
   std::size_t device_bytes = 0;
   int jobs_open = 0;           // jobs in the wavefront that use this scene
+  BvhStats bvh;                // of the tree on the device (host or device build)
+  bool device_built = false;   // the BVH was built on the GPU
 };
 
 // Per-job device framebuffer.
@@ -129,7 +132,12 @@ class Engine {
   cudaStream_t stream() const { return stream_; }
   EngineConfig& config() { return cfg_; }
 
+  // Host-built scenes are flattened on the host; scenes compiled without a BVH
+  // (compile_scene(desc, false)) get it built on the GPU (add_scene_gpu_bvh).
   int add_scene(std::shared_ptr<const CompiledScene> scene);
+  // Builds the scene's BVH on the GPU (device/bvh_gpu.h), whether or not the host
+  // compile holds one, and derives the device layout there.
+  int add_scene_gpu_bvh(std::shared_ptr<const CompiledScene> scene);
   // Several scenes at once: flattened in parallel on the host, then copied.
   std::vector<int> add_scenes(const std::vector<std::shared_ptr<const CompiledScene>>& scenes);
   void release_scene(int id);
@@ -227,6 +235,9 @@ class Engine {
   };
 
   int add_flat(std::shared_ptr<const CompiledScene> scene, FlatScene flat);
+  // One of the two pinned upload buffers, grown to `bytes`, once its previous copy
+  // is done; the caller records upload_ev_[b] after queuing its copy from it.
+  unsigned char* upload_staging(std::size_t bytes, int& b);
   void ensure_wave();
   GpuFrame make_frame(int w, int h);
   void free_frame(GpuFrame& f);

@@ -104,7 +104,9 @@ DevMaterial material_record(const Material& m) {
 // Collapses the binary tree into four-child nodes: starting from an interior
 // node's two children, the interior child with the largest surface area is
 // replaced by its own children until there are four (or only leaves). Leaves
-// keep their slot ranges. Nodes are numbered in creation order from the root.
+// keep their slot ranges. Four-wide nodes are numbered in the depth-first order
+// of the binary nodes they start from, which the device build computes with a
+// scan instead of a serial walk.
 void build_wide(const BinaryBvh& bvh, const std::vector<FBox>& fbox, FlatScene& f) {
   f.nodes4.clear();
   f.depth4 = 0;
@@ -117,25 +119,23 @@ void build_wide(const BinaryBvh& bvh, const std::vector<FBox>& fbox, FlatScene& 
     return;
   }
   // Topology first (serial, indices only), then the boxes in parallel.
-  struct Item {
-    std::size_t bin;   // binary interior node
-    std::size_t slot;  // its four-wide node
-    int depth;
-  };
   struct Kids {
     std::uint32_t bin[4];
-    std::int32_t link[4];
     int n;
   };
-  std::vector<Kids> kids_of(1);
-  std::vector<Item> work{{0, 0, 1}};
+  struct Root {
+    std::uint32_t bin;  // the binary interior node this four-wide node starts from
+    Kids kids;
+  };
+  std::vector<Root> roots;
+  std::vector<std::pair<std::uint32_t, int>> work{{0u, 1}};
   while (!work.empty()) {
-    const Item it = work.back();
+    const auto [bin, depth] = work.back();
     work.pop_back();
-    f.depth4 = std::max(f.depth4, it.depth);
+    f.depth4 = std::max(f.depth4, depth);
     Kids k{};
-    k.bin[k.n++] = static_cast<std::uint32_t>(it.bin + 1);
-    k.bin[k.n++] = bvh.nodes[it.bin].first;
+    k.bin[k.n++] = bin + 1;
+    k.bin[k.n++] = bvh.nodes[bin].first;
     while (k.n < 4) {
       int pick = -1;
       double pick_area = -1;
@@ -153,30 +153,23 @@ void build_wide(const BinaryBvh& bvh, const std::vector<FBox>& fbox, FlatScene& 
       k.bin[pick] = b + 1;
       k.bin[k.n++] = bvh.nodes[b].first;
     }
-    for (int q = 0; q < 4; ++q) {
-      if (q >= k.n) {
-        k.link[q] = kNoChild;
-        continue;
-      }
-      const BinaryNode& c = bvh.nodes[k.bin[q]];
-      if (c.leaf()) {
-        k.link[q] = ~static_cast<std::int32_t>(c.first);
-      } else {
-        k.link[q] = static_cast<std::int32_t>(kids_of.size());
-        work.push_back({k.bin[q], kids_of.size(), it.depth + 1});
-        kids_of.emplace_back();
-      }
-    }
-    kids_of[it.slot] = k;
+    for (int q = 0; q < k.n; ++q)
+      if (!bvh.nodes[k.bin[q]].leaf()) work.push_back({k.bin[q], depth + 1});
+    roots.push_back({bin, k});
   }
-  f.nodes4.resize(kids_of.size());
-  parallel_chunks(kids_of.size(), [&](std::size_t i0, std::size_t i1) {
+  std::sort(roots.begin(), roots.end(), [](const Root& x, const Root& y) { return x.bin < y.bin; });
+  std::vector<std::int32_t> wide_index(bvh.nodes.size(), -1);
+  for (std::size_t i = 0; i < roots.size(); ++i) wide_index[roots[i].bin] = static_cast<std::int32_t>(i);
+  f.nodes4.resize(roots.size());
+  parallel_chunks(roots.size(), [&](std::size_t i0, std::size_t i1) {
     for (std::size_t i = i0; i < i1; ++i) {
-      const Kids& k = kids_of[i];
+      const Kids& k = roots[i].kids;
       float lo[3][4], hi[3][4];
+      std::int32_t link[4];
       for (int q = 0; q < 4; ++q) {
         if (q >= k.n) {
           for (int a = 0; a < 3; ++a) lo[a][q] = hi[a][q] = 0.f;
+          link[q] = kNoChild;
           continue;
         }
         const FBox& b = fbox[k.bin[q]];
@@ -184,6 +177,8 @@ void build_wide(const BinaryBvh& bvh, const std::vector<FBox>& fbox, FlatScene& 
           lo[a][q] = b.lo[a];
           hi[a][q] = b.hi[a];
         }
+        const BinaryNode& c = bvh.nodes[k.bin[q]];
+        link[q] = c.leaf() ? ~static_cast<std::int32_t>(c.first) : wide_index[k.bin[q]];
       }
       DevNode4& d = f.nodes4[i];
       d.lo_x = make_float4(lo[0][0], lo[0][1], lo[0][2], lo[0][3]);
@@ -192,7 +187,7 @@ void build_wide(const BinaryBvh& bvh, const std::vector<FBox>& fbox, FlatScene& 
       d.hi_y = make_float4(hi[1][0], hi[1][1], hi[1][2], hi[1][3]);
       d.lo_z = make_float4(lo[2][0], lo[2][1], lo[2][2], lo[2][3]);
       d.hi_z = make_float4(hi[2][0], hi[2][1], hi[2][2], hi[2][3]);
-      d.link = make_int4(k.link[0], k.link[1], k.link[2], k.link[3]);
+      d.link = make_int4(link[0], link[1], link[2], link[3]);
       d.pad = make_int4(0, 0, 0, 0);
     }
   });
@@ -203,76 +198,31 @@ void build_wide(const BinaryBvh& bvh, const std::vector<FBox>& fbox, FlatScene& 
 
 }  // namespace
 
-FlatScene flatten(const CompiledScene& s) {
-  FlatScene f;
-  const BinaryBvh& bvh = s.bvh;
-
-  // Primitive slots in leaf order; mark the last slot of every leaf.
-  const std::size_t nslots = bvh.order.size();
-  if (s.prims.size() > kIdMask) throw std::runtime_error("too many primitives for the device layout");
-  std::vector<std::uint8_t> last(nslots, 0);
-  for (const BinaryNode& n : bvh.nodes)
-    if (n.leaf()) last[n.first + n.count - 1] = 1;
-  f.prims.resize(nslots * 3);
-  f.slot_material.resize(nslots);
-  f.slot_normals.resize(nslots * 3, make_float4(0.f, 0.f, 0.f, 0.f));
-  f.slot_prim.resize(nslots);
-  parallel_chunks(nslots, [&](std::size_t k0, std::size_t k1) {
-  for (std::size_t k = k0; k < k1; ++k) {
-    const std::uint32_t id = bvh.order[k];
-    const Prim& p = s.prims[id];
-    std::uint32_t word = id | (last[k] ? kLastInLeaf : 0u);
-    if (p.kind == Prim::kSphere) {
-      word |= kSphereBit;
-      f.prims[3 * k] = f4(p.a, float_of(word));
-      f.prims[3 * k + 1] = make_float4(float(p.b.x), float(p.b.x * p.b.x), 0.f, 0.f);
-      f.prims[3 * k + 2] = make_float4(0.f, 0.f, 0.f, 0.f);
-    } else {
-      f.prims[3 * k] = f4(p.a, float_of(word));
-      f.prims[3 * k + 1] = f4(p.b - p.a);
-      f.prims[3 * k + 2] = f4(p.c - p.a);
-      if (p.smooth) {
-        f.slot_normals[3 * k] = f4(p.n0);
-        f.slot_normals[3 * k + 1] = f4(p.n1);
-        f.slot_normals[3 * k + 2] = f4(p.n2);
-      }
+void slot_record(const Prim& p, std::uint32_t id, float4* rows, float4* normals, std::uint32_t& material) {
+  std::uint32_t word = id;
+  normals[0] = normals[1] = normals[2] = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (p.kind == Prim::kSphere) {
+    word |= kSphereBit;
+    rows[0] = f4(p.a, float_of(word));
+    rows[1] = make_float4(float(p.b.x), float(p.b.x * p.b.x), 0.f, 0.f);
+    rows[2] = make_float4(0.f, 0.f, 0.f, 0.f);
+  } else {
+    rows[0] = f4(p.a, float_of(word));
+    rows[1] = f4(p.b - p.a);
+    rows[2] = f4(p.c - p.a);
+    if (p.smooth) {
+      normals[0] = f4(p.n0);
+      normals[1] = f4(p.n1);
+      normals[2] = f4(p.n2);
     }
-    f.slot_material[k] = p.material | ((p.kind == Prim::kTriangle && p.smooth) ? 0x80000000u : 0u);
-    f.slot_prim[k] = id;
   }
-  });
+  material = p.material | ((p.kind == Prim::kTriangle && p.smooth) ? 0x80000000u : 0u);
+}
 
-  // Interior nodes in depth-first order -> DevNode indices.
-  std::vector<std::int32_t> dev_index(bvh.nodes.size(), -1);
-  std::int32_t ninterior = 0;
-  for (std::size_t i = 0; i < bvh.nodes.size(); ++i)
-    if (!bvh.nodes[i].leaf()) dev_index[i] = ninterior++;
-  auto link_of = [&](std::size_t child) -> std::int32_t {
-    const BinaryNode& c = bvh.nodes[child];
-    return c.leaf() ? ~static_cast<std::int32_t>(c.first) : dev_index[child];
-  };
-  // Every node's box rounded outward once; both device trees copy from here.
-  std::vector<FBox> fbox(bvh.nodes.size());
-  parallel_chunks(bvh.nodes.size(), [&](std::size_t i0, std::size_t i1) {
-    for (std::size_t i = i0; i < i1; ++i) fbox[i] = outward(bvh.nodes[i].box);
-  });
-  f.nodes.resize(static_cast<std::size_t>(ninterior));
-  parallel_chunks(bvh.nodes.size(), [&](std::size_t i0, std::size_t i1) {
-  for (std::size_t i = i0; i < i1; ++i) {
-    const BinaryNode& n = bvh.nodes[i];
-    if (n.leaf()) continue;
-    const FBox& L = fbox[i + 1];
-    const FBox& R = fbox[n.first];
-    DevNode& d = f.nodes[static_cast<std::size_t>(dev_index[i])];
-    d.xy0 = make_float4(L.lo[0], L.hi[0], L.lo[1], L.hi[1]);
-    d.xy1 = make_float4(R.lo[0], R.hi[0], R.lo[1], R.hi[1]);
-    d.zz = make_float4(L.lo[2], L.hi[2], R.lo[2], R.hi[2]);
-    d.link = make_int4(link_of(i + 1), link_of(n.first), static_cast<int>(n.axis) << 16, 0);
-  }
-  });
-  if (!bvh.nodes.empty()) f.root = link_of(0);
-  build_wide(bvh, fbox, f);
-
+void flatten_tables(const CompiledScene& s, FlatScene& f) {
+  f.planes.clear();
+  f.materials.clear();
+  f.lights.clear();
   for (const PlanePrim& pl : s.planes) {
     DevPlane dp;
     dp.point = f4(pl.point, float_of(pl.material));
@@ -306,6 +256,63 @@ FlatScene flatten(const CompiledScene& s) {
     }
     f.lights.push_back(L);
   }
+}
+
+FlatScene flatten(const CompiledScene& s) {
+  FlatScene f;
+  const BinaryBvh& bvh = s.bvh;
+
+  // Primitive slots in leaf order; mark the last slot of every leaf.
+  const std::size_t nslots = bvh.order.size();
+  if (s.prims.size() > kIdMask) throw std::runtime_error("too many primitives for the device layout");
+  std::vector<std::uint8_t> last(nslots, 0);
+  for (const BinaryNode& n : bvh.nodes)
+    if (n.leaf()) last[n.first + n.count - 1] = 1;
+  f.prims.resize(nslots * 3);
+  f.slot_material.resize(nslots);
+  f.slot_normals.resize(nslots * 3, make_float4(0.f, 0.f, 0.f, 0.f));
+  f.slot_prim.resize(nslots);
+  parallel_chunks(nslots, [&](std::size_t k0, std::size_t k1) {
+    for (std::size_t k = k0; k < k1; ++k) {
+      const std::uint32_t id = bvh.order[k];
+      slot_record(s.prims[id], id, &f.prims[3 * k], &f.slot_normals[3 * k], f.slot_material[k]);
+      if (last[k]) f.prims[3 * k].w = float_of(bits_of(f.prims[3 * k].w) | kLastInLeaf);
+      f.slot_prim[k] = id;
+    }
+  });
+
+  // Interior nodes in depth-first order -> DevNode indices.
+  std::vector<std::int32_t> dev_index(bvh.nodes.size(), -1);
+  std::int32_t ninterior = 0;
+  for (std::size_t i = 0; i < bvh.nodes.size(); ++i)
+    if (!bvh.nodes[i].leaf()) dev_index[i] = ninterior++;
+  auto link_of = [&](std::size_t child) -> std::int32_t {
+    const BinaryNode& c = bvh.nodes[child];
+    return c.leaf() ? ~static_cast<std::int32_t>(c.first) : dev_index[child];
+  };
+  // Every node's box rounded outward once; both device trees copy from here.
+  std::vector<FBox> fbox(bvh.nodes.size());
+  parallel_chunks(bvh.nodes.size(), [&](std::size_t i0, std::size_t i1) {
+    for (std::size_t i = i0; i < i1; ++i) fbox[i] = outward(bvh.nodes[i].box);
+  });
+  f.nodes.resize(static_cast<std::size_t>(ninterior));
+  parallel_chunks(bvh.nodes.size(), [&](std::size_t i0, std::size_t i1) {
+  for (std::size_t i = i0; i < i1; ++i) {
+    const BinaryNode& n = bvh.nodes[i];
+    if (n.leaf()) continue;
+    const FBox& L = fbox[i + 1];
+    const FBox& R = fbox[n.first];
+    DevNode& d = f.nodes[static_cast<std::size_t>(dev_index[i])];
+    d.xy0 = make_float4(L.lo[0], L.hi[0], L.lo[1], L.hi[1]);
+    d.xy1 = make_float4(R.lo[0], R.hi[0], R.lo[1], R.hi[1]);
+    d.zz = make_float4(L.lo[2], L.hi[2], R.lo[2], R.hi[2]);
+    d.link = make_int4(link_of(i + 1), link_of(n.first), static_cast<int>(n.axis) << 16, 0);
+  }
+  });
+  if (!bvh.nodes.empty()) f.root = link_of(0);
+  build_wide(bvh, fbox, f);
+
+  flatten_tables(s, f);
   return f;
 }
 

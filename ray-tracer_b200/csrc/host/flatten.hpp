@@ -34,6 +34,15 @@ struct FlatScene {
 
 FlatScene flatten(const CompiledScene& s);
 
+// One primitive's device records, indexed by primitive rather than slot: its three
+// slot rows (id bits set, no last-in-leaf bit), its three vertex normals (zero
+// unless smooth) and its material word. flatten() writes these in leaf order; the
+// device BVH build uploads them in primitive order and gathers them there.
+void slot_record(const Prim& p, std::uint32_t id, float4* rows, float4* normals, std::uint32_t& material);
+
+// The planes, materials and light list of a scene (f.planes, f.materials, f.lights).
+void flatten_tables(const CompiledScene& s, FlatScene& f);
+
 // Camera (set up for r's resolution), settings and background of a descriptor;
 // pointers and pass fields are filled in by the engine.
 void describe(const CompiledScene& s, const RenderSettings& r, RtgSceneDev& d);

@@ -118,6 +118,8 @@ _SIGNATURES = {
     "rtg_validate": (C.c_char_p, [C.c_char_p]),
     "rtg_scene_dump": (C.c_int64, [C.c_char_p, C.c_char_p, C.c_size_t]),
     "rtg_compile": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(C.c_void_p), C.c_char_p, C.c_size_t]),
+    "rtg_compile_flags": (C.c_int, [C.c_char_p, C.c_char_p, C.c_uint32, C.POINTER(C.c_void_p), C.c_char_p,
+                                    C.c_size_t]),
     "rtg_host_scene_free": (None, [C.c_void_p]),
     "rtg_host_scene_view": (C.c_int, [C.c_void_p, C.POINTER(_SceneView)]),
     "rtg_context_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
@@ -128,6 +130,8 @@ _SIGNATURES = {
     "rtg_scene_load_file": (C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_int32)]),
     "rtg_scene_upload": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int32)]),
     "rtg_scene_upload_batch": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_void_p), C.POINTER(C.c_int32)]),
+    "rtg_scene_upload_gpu_bvh": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int32)]),
+    "rtg_scene_layout": (C.c_int64, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_uint64]),
     "rtg_scene_settings": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(_Settings)]),
     "rtg_scene_get_info": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(_SceneInfo)]),
     "rtg_scene_release": (C.c_int, [C.c_void_p, C.c_int32]),
@@ -316,11 +320,24 @@ class HostScene:
         }
 
 
-def parse_scene(scene_json: str, base_dir: Optional[str] = None) -> HostScene:
-    """Parse + validate + compile a scene (raises SceneError with the field path)."""
+COMPILE_DEFER_BVH = 1
+# Parts of a scene's device layout (rtg_scene_layout): name -> (part, dtype, record width).
+LAYOUT_PARTS = {
+    "nodes": (0, np.float32, 16), "nodes4": (1, np.float32, 32), "prims": (2, np.float32, 12),
+    "slot_material": (3, np.uint32, 1), "slot_normals": (4, np.float32, 12), "planes": (5, np.float32, 8),
+    "materials": (6, np.float32, 16), "lights": (7, np.float32, 20), "slot_prim": (8, np.uint32, 1),
+    "roots": (9, np.int32, 4),
+}
+
+
+def parse_scene(scene_json: str, base_dir: Optional[str] = None, defer_bvh: bool = False) -> HostScene:
+    """Parse + validate + compile a scene (raises SceneError with the field path).
+
+    defer_bvh skips the host BVH build; uploading the scene then builds it on the GPU."""
     h = C.c_void_p()
     err = C.create_string_buffer(1024)
-    rc = lib().rtg_compile(scene_json.encode(), base_dir.encode() if base_dir else None, C.byref(h), err, 1024)
+    rc = lib().rtg_compile_flags(scene_json.encode(), base_dir.encode() if base_dir else None,
+                                 COMPILE_DEFER_BVH if defer_bvh else 0, C.byref(h), err, 1024)
     if rc != RTG_OK:
         raise SceneError(err.value.decode())
     return HostScene(h.value)
@@ -376,6 +393,24 @@ class Context:
         sid = C.c_int32()
         self._check(lib().rtg_scene_upload(self._h, scene.handle, C.byref(sid)))
         return sid.value
+
+    def upload_gpu_bvh(self, scene: HostScene) -> int:
+        """Uploads a host scene with its BVH built on the GPU (the same tree as the host build)."""
+        sid = C.c_int32()
+        self._check(lib().rtg_scene_upload_gpu_bvh(self._h, scene.handle, C.byref(sid)))
+        return sid.value
+
+    def scene_layout(self, scene_id: int, part: str) -> np.ndarray:
+        """One part of a scene's device layout, read back (records as rows; raw words)."""
+        code, dtype, width = LAYOUT_PARTS[part]
+        n = lib().rtg_scene_layout(self._h, scene_id, code, None, 0)
+        if n < 0:
+            self._check(int(n))
+        out = np.zeros(n // 4, dtype=dtype)
+        got = lib().rtg_scene_layout(self._h, scene_id, code, out.ctypes.data_as(C.c_void_p), n)
+        if got < 0:
+            self._check(int(got))
+        return out.reshape(-1, width)
 
     def upload_many(self, scenes: list[HostScene]) -> list[int]:
         """Uploads several host scenes at once (flattened in parallel)."""
