@@ -49,6 +49,8 @@ def args():
     p.add_argument("--serve-seconds", type=float, default=10.0,
                    help="length of the serving run (Poisson arrivals over 32 resident scenes of the mix)")
     p.add_argument("--no-serve", action="store_true", help="skip the serving run")
+    p.add_argument("--no-cold", action="store_true",
+                   help="skip the cold-scene time-to-first-pass comparison (BVH built on the host vs the GPU)")
     p.add_argument("--no-autotune", action="store_true", help="keep the default pool and block size")
     p.add_argument("--pool", type=int, default=0, help="path slots (implies --no-autotune)")
     p.add_argument("--block", type=int, default=0, help="threads per block: 64, 128, 256 (implies --no-autotune)")
@@ -259,6 +261,46 @@ def extend_traffic(pool_paths: int, rays_per_launch: float):
     return per_ray * rays_per_launch, f"ncu capture, {d['launches_captured']} launches ({os.path.basename(p)})"
 
 
+def cold_scene_ttfp(ctx, named_scenes, reps=3):
+    """Time to first pass for scenes that are not resident yet: scene JSON text in,
+    a 128x128, 4 spp, depth 4 preview image on the host out. Two ways: the host
+    compile builds the BVH and the upload flattens it (host_bvh), or the compile
+    skips the BVH and the upload builds it on the GPU (gpu_bvh). Medians over
+    `reps` alternating runs; the phases are compile, upload and first pass (render
+    plus image read-back)."""
+    import numpy as np
+    import rtg
+
+    out = {}
+    for name, scene in named_scenes:
+        text = json.dumps(scene)
+        runs = {"host_bvh": [], "gpu_bvh": []}
+        prims = None
+        for _ in range(reps):
+            for arm, defer in (("host_bvh", False), ("gpu_bvh", True)):
+                t0 = time.perf_counter()
+                host = rtg.parse_scene(text, defer_bvh=defer)
+                t1 = time.perf_counter()
+                sid = ctx.upload(host)
+                t2 = time.perf_counter()
+                st = ctx.scene_settings(sid)
+                st.width = st.height = 128
+                st.spp, st.max_depth = 4, 4
+                ctx.render(sid, st, rtg.RenderOptions(progressive=False))
+                ctx.image(-1, 128, 128)
+                t3 = time.perf_counter()
+                prims = ctx.scene_info(sid)["primitives"]
+                ctx.release(sid)
+                runs[arm].append((t1 - t0, t2 - t1, t3 - t2, t3 - t0))
+        entry = {"primitives": prims}
+        for arm, r in runs.items():
+            med = np.median(np.array(r), axis=0) * 1e3
+            entry[arm] = {"compile_ms": med[0], "upload_ms": med[1], "first_pass_ms": med[2], "ttfp_ms": med[3]}
+        entry["speedup"] = entry["host_bvh"]["ttfp_ms"] / entry["gpu_bvh"]["ttfp_ms"]
+        out[name] = entry
+    return out
+
+
 def run_rtg(a, dist, scenes, desc):
     import rtg
 
@@ -385,6 +427,15 @@ def run_rtg(a, dist, scenes, desc):
         serve = serving.serve(ctx, sids[:32], seconds=a.serve_seconds, rate=200.0, preview_share=0.9, seed=2025)
         serve["scenes"] = min(32, len(sids))
 
+    # Scenes that are not resident: the BVH built on the host or on the GPU.
+    cold = None
+    if not a.no_cold:
+        import workloads
+
+        big = sorted(range(len(hosts)), key=lambda k: -len(hosts[k].view()["prims"]))[:2]
+        cold = cold_scene_ttfp(ctx, [("mesh stress, 174k triangles", workloads.mesh_stress())]
+                               + [(f"mix scene {k}", scenes[k]) for k in big])
+
     cpu = None
     if dist.rank == 0 and dist.world == 1 and not a.no_cpu_baseline:
         n, secs, kind, threads, used = cpu_sample(scenes, budget_s=15.0)
@@ -415,6 +466,7 @@ def run_rtg(a, dist, scenes, desc):
             "cpu_baseline": cpu,
             "plain": plain,
             "serving": serve,
+            "cold_scene": cold,
             "invalid_samples": c_st["invalid_samples"],
         }
         print(json.dumps(line), flush=True)

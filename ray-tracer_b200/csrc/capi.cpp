@@ -13,6 +13,7 @@
 #include <unordered_map>
 #include <fstream>
 #include <memory>
+#include <mutex>
 #include <sstream>
 #include <string>
 
@@ -27,9 +28,10 @@ std::vector<std::uint8_t> encode_png(const std::uint8_t* rgb, int width, int hei
 
 struct rtg_host_scene {
   std::shared_ptr<const rtg::CompiledScene> scene;  // shared with every context it is uploaded to
-  // Reference-layout arrays behind rtg_scene_view.
-  std::vector<double> prims, planes, nodes, point_lights, materials;
-  std::vector<std::uint32_t> lights;
+  // Reference-layout arrays behind rtg_scene_view, made on its first call.
+  mutable std::once_flag view_once;
+  mutable std::vector<double> prims, planes, nodes, point_lights, materials;
+  mutable std::vector<std::uint32_t> lights;
 };
 
 struct rtg_context {
@@ -186,6 +188,68 @@ int64_t rtg_scene_dump(const char* scene_json, char* out, size_t cap) {
   }
 }
 
+namespace {
+
+// The compiled scene in the reference's own layout (rtg_scene_view's arrays).
+void build_view_arrays(const rtg_host_scene& hs) {
+  const rtg::CompiledScene& s = *hs.scene;
+  for (const rtg::Prim& p : s.prims) {
+    const rtg::D3 v[6] = {p.a, p.b, p.c, p.n0, p.n1, p.n2};
+    hs.prims.push_back(p.kind == rtg::Prim::kSphere ? 0.0 : 1.0);
+    hs.prims.push_back(p.material);
+    hs.prims.push_back(p.smooth ? 1.0 : 0.0);
+    for (const rtg::D3& q : v) {
+      hs.prims.push_back(q.x);
+      hs.prims.push_back(q.y);
+      hs.prims.push_back(q.z);
+    }
+    hs.prims.insert(hs.prims.end(), 3, 0.0);
+  }
+  for (const rtg::PlanePrim& pl : s.planes) {
+    const double r[8] = {pl.point.x, pl.point.y, pl.point.z, pl.normal.x, pl.normal.y, pl.normal.z, double(pl.material), 0};
+    hs.planes.insert(hs.planes.end(), r, r + 8);
+  }
+  for (const rtg::BinaryNode& n : s.bvh.nodes) {
+    const double r[10] = {n.box.lo.x, n.box.lo.y, n.box.lo.z, n.box.hi.x, n.box.hi.y, n.box.hi.z,
+                          double(n.first), double(n.count), double(n.axis), 0};
+    hs.nodes.insert(hs.nodes.end(), r, r + 10);
+  }
+  for (const rtg::LightEntry& l : s.lights) {
+    hs.lights.push_back(l.kind == rtg::LightEntry::kPoint ? 0u : 1u);
+    hs.lights.push_back(l.index);
+  }
+  for (const rtg::PointLight& pl : s.point_lights) {
+    const double r[6] = {pl.position.x, pl.position.y, pl.position.z, pl.intensity.x, pl.intensity.y, pl.intensity.z};
+    hs.point_lights.insert(hs.point_lights.end(), r, r + 6);
+  }
+  for (const rtg::Material& m : s.materials) {
+    double r[16] = {0};
+    if (const auto* l = std::get_if<rtg::Lambertian>(&m)) {
+      r[0] = 0;
+      r[1] = l->albedo.a.x; r[2] = l->albedo.a.y; r[3] = l->albedo.a.z;
+      r[4] = l->albedo.b.x; r[5] = l->albedo.b.y; r[6] = l->albedo.b.z;
+      r[7] = l->albedo.checker_scale;
+    } else if (const auto* me = std::get_if<rtg::Metal>(&m)) {
+      r[0] = 1;
+      r[1] = me->albedo.x; r[2] = me->albedo.y; r[3] = me->albedo.z;
+      r[8] = me->roughness;
+    } else if (const auto* di = std::get_if<rtg::Dielectric>(&m)) {
+      r[0] = 2;
+      r[1] = di->tint.x; r[2] = di->tint.y; r[3] = di->tint.z;
+      r[9] = di->ior;
+    } else {
+      const auto& e = std::get<rtg::Emissive>(m);
+      r[0] = 3;
+      r[1] = e.color.x; r[2] = e.color.y; r[3] = e.color.z;
+      r[10] = e.intensity;
+      r[11] = e.two_sided ? 1 : 0;
+    }
+    hs.materials.insert(hs.materials.end(), r, r + 16);
+  }
+}
+
+}  // namespace
+
 int rtg_compile(const char* scene_json, const char* base_dir, rtg_host_scene** out, char* err, size_t err_cap) {
   return rtg_compile_flags(scene_json, base_dir, 0, out, err, err_cap);
 }
@@ -206,60 +270,6 @@ int rtg_compile_flags(const char* scene_json, const char* base_dir, uint32_t fla
     if (base_dir) d.base_dir = base_dir;
     auto hs = std::make_unique<rtg_host_scene>();
     hs->scene = std::make_shared<const rtg::CompiledScene>(rtg::compile_scene(d, !(flags & RTG_COMPILE_DEFER_BVH)));
-    const rtg::CompiledScene& s = *hs->scene;
-    for (const rtg::Prim& p : s.prims) {
-      const rtg::D3 v[6] = {p.a, p.b, p.c, p.n0, p.n1, p.n2};
-      hs->prims.push_back(p.kind == rtg::Prim::kSphere ? 0.0 : 1.0);
-      hs->prims.push_back(p.material);
-      hs->prims.push_back(p.smooth ? 1.0 : 0.0);
-      for (const rtg::D3& q : v) {
-        hs->prims.push_back(q.x);
-        hs->prims.push_back(q.y);
-        hs->prims.push_back(q.z);
-      }
-      hs->prims.insert(hs->prims.end(), 3, 0.0);
-    }
-    for (const rtg::PlanePrim& pl : s.planes) {
-      const double r[8] = {pl.point.x, pl.point.y, pl.point.z, pl.normal.x, pl.normal.y, pl.normal.z, double(pl.material), 0};
-      hs->planes.insert(hs->planes.end(), r, r + 8);
-    }
-    for (const rtg::BinaryNode& n : s.bvh.nodes) {
-      const double r[10] = {n.box.lo.x, n.box.lo.y, n.box.lo.z, n.box.hi.x, n.box.hi.y, n.box.hi.z,
-                            double(n.first), double(n.count), double(n.axis), 0};
-      hs->nodes.insert(hs->nodes.end(), r, r + 10);
-    }
-    for (const rtg::LightEntry& l : s.lights) {
-      hs->lights.push_back(l.kind == rtg::LightEntry::kPoint ? 0u : 1u);
-      hs->lights.push_back(l.index);
-    }
-    for (const rtg::PointLight& pl : s.point_lights) {
-      const double r[6] = {pl.position.x, pl.position.y, pl.position.z, pl.intensity.x, pl.intensity.y, pl.intensity.z};
-      hs->point_lights.insert(hs->point_lights.end(), r, r + 6);
-    }
-    for (const rtg::Material& m : s.materials) {
-      double r[16] = {0};
-      if (const auto* l = std::get_if<rtg::Lambertian>(&m)) {
-        r[0] = 0;
-        r[1] = l->albedo.a.x; r[2] = l->albedo.a.y; r[3] = l->albedo.a.z;
-        r[4] = l->albedo.b.x; r[5] = l->albedo.b.y; r[6] = l->albedo.b.z;
-        r[7] = l->albedo.checker_scale;
-      } else if (const auto* me = std::get_if<rtg::Metal>(&m)) {
-        r[0] = 1;
-        r[1] = me->albedo.x; r[2] = me->albedo.y; r[3] = me->albedo.z;
-        r[8] = me->roughness;
-      } else if (const auto* di = std::get_if<rtg::Dielectric>(&m)) {
-        r[0] = 2;
-        r[1] = di->tint.x; r[2] = di->tint.y; r[3] = di->tint.z;
-        r[9] = di->ior;
-      } else {
-        const auto& e = std::get<rtg::Emissive>(m);
-        r[0] = 3;
-        r[1] = e.color.x; r[2] = e.color.y; r[3] = e.color.z;
-        r[10] = e.intensity;
-        r[11] = e.two_sided ? 1 : 0;
-      }
-      hs->materials.insert(hs->materials.end(), r, r + 16);
-    }
     *out = hs.release();
     return RTG_OK;
   } catch (const std::exception& e) {
@@ -272,6 +282,7 @@ void rtg_host_scene_free(rtg_host_scene* scene) { delete scene; }
 
 int rtg_host_scene_view(const rtg_host_scene* hs, rtg_scene_view* out) {
   if (!hs || !out) return RTG_ERR_INVALID;
+  std::call_once(hs->view_once, [hs] { build_view_arrays(*hs); });
   const rtg::CompiledScene& s = *hs->scene;
   *out = rtg_scene_view{};
   out->n_prims = s.prims.size();

@@ -222,22 +222,19 @@ struct LevelArgs {
   std::uint32_t* chunk_start_next;
 };
 
-__device__ __forceinline__ void init_node_keys(long long* k) {
-  for (int a = 0; a < 3; ++a) {
-    k[a] = kKeyPosInf;
-    k[3 + a] = kKeyNegInf;
-    k[6 + a] = kKeyPosInf;
-    k[9 + a] = kKeyNegInf;
-  }
-}
+// One bin of one axis as a lane holds it.
+struct BinData {
+  double lo[3], hi[3];
+  unsigned n;
+};
 
-__device__ __forceinline__ void init_bin_words(long long* g) {
-  for (int q = 0; q < 3 * kBins; ++q) {
-    long long* e = g + 7 * q;
-    e[0] = e[1] = e[2] = kKeyPosInf;
-    e[3] = e[4] = e[5] = kKeyNegInf;
-    e[6] = 0;
+__device__ __forceinline__ void bin_clear(BinData& e) {
+  const double inf = pos_inf();
+  for (int k = 0; k < 3; ++k) {
+    e.lo[k] = inf;
+    e.hi[k] = -inf;
   }
+  e.n = 0;
 }
 
 __device__ __forceinline__ void note_leaf(Counters* c, std::uint32_t n, int d) {
@@ -249,39 +246,54 @@ __device__ __forceinline__ void note_leaf(Counters* c, std::uint32_t n, int d) {
 
 // Registers node c (primitives [first, first + n) of the working order, at
 // `depth`) as a large node of the next level, with its chunks, or as the root
-// of a subtree that one warp builds whole.
+// of a subtree that one warp builds whole. Called by all 32 lanes of a warp.
 __device__ void enqueue_node(const LevelArgs& a, int c, std::uint32_t first, std::uint32_t n, int depth) {
-  a.first[c] = first;
-  a.count[c] = n;
-  a.depth[c] = depth;
-  a.sub[c] = -1;
-  a.left[c] = -1;
-  a.right[c] = -1;
+  const int lane = threadIdx.x & 31;
+  if (lane == 0) {
+    a.first[c] = first;
+    a.count[c] = n;
+    a.depth[c] = depth;
+    a.sub[c] = -1;
+    a.left[c] = -1;
+    a.right[c] = -1;
+  }
   if (n > static_cast<std::uint32_t>(kSmallItems)) {
-    const int slot = atomicAdd(&a.counters->lvl[a.parity ^ 1].tasks, 1);
-    a.tasks_next[slot] = c;
-    init_node_keys(a.key + 12ll * c);
-    init_bin_words(a.bins_next + static_cast<long long>(slot) * kBinWords);
     const int nch = static_cast<int>((n + kChunk - 1) / kChunk);
-    const int c0 = atomicAdd(&a.counters->lvl[a.parity ^ 1].chunks, nch);
-    a.task_chunk0_next[slot] = c0;
-    a.task_nchunks_next[slot] = nch;
-    for (int j = 0; j < nch; ++j) {
+    int slot = 0, c0 = 0;
+    if (lane == 0) {
+      slot = atomicAdd(&a.counters->lvl[a.parity ^ 1].tasks, 1);
+      c0 = atomicAdd(&a.counters->lvl[a.parity ^ 1].chunks, nch);
+      a.tasks_next[slot] = c;
+      a.task_chunk0_next[slot] = c0;
+      a.task_nchunks_next[slot] = nch;
+    }
+    slot = __shfl_sync(0xFFFFFFFFu, slot, 0);
+    c0 = __shfl_sync(0xFFFFFFFFu, c0, 0);
+    // Empty bounds (lo +inf, hi -inf for the box and the centroids) and bins.
+    if (lane < 12) a.key[12ll * c + lane] = (lane % 6) < 3 ? kKeyPosInf : kKeyNegInf;
+    long long* g = a.bins_next + static_cast<long long>(slot) * kBinWords;
+    for (int i = lane; i < kBinWords; i += 32) {
+      const int f = i % 7;
+      g[i] = f < 3 ? kKeyPosInf : (f < 6 ? kKeyNegInf : 0);
+    }
+    for (int j = lane; j < nch; j += 32) {
       a.chunk_task_next[c0 + j] = slot;
       a.chunk_start_next[c0 + j] = first + static_cast<std::uint32_t>(j) * kChunk;
     }
-  } else {
+  } else if (lane == 0) {
     a.small_roots[atomicAdd(&a.counters->small_roots, 1)] = c;
   }
 }
 
-// The root: node 0 over every primitive. Launched with one thread; `a.parity`
-// is 1 so that the root lands in level 0's arrays.
+// The root: node 0 over every primitive. Launched with one warp; `a.parity` is 1
+// so that the root lands in level 0's arrays.
 __global__ void k_init(LevelArgs a, std::uint32_t n, int* dfs, int* idfs) {
-  if (blockIdx.x != 0 || threadIdx.x != 0) return;
-  a.counters->nodes = 1;
-  dfs[0] = 0;
-  idfs[0] = 0;
+  if (blockIdx.x != 0) return;
+  if (threadIdx.x == 0) {
+    a.counters->nodes = 1;
+    dfs[0] = 0;
+    idfs[0] = 0;
+  }
   enqueue_node(a, 0, 0, n, 0);
 }
 
@@ -350,24 +362,46 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_bins(LevelArgs a) {
     s[i] = f < 3 ? kKeyPosInf : (f < 6 ? kKeyNegInf : 0);
   }
   __syncwarp();
+  // Each lane takes 8 consecutive primitives (neighbours in the working order
+  // are usually neighbours in space) and merges a run of primitives that fall in
+  // the same bin before it touches shared memory.
   const std::uint32_t start = a.chunk_start[w];
   const std::uint32_t end = min(start + static_cast<std::uint32_t>(kChunk), a.first[t] + a.count[t]);
-  for (int j = 0; j < kChunk / 32; ++j) {
-    const std::uint32_t pos = start + static_cast<std::uint32_t>(j * 32 + lane);
+  constexpr int kPerLane = kChunk / 32;
+  int run_bin[3] = {-1, -1, -1};
+  BinData run[3];
+  auto flush = [&](int k) {
+    if (run_bin[k] < 0) return;
+    long long* e = s + 7 * (k * kBins + run_bin[k]);
+    for (int m = 0; m < 3; ++m) {
+      atomicMin(&e[m], key_of(run[k].lo[m]));
+      atomicMax(&e[3 + m], key_of(run[k].hi[m]));
+    }
+    atomicAdd(reinterpret_cast<unsigned long long*>(&e[6]), static_cast<unsigned long long>(run[k].n));
+  };
+  for (int j = 0; j < kPerLane; ++j) {
+    const std::uint32_t pos = start + static_cast<std::uint32_t>(lane * kPerLane + j);
     if (pos >= end) break;
     double bl[3], bh[3];
     load_box(a.boxes, a.items[pos], bl, bh);
+#pragma unroll
     for (int k = 0; k < 3; ++k) {
       if (!use[k]) continue;
       const int b = bin_of(0.5 * (bl[k] + bh[k]), clo[k], inv[k]);
-      long long* e = s + 7 * (k * kBins + b);
-      for (int m = 0; m < 3; ++m) {
-        atomicMin(&e[m], key_of(bl[m]));
-        atomicMax(&e[3 + m], key_of(bh[m]));
+      if (b != run_bin[k]) {
+        flush(k);
+        run_bin[k] = b;
+        bin_clear(run[k]);
       }
-      atomicAdd(reinterpret_cast<unsigned long long*>(&e[6]), 1ull);
+      for (int m = 0; m < 3; ++m) {
+        run[k].lo[m] = fmin(run[k].lo[m], bl[m]);
+        run[k].hi[m] = fmax(run[k].hi[m], bh[m]);
+      }
+      ++run[k].n;
     }
   }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) flush(k);
   __syncwarp();
   long long* g = a.bins + static_cast<long long>(lt) * kBinWords;
   for (int q = lane; q < 3 * kBins; q += 32) {
@@ -382,53 +416,100 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_bins(LevelArgs a) {
   }
 }
 
-// The reference's SAH sweep over one axis's 16 bins (7 words each: box keys,
-// count): suffix areas and counts from the right, then the prefix sweep; the
-// first strictly cheaper plane wins, across axes in order.
-__device__ void sah_sweep(const long long* g, double parent_area, int ax, double& best_cost, int& best_axis,
-                          int& best_bin) {
-  const double inf = pos_inf();
-  double right_area[kBins];
-  std::uint32_t right_n[kBins];
-  double lo[3] = {inf, inf, inf}, hi[3] = {-inf, -inf, -inf};
-  std::uint32_t cnt = 0;
-  for (int b = kBins - 1; b > 0; --b) {
-    const long long* e = g + 7 * b;
-    for (int k = 0; k < 3; ++k) {
-      lo[k] = fmin(lo[k], value_of(e[k]));
-      hi[k] = fmax(hi[k], value_of(e[3 + k]));
-    }
-    cnt += static_cast<std::uint32_t>(e[6]);
-    right_area[b] = box_area(lo, hi);
-    right_n[b] = cnt;
-  }
+// The reference's SAH sweep over one axis's 16 bins (src/geometry/bvh.cpp:62-88),
+// with lane b of each 16-lane half holding bin b of that half's axis. The prefix
+// and suffix unions are scans (min / max and integer sums give the same values
+// in any order), every lane prices the plane after its bin, and the cheapest plane
+// wins with the lowest bin on ties, which is the first strictly cheaper plane of
+// the reference's loop. On return every lane of the half holds the axis's result
+// (cost +inf when no plane separates anything) and the primitives left of it.
+__device__ void half_sweep(const BinData& d, double area_floor, double& cost, int& bin, unsigned& left_n) {
+  const unsigned full = 0xFFFFFFFFu;
+  const int b = threadIdx.x & 15;
+  double pl[3], ph[3], sl[3], sh[3];
+  unsigned pn = d.n, sn = d.n;
   for (int k = 0; k < 3; ++k) {
-    lo[k] = inf;
-    hi[k] = -inf;
+    pl[k] = sl[k] = d.lo[k];
+    ph[k] = sh[k] = d.hi[k];
   }
-  cnt = 0;
-  const double area_floor = parent_area < 1e-30 ? 1e-30 : parent_area;
-  for (int b = 0; b < kBins - 1; ++b) {
-    const long long* e = g + 7 * b;
+  for (int o = 1; o < 16; o <<= 1) {
+    double ul[3], uh[3], dl[3], dh[3];
     for (int k = 0; k < 3; ++k) {
-      lo[k] = fmin(lo[k], value_of(e[k]));
-      hi[k] = fmax(hi[k], value_of(e[3 + k]));
+      ul[k] = __shfl_up_sync(full, pl[k], o, 16);
+      uh[k] = __shfl_up_sync(full, ph[k], o, 16);
+      dl[k] = __shfl_down_sync(full, sl[k], o, 16);
+      dh[k] = __shfl_down_sync(full, sh[k], o, 16);
     }
-    cnt += static_cast<std::uint32_t>(e[6]);
-    const std::uint32_t rn = right_n[b + 1];
-    if (cnt == 0 || rn == 0) continue;
-    const double cost = 1.0 + (box_area(lo, hi) * double(cnt) + right_area[b + 1] * double(rn)) / area_floor;
-    if (cost < best_cost) {
-      best_cost = cost;
-      best_axis = ax;
-      best_bin = b;
+    const unsigned un = __shfl_up_sync(full, pn, o, 16), dn = __shfl_down_sync(full, sn, o, 16);
+    if (b >= o) {
+      for (int k = 0; k < 3; ++k) {
+        pl[k] = fmin(pl[k], ul[k]);
+        ph[k] = fmax(ph[k], uh[k]);
+      }
+      pn += un;
+    }
+    if (b + o < 16) {
+      for (int k = 0; k < 3; ++k) {
+        sl[k] = fmin(sl[k], dl[k]);
+        sh[k] = fmax(sh[k], dh[k]);
+      }
+      sn += dn;
+    }
+  }
+  double rl[3], rh[3];
+  for (int k = 0; k < 3; ++k) {
+    rl[k] = __shfl_down_sync(full, sl[k], 1, 16);
+    rh[k] = __shfl_down_sync(full, sh[k], 1, 16);
+  }
+  const unsigned rn = __shfl_down_sync(full, sn, 1, 16);
+  cost = pos_inf();
+  if (b < kBins - 1 && pn != 0 && rn != 0)
+    cost = 1.0 + (box_area(pl, ph) * double(pn) + box_area(rl, rh) * double(rn)) / area_floor;
+  bin = b;
+  left_n = pn;
+  for (int o = 8; o >= 1; o >>= 1) {
+    const double oc = __shfl_xor_sync(full, cost, o, 16);
+    const int ob = __shfl_xor_sync(full, bin, o, 16);
+    const unsigned ol = __shfl_xor_sync(full, left_n, o, 16);
+    if (oc < cost || (oc == cost && ob < bin)) {
+      cost = oc;
+      bin = ob;
+      left_n = ol;
     }
   }
 }
 
-// One thread per large node: box from the keys, SAH decision, children.
-__global__ void k_decide(LevelArgs a) {
-  const int i = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
+// The best split over the three axes, on every lane: r0 holds axis 0 (lanes
+// 0-15) and axis 1 (lanes 16-31), r1 axis 2 (lanes 0-15). Axes in order, the
+// first strictly cheaper wins; an axis whose centroids coincide is skipped.
+__device__ void warp_best_split(const BinData& r0, const BinData& r1, const bool use[3], double parent_area,
+                                double& best_cost, int& best_axis, int& best_bin, unsigned& best_left) {
+  const unsigned full = 0xFFFFFFFFu;
+  const double area_floor = parent_area < 1e-30 ? 1e-30 : parent_area;
+  double c0, c1;
+  int b0, b1;
+  unsigned l0, l1;
+  half_sweep(r0, area_floor, c0, b0, l0);
+  half_sweep(r1, area_floor, c1, b1, l1);
+  const double cost[3] = {__shfl_sync(full, c0, 0), __shfl_sync(full, c0, 16), __shfl_sync(full, c1, 0)};
+  const int bin[3] = {__shfl_sync(full, b0, 0), __shfl_sync(full, b0, 16), __shfl_sync(full, b1, 0)};
+  const unsigned left[3] = {__shfl_sync(full, l0, 0), __shfl_sync(full, l0, 16), __shfl_sync(full, l1, 0)};
+  best_cost = pos_inf();
+  best_axis = -1;
+  best_bin = -1;
+  best_left = 0;
+  for (int ax = 0; ax < 3; ++ax)
+    if (use[ax] && cost[ax] < best_cost) {
+      best_cost = cost[ax];
+      best_axis = ax;
+      best_bin = bin[ax];
+      best_left = left[ax];
+    }
+}
+
+// One warp per large node: box from the keys, SAH decision, children.
+__global__ void __launch_bounds__(128) k_decide(LevelArgs a) {
+  const int i = static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
   if (i >= a.n_tasks) return;
   const int t = a.tasks_cur[i];
   const long long* key = a.key + 12ll * t;
@@ -439,59 +520,74 @@ __global__ void k_decide(LevelArgs a) {
     clo[k] = value_of(key[6 + k]);
     chi[k] = value_of(key[9 + k]);
   }
-  double* bx = a.box + 6ll * t;
-  for (int k = 0; k < 3; ++k) {
-    bx[k] = lo[k];
-    bx[3 + k] = hi[k];
-  }
+  if (lane == 0)
+    for (int k = 0; k < 3; ++k) {
+      a.box[6ll * t + k] = lo[k];
+      a.box[6ll * t + 3 + k] = hi[k];
+    }
   const std::uint32_t n = a.count[t], f0 = a.first[t];
   const int d = a.depth[t];
-  a.need_part[i] = 0;
   bool leaf = n <= 4 || d >= kDepthCap;
-  int split_axis = -1, split_bin = -1;
-  double split_cost = pos_inf();
+  int split_axis = -1;
   std::uint32_t mid = 0;
   bool part = false;
+  int best_bin = -1;
   if (!leaf) {
-    const double parent_area = box_area(lo, hi);
+    bool use[3];
+    for (int k = 0; k < 3; ++k) use[k] = chi[k] > clo[k];
     const long long* g = a.bins + static_cast<long long>(i) * kBinWords;
-    for (int ax = 0; ax < 3; ++ax)
-      if (chi[ax] > clo[ax]) sah_sweep(g + ax * kBins * 7, parent_area, ax, split_cost, split_axis, split_bin);
+    BinData r[2];
+    for (int round = 0; round < 2; ++round) {
+      bin_clear(r[round]);
+      if (round == 1 && lane >= 16) continue;
+      const long long* e = g + 7 * ((round == 0 ? (lane >> 4) : 2) * kBins + (lane & 15));
+      for (int k = 0; k < 3; ++k) {
+        r[round].lo[k] = value_of(e[k]);
+        r[round].hi[k] = value_of(e[3 + k]);
+      }
+      r[round].n = static_cast<unsigned>(e[6]);
+    }
+    double best_cost;
+    unsigned left_n;
+    warp_best_split(r[0], r[1], use, box_area(lo, hi), best_cost, split_axis, best_bin, left_n);
     if (split_axis < 0) {
       mid = n / 2;  // every centroid coincides
       split_axis = widest_axis(clo, chi);
-    } else if (split_cost >= double(n) && n <= 16) {
+    } else if (best_cost >= double(n) && n <= 16) {
       leaf = true;
+    } else if (left_n == 0 || left_n == n) {
+      mid = n / 2;  // rounding put everything on one side
     } else {
-      std::uint32_t left_n = 0;
-      for (int b = 0; b <= split_bin; ++b) left_n += static_cast<std::uint32_t>(g[7 * (split_axis * kBins + b) + 6]);
-      if (left_n == 0 || left_n == n) {
-        mid = n / 2;  // rounding put everything on one side
-      } else {
-        mid = left_n;
-        part = true;
-      }
+      mid = left_n;
+      part = true;
     }
   }
   if (leaf) {
-    a.left[t] = -1;
-    a.right[t] = -1;
-    a.axis[t] = 0;
-    note_leaf(a.counters, n, d);
+    if (lane == 0) {
+      a.left[t] = -1;
+      a.right[t] = -1;
+      a.axis[t] = 0;
+      a.need_part[i] = 0;
+      note_leaf(a.counters, n, d);
+    }
     return;
   }
-  a.axis[t] = split_axis;
-  if (part) {
-    a.need_part[i] = 1;
-    a.part_t[i] = static_cast<int>(mid);
-    a.part_axis[i] = split_axis;
-    a.part_bin[i] = split_bin;
-    a.part_lo[i] = clo[split_axis];
-    a.part_inv[i] = kBins / (chi[split_axis] - clo[split_axis]);
+  int c = 0;
+  if (lane == 0) {
+    a.axis[t] = split_axis;
+    a.need_part[i] = part ? 1 : 0;
+    if (part) {
+      a.part_t[i] = static_cast<int>(mid);
+      a.part_axis[i] = split_axis;
+      a.part_bin[i] = best_bin;
+      a.part_lo[i] = clo[split_axis];
+      a.part_inv[i] = kBins / (chi[split_axis] - clo[split_axis]);
+    }
+    c = atomicAdd(&a.counters->nodes, 2);
+    a.left[t] = c;
+    a.right[t] = c + 1;
   }
-  const int c = atomicAdd(&a.counters->nodes, 2);
-  a.left[t] = c;
-  a.right[t] = c + 1;
+  c = __shfl_sync(0xFFFFFFFFu, c, 0);
   enqueue_node(a, c, f0, mid, d + 1);
   enqueue_node(a, c + 1, f0 + mid, n - mid, d + 1);
 }
@@ -656,7 +752,6 @@ struct SmallWarp {
   double box[kSmallItems][6];
   double cen[kSmallItems][3];
   std::uint32_t id[kSmallItems];
-  long long bins[kBinWords];
   double nbox[kSmallNodes][6];
   int nl[kSmallNodes], nr[kSmallNodes], nfirst[kSmallNodes], ncount[kSmallNodes], naxis[kSmallNodes];
   int ndepth[kSmallNodes], nsize[kSmallNodes], nisize[kSmallNodes], nilocal[kSmallNodes];
@@ -735,63 +830,54 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_small(SmallArgs a) {
     int kind = 0;  // 0 leaf, 1 middle split, 2 SAH partition
     int sp_axis = 0, sp_bin = -1, mid = lo;
     if (!(cnt <= 4 || d >= kDepthCap)) {
-      for (int q = lane; q < 3 * kBins; q += 32) {
-        const int ax = q / kBins, b = q % kBins;
-        double el[3] = {inf, inf, inf}, eh[3] = {-inf, -inf, -inf};
-        long long c = 0;
-        if (ch[ax] > cl[ax]) {
-          const double inv = kBins / (ch[ax] - cl[ax]);
-          for (int p = lo; p < hi; ++p) {
-            if (bin_of(s.cen[p][ax], cl[ax], inv) != b) continue;
-            for (int k = 0; k < 3; ++k) {
-              el[k] = fmin(el[k], s.box[p][k]);
-              eh[k] = fmax(eh[k], s.box[p][3 + k]);
-            }
-            ++c;
-          }
-        }
-        long long* e = s.bins + 7 * q;
-        for (int k = 0; k < 3; ++k) {
-          e[k] = key_of(el[k]);
-          e[3 + k] = key_of(eh[k]);
-        }
-        e[6] = c;
+      // Lane (axis, bin) bins the node's primitives itself: round 0 covers axes
+      // 0 and 1 (lanes 0-15, 16-31), round 1 axis 2 (lanes 0-15).
+      bool use[3];
+      double inv[3];
+      for (int k = 0; k < 3; ++k) {
+        use[k] = ch[k] > cl[k];
+        inv[k] = use[k] ? kBins / (ch[k] - cl[k]) : 0.0;
       }
-      __syncwarp();
-      if (lane == 0) {
-        const double parent_area = box_area(bl, bh);
-        int best_axis = -1, best_bin = -1;
-        double best_cost = inf;
-        for (int ax = 0; ax < 3; ++ax)
-          if (ch[ax] > cl[ax]) sah_sweep(s.bins + ax * kBins * 7, parent_area, ax, best_cost, best_axis, best_bin);
-        if (best_axis < 0) {
+      BinData r[2];
+      for (int round = 0; round < 2; ++round) {
+        BinData& e = r[round];
+        bin_clear(e);
+        const int ax = round == 0 ? (lane >> 4) : 2, b = lane & 15;
+        if ((round == 1 && lane >= 16) || !use[ax]) continue;
+        for (int p = lo; p < hi; ++p) {
+          if (bin_of(s.cen[p][ax], cl[ax], inv[ax]) != b) continue;
+          for (int k = 0; k < 3; ++k) {
+            e.lo[k] = fmin(e.lo[k], s.box[p][k]);
+            e.hi[k] = fmax(e.hi[k], s.box[p][3 + k]);
+          }
+          ++e.n;
+        }
+      }
+      double best_cost;
+      int best_axis, best_bin;
+      unsigned left_n;
+      warp_best_split(r[0], r[1], use, box_area(bl, bh), best_cost, best_axis, best_bin, left_n);
+      if (best_axis < 0) {
+        kind = 1;
+        sp_axis = widest_axis(cl, ch);
+        mid = lo + cnt / 2;
+      } else if (!(best_cost >= double(cnt) && cnt <= 16)) {
+        sp_axis = best_axis;
+        sp_bin = best_bin;
+        if (left_n == 0 || left_n == static_cast<unsigned>(cnt)) {
           kind = 1;
-          sp_axis = widest_axis(cl, ch);
           mid = lo + cnt / 2;
-        } else if (!(best_cost >= double(cnt) && cnt <= 16)) {
-          int left_n = 0;
-          for (int b = 0; b <= best_bin; ++b) left_n += static_cast<int>(s.bins[7 * (best_axis * kBins + b) + 6]);
-          sp_axis = best_axis;
-          sp_bin = best_bin;
-          if (left_n == 0 || left_n == cnt) {
-            kind = 1;
-            mid = lo + cnt / 2;
-          } else {
-            kind = 2;
-            mid = lo + left_n;
-          }
-        }
-        // Two more stack entries always fit (at most 29 for 32 primitives); the
-        // check only keeps shared memory safe.
-        if (kind != 0 && top + 2 > kSmallItems) {
-          kind = 0;
-          overflow = true;
+        } else {
+          kind = 2;
+          mid = lo + static_cast<int>(left_n);
         }
       }
-      kind = __shfl_sync(0xFFFFFFFFu, kind, 0);
-      sp_axis = __shfl_sync(0xFFFFFFFFu, sp_axis, 0);
-      sp_bin = __shfl_sync(0xFFFFFFFFu, sp_bin, 0);
-      mid = __shfl_sync(0xFFFFFFFFu, mid, 0);
+      // Two more stack entries always fit (at most 29 for 32 primitives); the
+      // check only keeps shared memory safe.
+      if (kind != 0 && top + 2 > kSmallItems) {
+        kind = 0;
+        overflow = true;
+      }
     }
     if (kind == 0) {
       if (lane == 0) {
@@ -1342,7 +1428,7 @@ GpuBvhCounts GpuBvhBuilder::build(const GpuBvhInput& in) {
     k_bounds<<<blocks_for(32ll * nc, 128), 128, 0, stream_>>>(a);
     k_bins<<<blocks_for(nc, kWarpsPerBlock), kWarpsPerBlock * 32, 0, stream_>>>(a);
     BVH_CK(cudaMemsetAsync(&s.counters->lvl[p ^ 1], 0, sizeof(LevelCount), stream_));
-    k_decide<<<blocks_for(nt, 128), 128, 0, stream_>>>(a);
+    k_decide<<<blocks_for(32ll * nt, 128), 128, 0, stream_>>>(a);
     k_pcount<<<blocks_for(32ll * nc, 128), 128, 0, stream_>>>(a);
     k_pscan<<<blocks_for(32ll * nt, 128), 128, 0, stream_>>>(a);
     k_pranks<<<blocks_for(32ll * nc, 128), 128, 0, stream_>>>(a);

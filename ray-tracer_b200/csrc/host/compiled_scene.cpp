@@ -1,8 +1,10 @@
 #include "host/compiled_scene.hpp"
 
 #include <algorithm>
+#include <array>
 #include <filesystem>
 #include <stdexcept>
+#include <thread>
 
 #include "host/mesh.hpp"
 
@@ -54,6 +56,31 @@ void CameraFrame::setup(const CameraDesc& d, int width, int height) {
   lens_radius = d.aperture / 2;
 }
 
+namespace {
+
+constexpr double kMinTriangleArea = 1e-14;  // smaller triangles are dropped as degenerate
+
+// Runs body(begin, end) over [0, n) in contiguous chunks on the host cores.
+template <class F>
+void parallel_for(std::size_t n, F&& body) {
+  const std::size_t workers = std::min<std::size_t>({16, std::max(1u, std::thread::hardware_concurrency()),
+                                                     (n + 1023) / 1024});
+  if (workers <= 1) {
+    body(std::size_t(0), n);
+    return;
+  }
+  std::vector<std::thread> pool;
+  const std::size_t chunk = (n + workers - 1) / workers;
+  for (std::size_t w = 1; w < workers; ++w) {
+    const std::size_t b = std::min(n, w * chunk), e = std::min(n, b + chunk);
+    pool.emplace_back([&body, b, e] { body(b, e); });
+  }
+  body(std::size_t(0), std::min(n, chunk));
+  for (auto& t : pool) t.join();
+}
+
+}  // namespace
+
 CompiledScene compile_scene(const SceneDesc& desc, bool build_bvh) {
   CompiledScene s;
   s.settings = desc.render;
@@ -69,7 +96,7 @@ CompiledScene compile_scene(const SceneDesc& desc, bool build_bvh) {
   };
 
   auto add_tri = [&](const Prim& t) {
-    if (t.area() < 1e-14) {  // degenerate: cannot be hit reliably
+    if (t.area() < kMinTriangleArea) {  // degenerate: cannot be hit reliably
       s.info.degenerate_skipped++;
       return;
     }
@@ -134,17 +161,49 @@ CompiledScene compile_scene(const SceneDesc& desc, bool build_bvh) {
       if (md.smooth && mesh.normals.empty()) mesh.smooth_normals();
       const Placement place{md.scale, md.rotate_y, md.translate};
       const bool smooth = md.smooth && !mesh.normals.empty();
-      for (const auto& f : mesh.faces) {
-        Prim t = flat_tri(place.point(mesh.positions[f[0]]), place.point(mesh.positions[f[1]]),
-                          place.point(mesh.positions[f[2]]), mat);
+      // Every vertex is placed once (the same arithmetic the per-corner placement
+      // does), then the faces are filled on all host cores: each chunk counts its
+      // non-degenerate faces, and writes them at its offset, in face order.
+      std::vector<D3> pos(mesh.positions.size()), nrm(smooth ? mesh.normals.size() : 0);
+      parallel_for(pos.size(), [&](std::size_t i0, std::size_t i1) {
+        for (std::size_t i = i0; i < i1; ++i) pos[i] = place.point(mesh.positions[i]);
+        for (std::size_t i = i0; i < std::min(i1, nrm.size()); ++i) nrm[i] = place.normal(mesh.normals[i]);
+      });
+      auto face_prim = [&](const std::array<std::uint32_t, 3>& f) {
+        Prim t = flat_tri(pos[f[0]], pos[f[1]], pos[f[2]], mat);
         if (smooth) {
-          t.n0 = place.normal(mesh.normals[f[0]]);
-          t.n1 = place.normal(mesh.normals[f[1]]);
-          t.n2 = place.normal(mesh.normals[f[2]]);
+          t.n0 = nrm[f[0]];
+          t.n1 = nrm[f[1]];
+          t.n2 = nrm[f[2]];
           t.smooth = true;
         }
-        add_tri(t);
-      }
+        return t;
+      };
+      const std::size_t nf = mesh.faces.size();
+      const std::size_t chunks = std::min<std::size_t>(64, (nf + 4095) / 4096);
+      std::vector<std::size_t> kept(chunks + 1, 0);
+      auto chunk_range = [&](std::size_t c) { return std::pair{nf * c / chunks, nf * (c + 1) / chunks}; };
+      parallel_for(chunks, [&](std::size_t c0, std::size_t c1) {
+        for (std::size_t c = c0; c < c1; ++c) {
+          const auto [f0, f1] = chunk_range(c);
+          for (std::size_t i = f0; i < f1; ++i) kept[c + 1] += face_prim(mesh.faces[i]).area() >= kMinTriangleArea;
+        }
+      });
+      for (std::size_t c = 0; c < chunks; ++c) kept[c + 1] += kept[c];
+      const std::size_t base = s.prims.size();
+      s.prims.resize(base + kept[chunks]);
+      parallel_for(chunks, [&](std::size_t c0, std::size_t c1) {
+        for (std::size_t c = c0; c < c1; ++c) {
+          const auto [f0, f1] = chunk_range(c);
+          std::size_t at = base + kept[c];
+          for (std::size_t i = f0; i < f1; ++i) {
+            const Prim t = face_prim(mesh.faces[i]);
+            if (t.area() >= kMinTriangleArea) s.prims[at++] = t;
+          }
+        }
+      });
+      s.info.triangles += kept[chunks];
+      s.info.degenerate_skipped += nf - kept[chunks];
     }
   }
 

@@ -5,7 +5,6 @@
 #include <fstream>
 #include <sstream>
 #include <stdexcept>
-#include <unordered_map>
 
 namespace rtg {
 
@@ -48,15 +47,24 @@ IndexedMesh icosphere(int subdivisions) {
   for (int level = 0; level < subdivisions; ++level) {
     // Each edge gets one midpoint vertex, created the first time the edge is
     // met while walking the faces in order (so vertex numbering is stable).
-    std::unordered_map<std::uint64_t, std::uint32_t> edge_mid;
-    edge_mid.reserve(m.faces.size() * 2);
+    // Open-addressing table edge -> midpoint vertex, at most half full. A key
+    // is never 0: an edge's larger endpoint index is at least 1.
+    int bits = 1;
+    while ((std::size_t(1) << bits) < m.faces.size() * 4) ++bits;
+    const std::size_t mask = (std::size_t(1) << bits) - 1;
+    std::vector<std::uint64_t> keys(mask + 1, 0);
+    std::vector<std::uint32_t> mids(mask + 1, 0);
     auto midpoint = [&](std::uint32_t a, std::uint32_t b) -> std::uint32_t {
       const std::uint64_t key = (std::uint64_t(std::min(a, b)) << 32) | std::max(a, b);
-      const auto found = edge_mid.find(key);
-      if (found != edge_mid.end()) return found->second;
+      std::size_t h = static_cast<std::size_t>((key * 0x9E3779B97F4A7C15ull) >> (64 - bits));
+      while (keys[h] != 0) {
+        if (keys[h] == key) return mids[h];
+        h = (h + 1) & mask;
+      }
       m.positions.push_back(unit(m.positions[a] + m.positions[b]));
       const auto id = static_cast<std::uint32_t>(m.positions.size() - 1);
-      edge_mid.emplace(key, id);
+      keys[h] = key;
+      mids[h] = id;
       return id;
     };
     std::vector<std::array<std::uint32_t, 3>> finer;
