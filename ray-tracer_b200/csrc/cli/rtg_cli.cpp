@@ -41,6 +41,7 @@ void usage() {
                "  --seed N               RNG seed\n"
                "  --exposure X           exposure multiplier\n"
                "  --no-bvh               brute-force intersection (reference)\n"
+               "  --gpu-bvh              build the BVH on the GPU instead of the host (same tree)\n"
                "  --no-light-sampling    disable next-event estimation\n"
                "  --single-pass          render all samples in one pass\n"
                "  --max-pass N           cap samples per progressive pass (default 32)\n"
@@ -143,7 +144,7 @@ int main(int argc, char** argv) {
   std::optional<long long> seed;
   std::optional<double> exposure;
   std::optional<std::string> integrator;
-  bool no_bvh = false, no_nee = false, single_pass = false, stream = false, quiet = false;
+  bool no_bvh = false, gpu_bvh = false, no_nee = false, single_pass = false, stream = false, quiet = false;
   bool validate_only = false, dump = false, save_every = false;
   int device = 0;
   for (int i = 1; i < argc; ++i) {
@@ -176,6 +177,7 @@ int main(int argc, char** argv) {
     else if (a == "--integrator") integrator = next();
     else if (a == "--device") device = next_int();
     else if (a == "--no-bvh") no_bvh = true;
+    else if (a == "--gpu-bvh") gpu_bvh = true;
     else if (a == "--no-light-sampling") no_nee = true;
     else if (a == "--single-pass") single_pass = true;
     else if (a == "--stream") stream = true;
@@ -221,7 +223,9 @@ int main(int argc, char** argv) {
 
   char err[1024] = {0};
   rtg_host_scene* host = nullptr;
-  if (rtg_compile(text.c_str(), base_dir.c_str(), &host, err, sizeof err) != RTG_OK) return scene_error(err);
+  if (rtg_compile_flags(text.c_str(), base_dir.c_str(), gpu_bvh ? RTG_COMPILE_DEFER_BVH : 0u, &host, err,
+                        sizeof err) != RTG_OK)
+    return scene_error(err);
   rtg_scene_view view{};
   rtg_host_scene_view(host, &view);
   rtg_settings s = view.settings;
