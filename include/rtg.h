@@ -36,7 +36,9 @@ typedef int32_t rtg_scene_id;
 typedef struct rtg_settings {
   int32_t width, height, spp, max_depth, rr_min_depth;
   int32_t integrator; /* 0 path, 1 direct, 2 normals */
-  int32_t light_sampling;
+  int32_t light_sampling; /* 0 off, 1 next-event estimation, 2 NEE + multiple importance
+                           * sampling with BSDF sampling (power heuristic; no reference
+                           * counterpart: its docs/performance.md lists MIS as future work) */
   int32_t tone_map;   /* 0 clamp, 1 reinhard, 2 aces */
   uint64_t seed;
   double exposure;

@@ -63,6 +63,7 @@ rtg::RenderSettings from_c(const rtg_settings& c) {
   s.rr_min_depth = c.rr_min_depth;
   s.integrator = static_cast<rtg::Integrator>(c.integrator);
   s.light_sampling = c.light_sampling != 0;
+  s.mis = c.light_sampling == 2;
   s.tone_map = static_cast<rtg::ToneMap>(c.tone_map);
   s.seed = c.seed;
   s.exposure = c.exposure;
@@ -80,7 +81,7 @@ rtg_settings to_c(const rtg::RenderSettings& s) {
   c.max_depth = s.max_depth;
   c.rr_min_depth = s.rr_min_depth;
   c.integrator = static_cast<int32_t>(s.integrator);
-  c.light_sampling = s.light_sampling ? 1 : 0;
+  c.light_sampling = s.light_sampling ? (s.mis ? 2 : 1) : 0;
   c.tone_map = static_cast<int32_t>(s.tone_map);
   c.seed = s.seed;
   c.exposure = s.exposure;

@@ -43,6 +43,7 @@ void usage() {
                "  --no-bvh               brute-force intersection (reference)\n"
                "  --gpu-bvh              build the BVH on the GPU instead of the host (same tree)\n"
                "  --no-light-sampling    disable next-event estimation\n"
+               "  --mis                  weight NEE and BSDF sampling by multiple importance sampling\n"
                "  --single-pass          render all samples in one pass\n"
                "  --max-pass N           cap samples per progressive pass (default 32)\n"
                "  --stream               write progressive PNG frames to stdout\n"
@@ -144,7 +145,7 @@ int main(int argc, char** argv) {
   std::optional<long long> seed;
   std::optional<double> exposure;
   std::optional<std::string> integrator;
-  bool no_bvh = false, gpu_bvh = false, no_nee = false, single_pass = false, stream = false, quiet = false;
+  bool no_bvh = false, gpu_bvh = false, no_nee = false, mis = false, single_pass = false, stream = false, quiet = false;
   bool validate_only = false, dump = false, save_every = false;
   int device = 0;
   for (int i = 1; i < argc; ++i) {
@@ -179,6 +180,7 @@ int main(int argc, char** argv) {
     else if (a == "--no-bvh") no_bvh = true;
     else if (a == "--gpu-bvh") gpu_bvh = true;
     else if (a == "--no-light-sampling") no_nee = true;
+    else if (a == "--mis") mis = true;
     else if (a == "--single-pass") single_pass = true;
     else if (a == "--stream") stream = true;
     else if (a == "--save-every-pass") save_every = true;
@@ -236,6 +238,7 @@ int main(int argc, char** argv) {
   if (seed) s.seed = static_cast<std::uint64_t>(*seed);
   if (exposure) s.exposure = *exposure;
   if (no_bvh) s.use_bvh = 0;
+  if (mis && s.light_sampling) s.light_sampling = 2;
   if (no_nee) s.light_sampling = 0;
   if (integrator) {
     if (*integrator == "path") s.integrator = 0;

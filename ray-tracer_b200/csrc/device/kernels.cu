@@ -248,8 +248,10 @@ __global__ void __launch_bounds__(kBlock) k_extend(WaveBuffers wb, int par) {
 }
 
 // ---------------------------------------------------------------------------
-template <int kBlock>
 // 64 registers (8 blocks of 128 per SM) with a few spills measured 4% faster than 80.
+// kMis: some open job uses multiple importance sampling. Without one, the MIS code
+// is compiled out and the kernel keeps its registers for the common path.
+template <int kBlock, bool kMis>
 __global__ void __launch_bounds__(kBlock, 1024 / kBlock) k_shade(WaveBuffers wb, int par) {
   constexpr int kWarps = kBlock / 32;
   __shared__ std::uint32_t s_cnt[2][kWarps];
@@ -270,6 +272,7 @@ __global__ void __launch_bounds__(kBlock, 1024 / kBlock) k_shade(WaveBuffers wb,
     float3 o_next = f3(0.f, 0.f, 0.f), d_next = o_next, beta = o_next, sh_o = o_next, sh_d = o_next, sh_c = o_next;
     float sh_tmax = 0.f;
     std::uint32_t sample = 0, meta_next = 0, job = 0, seg = 0;
+    float pdf_next = -1.f;  // set when the next hit may need a MIS weight
     Pcg rng{0, 0};
     if (i < n) {
       const float4 a = __ldcs(&A[i]), b = __ldcs(&B[i]), c = __ldcs(&Cc[i]), hv = __ldcs(&wb.hits[i]);
@@ -302,11 +305,20 @@ __global__ void __launch_bounds__(kBlock, 1024 / kBlock) k_shade(WaveBuffers wb,
         const Surface s = make_surface(J, o, d, h);
         const DevMaterial m = J.materials[s.material];
         const float3 le = emitted(m, s.front);
-        // A light reached by a diffuse bounce was already counted by NEE.
-        if (!is_zero3(le) && (specular_bounce || !J.light_sampling || s.is_plane)) {
-          const float3 add = beta * le;
-          const float4 acc = *slot;
-          *slot = make_float4(acc.x + add.x, acc.y + add.y, acc.z + add.z, 0.f);
+        // A light reached by a diffuse bounce was already counted by NEE. With
+        // MIS both count, each weighted by the power heuristic against the other.
+        if (!is_zero3(le)) {
+          float w = 1.f;
+          if (!specular_bounce && J.light_sampling && !s.is_plane)
+            w = kMis && J.light_sampling == 2
+                    ? power_heuristic(__ldcs(&wb.st_e[par][i]),
+                                      light_pdf_of_hit(J, o, d, h, s) / static_cast<float>(J.n_lights))
+                    : 0.f;
+          if (w > 0.f) {
+            const float3 add = beta * le * w;
+            const float4 acc = *slot;
+            *slot = make_float4(acc.x + add.x, acc.y + add.y, acc.z + add.z, 0.f);
+          }
         }
         Scatter sr;
         if (scatter(m, d, s, rng, sr)) {
@@ -321,7 +333,10 @@ __global__ void __launch_bounds__(kBlock, 1024 / kBlock) k_shade(WaveBuffers wb,
                 sh_o = sray.o;
                 sh_d = sray.d;
                 sh_tmax = sray.tmax;
-                sh_c = beta * (f * ls.li_over_pdf) * static_cast<float>(nl);
+                float w = 1.f;  // a point light (pdf 0) cannot be hit by BSDF sampling
+                if (kMis && J.light_sampling == 2 && ls.pdf > 0.f)
+                  w = power_heuristic(ls.pdf / static_cast<float>(nl), dot3(s.n, ls.wi) * kInvPiF);
+                sh_c = beta * (f * ls.li_over_pdf) * (static_cast<float>(nl) * w);
                 shadow = true;
               }
             }
@@ -342,6 +357,8 @@ __global__ void __launch_bounds__(kBlock, 1024 / kBlock) k_shade(WaveBuffers wb,
             o_next = spawn_towards(s.p, s.gn, sr.dir);
             d_next = sr.dir;
             meta_next = (depth + 1) | (sr.specular ? kFlagSpecular : 0u) | (job << kMetaSceneShift);
+            // Cosine-hemisphere pdf of this bounce, for the MIS weight at the next hit.
+            if (kMis && J.light_sampling == 2 && !sr.specular) pdf_next = dot3(s.n, sr.dir) * kInvPiF;
           }
         }
       }
@@ -379,6 +396,7 @@ __global__ void __launch_bounds__(kBlock, 1024 / kBlock) k_shade(WaveBuffers wb,
       __stcs(&wb.st_c[par ^ 1][cpos], make_float4(beta.x, beta.y, beta.z, __uint_as_float(seg)));
       __stcs(&wb.st_d[par ^ 1][cpos], make_uint4(static_cast<std::uint32_t>(rng.state), static_cast<std::uint32_t>(rng.state >> 32),
                                           static_cast<std::uint32_t>(rng.inc), static_cast<std::uint32_t>(rng.inc >> 32)));
+      if (kMis && pdf_next >= 0.f) __stcs(&wb.st_e[par ^ 1][cpos], pdf_next);
     }
     if (shadow) {
       __stcs(&wb.sh_a[spos], make_float4(sh_o.x, sh_o.y, sh_o.z, __uint_as_float(sample)));
@@ -634,7 +652,7 @@ int persistent_blocks(K kernel, int block) {
 }
 
 struct BlockCounts {
-  int extend = 0, extend_counting = 0, shade = 0, shadow = 0, shadow_counting = 0;
+  int extend = 0, extend_counting = 0, shade = 0, shade_mis = 0, shadow = 0, shadow_counting = 0;
 };
 
 template <int kBlock>
@@ -643,7 +661,8 @@ const BlockCounts& block_counts() {
     BlockCounts b;
     b.extend = persistent_blocks(k_extend<kBlock, false>, kBlock);
     b.extend_counting = persistent_blocks(k_extend<kBlock, true>, kBlock);
-    b.shade = persistent_blocks(k_shade<kBlock>, kBlock);
+    b.shade = persistent_blocks(k_shade<kBlock, false>, kBlock);
+    b.shade_mis = persistent_blocks(k_shade<kBlock, true>, kBlock);
     b.shadow = persistent_blocks(k_shadow<kBlock, false>, kBlock);
     b.shadow_counting = persistent_blocks(k_shadow<kBlock, true>, kBlock);
     return b;
@@ -683,8 +702,9 @@ cudaError_t stage_impl(Stage stage, const WaveBuffers& wb, int par, const Launch
                    : launch_chained(k_extend<kBlock, false>, blocks, kBlock, pdl, stream, wb, par);
     }
     case Stage::Shade: {
-      const int blocks = shape.shade_blocks ? shape.shade_blocks : bc.shade;
-      return launch_chained(k_shade<kBlock>, blocks, kBlock, pdl, stream, wb, par);
+      const int blocks = shape.shade_blocks ? shape.shade_blocks : (shape.mis ? bc.shade_mis : bc.shade);
+      return shape.mis ? launch_chained(k_shade<kBlock, true>, blocks, kBlock, pdl, stream, wb, par)
+                       : launch_chained(k_shade<kBlock, false>, blocks, kBlock, pdl, stream, wb, par);
     }
     case Stage::Shadow: {
       const int blocks = shape.shadow_blocks ? shape.shadow_blocks : (count ? bc.shadow_counting : bc.shadow);

@@ -102,7 +102,7 @@ struct alignas(16) RtgSceneDev {
   // settings
   std::int32_t width, height, max_depth, rr_min_depth;
   std::int32_t integrator;    // 0 path, 1 direct, 2 normals
-  std::int32_t light_sampling;
+  std::int32_t light_sampling;  // 0 off, 1 NEE, 2 NEE with MIS
   std::int32_t use_bvh;
   std::uint32_t pad0;
   std::uint64_t seed;

@@ -163,6 +163,7 @@ struct LightSample {
   float3 wi;
   float dist;
   float3 li_over_pdf;  // incident radiance / pdf (I / d^2 for point lights)
+  float pdf;           // solid-angle pdf of wi (0 for point lights: a delta)
   bool valid;
 };
 
@@ -201,6 +202,7 @@ __device__ __forceinline__ LightSample sample_light(const DevLight* __restrict__
     out.dist = sqrtf(d2);
     out.wi = dv * (1.f / out.dist);
     out.li_over_pdf = f3(__ldg(&Lp->q1)) * (1.f / d2);
+    out.pdf = 0.f;
     out.valid = true;
     return out;
   }
@@ -224,6 +226,7 @@ __device__ __forceinline__ LightSample sample_light(const DevLight* __restrict__
       const float cos_l = fabsf(dot3(nl, out.wi));
       if (cos_l < 1e-9f) return out;
       out.li_over_pdf = emit * (cos_l * area / dd2);
+      out.pdf = dd2 / (cos_l * area);
       out.valid = true;
       return out;
     }
@@ -236,6 +239,7 @@ __device__ __forceinline__ LightSample sample_light(const DevLight* __restrict__
     if (!sphere_test(p, out.wi, c, r, 0.f, __int_as_float(0x7f800000), t)) return out;  // grazing miss
     out.dist = t;
     out.li_over_pdf = emit * (2.f * kPiF * one_minus_cos);
+    out.pdf = 1.f / (2.f * kPiF * one_minus_cos);
     out.valid = true;
     return out;
   }
@@ -256,8 +260,39 @@ __device__ __forceinline__ LightSample sample_light(const DevLight* __restrict__
   const float cos_l = fabsf(cos_signed);
   if (cos_l < 1e-9f) return out;
   out.li_over_pdf = f3(__ldg(&Lp->q4)) * (cos_l * area / d2);
+  out.pdf = d2 / (cos_l * area);
   out.valid = true;
   return out;
+}
+
+// Solid-angle pdf with which sample_light would have produced direction d from
+// o toward the emitter the ray hit (slot h.word, distance h.t, surface s): the
+// same cone / area cases as above, seen from the ray origin. Multiple importance
+// sampling weighs a BSDF-sampled hit on a light with it.
+__device__ __forceinline__ float light_pdf_of_hit(const RtgSceneDev& sc, float3 o, float3 d, const RayHit& h,
+                                                  const Surface& s) {
+  const int slot = static_cast<int>(h.word);
+  const float4 p0 = __ldg(&sc.prims[3 * slot]);
+  const float4 p1 = __ldg(&sc.prims[3 * slot + 1]);
+  const float cos_l = fabsf(dot3(s.gn, d));
+  if (__float_as_uint(p0.w) & kSphereBit) {
+    const float r = p1.x, r2 = p1.y;
+    const float3 oc = f3(p0) - o;
+    const float d2 = dot3(oc, oc);
+    if (d2 <= r2) return cos_l > 0.f ? h.t * h.t / (cos_l * 4.f * kPiF * r2) : 0.f;
+    const float x = r2 / d2;
+    return 1.f / (2.f * kPiF * (x / (1.f + sqrtf(1.f - x))));
+  }
+  const float4 p2 = __ldg(&sc.prims[3 * slot + 2]);
+  const float3 c = cross3(f3(p1), f3(p2));
+  const float area = 0.5f * sqrtf(dot3(c, c));
+  return cos_l > 0.f && area > 0.f ? h.t * h.t / (cos_l * area) : 0.f;
+}
+
+// Power heuristic (Veach, beta = 2) of the strategy with pdf a against one with pdf b.
+__device__ __forceinline__ float power_heuristic(float a, float b) {
+  const float a2 = a * a, b2 = b * b;
+  return a2 + b2 > 0.f ? a2 / (a2 + b2) : 0.f;
 }
 
 }  // namespace rtg

@@ -16,6 +16,7 @@ struct WaveBuffers {
   float4* st_b[2];
   float4* st_c[2];
   uint4* st_d[2];
+  float* st_e[2];  // pdf of the direction a diffuse bounce sampled (read only by MIS jobs)
   float4* hits;
   float4* sh_a;
   float4* sh_b;
@@ -36,6 +37,7 @@ struct LaunchShape {
   int extend_blocks = 0, shade_blocks = 0, shadow_blocks = 0;  // 0 = derived from the SM count
   int extend_block = 128;  // 64, 128 or 256
   bool chained = true;     // programmatic dependent launch between the wavefront kernels
+  bool mis = false;        // a job with multiple importance sampling is open (shade kernel variant)
 };
 
 enum class Stage { Plan, Extend, Shade, Shadow };

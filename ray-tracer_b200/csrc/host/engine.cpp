@@ -171,7 +171,7 @@ void Engine::reset_wave() {
   cudaStreamSynchronize(stream_);
   if (wave_) {
     WaveBuffers& b = wave_->wb;
-    for (int i = 0; i < 2; ++i) { dev_free(b.st_a[i]); dev_free(b.st_b[i]); dev_free(b.st_c[i]); dev_free(b.st_d[i]); }
+    for (int i = 0; i < 2; ++i) { dev_free(b.st_a[i]); dev_free(b.st_b[i]); dev_free(b.st_c[i]); dev_free(b.st_d[i]); dev_free(b.st_e[i]); }
     dev_free(b.hits); dev_free(b.sh_a); dev_free(b.sh_b); dev_free(b.sh_c); dev_free(b.radiance); dev_free(b.cnt);
     dev_free(wave_->jobs_dev); dev_free(wave_->segs_dev); dev_free(wave_->prog_dev);
     dev_free(wave_->gen_dev); dev_free(wave_->plan_dev);
@@ -454,6 +454,7 @@ void Engine::ensure_wave() {
     b.st_b[i] = dev_alloc<float4>(P);
     b.st_c[i] = dev_alloc<float4>(P);
     b.st_d[i] = dev_alloc<uint4>(P);
+    b.st_e[i] = dev_alloc<float>(P);
   }
   b.hits = dev_alloc<float4>(P);
   b.sh_a = dev_alloc<float4>(P);
@@ -624,6 +625,7 @@ int Engine::open_job(const JobSpec& spec, bool serving, PassCallback cb) {
   const RtgSceneDev d = job_descriptor(sc, spec.settings, j.frame);
   stage(W.jobs_dev + j.desc_slot, &d, sizeof(d));
   sc.jobs_open++;
+  if (j.settings.light_sampling && j.settings.mis) ++mis_jobs_;
   const int h = j.handle;
   jobs_.emplace(h, std::move(j));
   return h;
@@ -632,6 +634,7 @@ int Engine::open_job(const JobSpec& spec, bool serving, PassCallback cb) {
 void Engine::close_job(Job& j) {
   Wave& W = *wave_;
   W.free_jobs.push_back(j.desc_slot);
+  if (j.settings.light_sampling && j.settings.mis) --mis_jobs_;
   auto it = scenes_.find(j.scene_id);
   if (it != scenes_.end()) it->second->jobs_open--;
 }
@@ -868,9 +871,11 @@ void Engine::launch_one_iteration() {
   const bool timed = cfg_.time_kernels;
   const bool count = cfg_.count_traversal;
   const Stage stages[4] = {Stage::Plan, Stage::Extend, Stage::Shade, Stage::Shadow};
+  LaunchShape shape = cfg_.shape;
+  shape.mis = mis_jobs_ > 0;
   for (int k = 0; k < 4; ++k) {
     if (timed) CK(cudaEventRecord(W.tev[2 * k], stream_));
-    CK(launch_stage(stages[k], W.wb, par, cfg_.shape, count, stream_));
+    CK(launch_stage(stages[k], W.wb, par, shape, count, stream_));
     if (timed) CK(cudaEventRecord(W.tev[2 * k + 1], stream_));
   }
   // After the whole iteration, so no event sits between chained kernels; the

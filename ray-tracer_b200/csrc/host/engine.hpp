@@ -287,6 +287,7 @@ class Engine {
   int next_job_ = 1;
   std::uint64_t job_seq_ = 0;
   std::size_t serve_open_ = 0;
+  int mis_jobs_ = 0;               // open jobs with multiple importance sampling
   bool gen_dirty_ = false;
   WaveCounters last_counters_{};   // from the latest snapshot
   WaveCounters base_counters_{};   // at the start of the current render

@@ -331,7 +331,7 @@ void describe(const CompiledScene& s, const RenderSettings& r, RtgSceneDev& d) {
   d.max_depth = r.max_depth;
   d.rr_min_depth = r.rr_min_depth;
   d.integrator = static_cast<std::int32_t>(r.integrator);
-  d.light_sampling = r.light_sampling ? 1 : 0;
+  d.light_sampling = r.light_sampling ? (r.mis ? 2 : 1) : 0;
   d.use_bvh = r.use_bvh ? 1 : 0;
   d.seed = r.seed;
   d.bg_top = f3h(s.background.top);

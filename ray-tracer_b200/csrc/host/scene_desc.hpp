@@ -42,6 +42,10 @@ struct RenderSettings {
   int threads = 0;      // CPU worker count in the reference; ignored on the GPU
   int tile_size = 16;   // CPU tile edge in the reference; ignored on the GPU
   bool use_bvh = true;  // false selects the brute-force kernel
+  // Multiple importance sampling of next-event estimation and BSDF sampling (power
+  // heuristic). No counterpart in the reference, which lists it as future work;
+  // off by default, and only with light_sampling.
+  bool mis = false;
   bool operator==(const RenderSettings&) const = default;
 };
 

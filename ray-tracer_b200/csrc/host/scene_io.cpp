@@ -240,6 +240,7 @@ SceneDesc scene_from_json(const JsonValue& root) {
     R.max_depth = c.integer("max_depth", R.max_depth);
     R.rr_min_depth = c.integer("rr_min_depth", R.rr_min_depth);
     R.light_sampling = c.flag("light_sampling", R.light_sampling);
+    R.mis = c.flag("mis", R.mis);  // schema extension (no reference counterpart)
     // The seed goes through a 32-bit integer read, as in the reference loader.
     R.seed = static_cast<std::uint64_t>(c.integer("seed", static_cast<int>(R.seed)));
     R.exposure = c.num("exposure", R.exposure);
@@ -323,6 +324,7 @@ JsonValue scene_to_json(const SceneDesc& s) {
   r["rr_min_depth"] = R.rr_min_depth;
   r["integrator"] = integrator_name(R.integrator);
   r["light_sampling"] = R.light_sampling;
+  if (R.mis) r["mis"] = true;
   r["seed"] = R.seed;
   r["tone_map"] = tone_map_name(R.tone_map);
   r["exposure"] = R.exposure;

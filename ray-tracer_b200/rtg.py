@@ -218,10 +218,12 @@ class RenderSettings:
     threads: int = 0
     tile_size: int = 16
     use_bvh: bool = True
+    mis: bool = False  # multiple importance sampling with NEE (no reference counterpart)
 
     def to_c(self) -> _Settings:
+        ls = (2 if self.mis else 1) if self.light_sampling else 0
         return _Settings(self.width, self.height, self.spp, self.max_depth, self.rr_min_depth,
-                         INTEGRATORS[self.integrator], int(self.light_sampling), TONE_MAPS[self.tone_map],
+                         INTEGRATORS[self.integrator], ls, TONE_MAPS[self.tone_map],
                          self.seed, self.exposure, self.threads, self.tile_size, int(self.use_bvh), 0)
 
     @staticmethod
@@ -230,7 +232,7 @@ class RenderSettings:
         inv_t = {v: k for k, v in TONE_MAPS.items()}
         return RenderSettings(c.width, c.height, c.spp, c.max_depth, c.rr_min_depth, inv_i[c.integrator],
                               bool(c.light_sampling), c.seed, inv_t[c.tone_map], c.exposure, c.threads,
-                              c.tile_size, bool(c.use_bvh))
+                              c.tile_size, bool(c.use_bvh), c.light_sampling == 2)
 
 
 @dataclasses.dataclass

@@ -151,3 +151,16 @@ def test_ppm_output_and_output_errors(tmp_path, scene_file):
     assert data.startswith(b"P6\n32 32\n255\n") and len(data) == len(b"P6\n32 32\n255\n") + 32 * 32 * 3
     assert run([str(scene_file), "-o", str(tmp_path / "x.bmp"), "-q"]).returncode == 3
     assert run([str(scene_file), "-o", str(tmp_path / "no" / "dir.png"), "-q"]).returncode == 3
+
+
+@pytest.mark.gpu
+def test_mis_flag(tmp_path, scene_file):
+    """--mis switches the estimator (NEE weighted against BSDF sampling): a
+    different, equally valid image; with --no-light-sampling it changes nothing."""
+    a, b, c, d = (tmp_path / f"{k}.png" for k in "abcd")
+    assert run([str(scene_file), "-o", str(a), "-q"]).returncode == 0
+    assert run([str(scene_file), "-o", str(b), "-q", "--mis"]).returncode == 0
+    assert a.read_bytes() != b.read_bytes()
+    assert run([str(scene_file), "-o", str(c), "-q", "--no-light-sampling"]).returncode == 0
+    assert run([str(scene_file), "-o", str(d), "-q", "--no-light-sampling", "--mis"]).returncode == 0
+    assert c.read_bytes() == d.read_bytes()
