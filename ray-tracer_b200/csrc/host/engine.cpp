@@ -220,13 +220,76 @@ std::vector<int> Engine::add_scenes(const std::vector<std::shared_ptr<const Comp
   work();
   for (auto& t : pool) t.join();
   if (failed) std::rethrow_exception(failed);
+  // All scenes go through one pinned staging buffer, filled on all host cores
+  // (the copy into pinned memory was the serial part of the upload), then one
+  // device block and one copy per scene.
+  CK(cudaSetDevice(device_));
+  std::vector<StagedParts> parts(scenes.size());
+  std::vector<std::size_t> offset(scenes.size());
+  std::size_t total = 0;
+  for (std::size_t k = 0; k < scenes.size(); ++k) {
+    parts[k] = staged_parts(flats[k]);
+    offset[k] = total;
+    total += parts[k].total;
+  }
+  int b = 0;
+  unsigned char* host = upload_staging(std::max<std::size_t>(total, 1), b, 0);
+  next = 0;
+  auto copy = [&] {
+    for (std::size_t k; (k = next.fetch_add(1)) < scenes.size();) stage_flat(flats[k], parts[k], host + offset[k]);
+  };
+  pool.clear();
+  for (std::size_t w = 1; w < workers; ++w) pool.emplace_back(copy);
+  copy();
+  for (auto& t : pool) t.join();
   std::vector<int> ids;
   ids.reserve(scenes.size());
-  for (std::size_t k = 0; k < scenes.size(); ++k) ids.push_back(add_flat(scenes[k], std::move(flats[k])));
+  for (std::size_t k = 0; k < scenes.size(); ++k)
+    ids.push_back(register_flat(scenes[k], std::move(flats[k]), parts[k], host + offset[k]));
+  CK(cudaEventRecord(upload_ev_[b], stream_));
+  upload_pending_[b] = true;
   return ids;
 }
 
+Engine::StagedParts Engine::staged_parts(const FlatScene& f) {
+  StagedParts p{};
+  const std::size_t bytes[8] = {f.nodes.size() * sizeof(DevNode), f.nodes4.size() * sizeof(DevNode4),
+                                f.prims.size() * sizeof(float4), f.slot_material.size() * sizeof(std::uint32_t),
+                                f.slot_normals.size() * sizeof(float4), f.planes.size() * sizeof(DevPlane),
+                                f.materials.size() * sizeof(DevMaterial), f.lights.size() * sizeof(DevLight)};
+  p.total = 0;
+  for (int k = 0; k < 8; ++k) {
+    p.bytes[k] = bytes[k];
+    p.at[k] = p.total;
+    p.total += (std::max<std::size_t>(bytes[k], 1) + 255) & ~std::size_t(255);
+  }
+  return p;
+}
+
+void Engine::stage_flat(const FlatScene& f, const StagedParts& p, unsigned char* dst) {
+  const void* src[8] = {f.nodes.data(), f.nodes4.data(), f.prims.data(), f.slot_material.data(),
+                        f.slot_normals.data(), f.planes.data(), f.materials.data(), f.lights.data()};
+  for (int k = 0; k < 8; ++k)
+    if (p.bytes[k]) std::memcpy(dst + p.at[k], src[k], p.bytes[k]);
+}
+
 int Engine::add_flat(std::shared_ptr<const CompiledScene> scene, FlatScene flat) {
+  // One device allocation and one copy per scene, through a pinned staging
+  // buffer: the copy runs while the caller flattens the next scene (two buffers
+  // alternate), and the flattened vectors can go at once.
+  CK(cudaSetDevice(device_));
+  const StagedParts p = staged_parts(flat);
+  int b = 0;
+  unsigned char* host = upload_staging(p.total, b);
+  stage_flat(flat, p, host);
+  const int id = register_flat(std::move(scene), std::move(flat), p, host);
+  CK(cudaEventRecord(upload_ev_[b], stream_));
+  upload_pending_[b] = true;
+  return id;
+}
+
+int Engine::register_flat(std::shared_ptr<const CompiledScene> scene, FlatScene flat, const StagedParts& p,
+                          const unsigned char* staged) {
   CK(cudaSetDevice(device_));
   auto gs = std::make_unique<GpuScene>();
   gs->root = flat.root;
@@ -236,32 +299,10 @@ int Engine::add_flat(std::shared_ptr<const CompiledScene> scene, FlatScene flat)
   gs->root4 = flat.root4;
   gs->n_interior = static_cast<std::int32_t>(flat.nodes.size());
   gs->n_wide = static_cast<std::int32_t>(flat.nodes4.size());
-  // One device allocation and one copy per scene, through a pinned staging
-  // buffer: the copy runs while the caller flattens the next scene (two buffers
-  // alternate), and the flattened vectors can go at once.
-  struct Part {
-    const void* src;
-    std::size_t bytes;
-    std::size_t at;
-  };
-  auto part = [](const auto& v) { return Part{v.data(), v.size() * sizeof(v[0]), 0}; };
-  Part parts[8] = {part(flat.nodes), part(flat.nodes4), part(flat.prims), part(flat.slot_material),
-                   part(flat.slot_normals), part(flat.planes), part(flat.materials), part(flat.lights)};
-  std::size_t total = 0;
-  for (Part& p : parts) {
-    p.at = total;
-    total += (std::max<std::size_t>(p.bytes, 1) + 255) & ~std::size_t(255);
-  }
   void* block = nullptr;
-  CK(cudaMallocFromPoolAsync(&block, total, pool_, stream_));
-  int b = 0;
-  unsigned char* host = upload_staging(total, b);
-  for (const Part& p : parts)
-    if (p.bytes) std::memcpy(host + p.at, p.src, p.bytes);
-  CK(cudaMemcpyAsync(block, host, total, cudaMemcpyHostToDevice, stream_));
-  CK(cudaEventRecord(upload_ev_[b], stream_));
-  upload_pending_[b] = true;
-  auto at = [&](int k) { return static_cast<void*>(static_cast<unsigned char*>(block) + parts[k].at); };
+  CK(cudaMallocFromPoolAsync(&block, p.total, pool_, stream_));
+  CK(cudaMemcpyAsync(block, staged, p.total, cudaMemcpyHostToDevice, stream_));
+  auto at = [&](int k) { return static_cast<void*>(static_cast<unsigned char*>(block) + p.at[k]); };
   gs->block = block;
   gs->nodes = static_cast<DevNode*>(at(0));
   gs->nodes4 = static_cast<DevNode4*>(at(1));
@@ -271,7 +312,7 @@ int Engine::add_flat(std::shared_ptr<const CompiledScene> scene, FlatScene flat)
   gs->planes = static_cast<DevPlane*>(at(5));
   gs->materials = static_cast<DevMaterial*>(at(6));
   gs->lights = static_cast<DevLight*>(at(7));
-  gs->device_bytes = total;
+  gs->device_bytes = p.total;
   gs->slot_prim = std::move(flat.slot_prim);
   gs->bvh = scene->info.bvh;
   gs->host = std::move(scene);
@@ -280,9 +321,13 @@ int Engine::add_flat(std::shared_ptr<const CompiledScene> scene, FlatScene flat)
   return id;
 }
 
-unsigned char* Engine::upload_staging(std::size_t bytes, int& b) {
-  b = upload_next_;
-  upload_next_ ^= 1;
+unsigned char* Engine::upload_staging(std::size_t bytes, int& b, int want) {
+  if (want >= 0) {
+    b = want;
+  } else {
+    b = upload_next_;
+    upload_next_ ^= 1;
+  }
   if (upload_pending_[b]) CK(cudaEventSynchronize(upload_ev_[b]));
   upload_pending_[b] = false;
   if (upload_cap_[b] < bytes) {

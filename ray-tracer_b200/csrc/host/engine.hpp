@@ -235,9 +235,23 @@ class Engine {
   };
 
   int add_flat(std::shared_ptr<const CompiledScene> scene, FlatScene flat);
+  // Byte offsets of a flattened scene's arrays in its device block (and in its
+  // pinned staging copy): nodes, nodes4, prims, slot_material, slot_normals,
+  // planes, materials, lights, each 256-byte aligned.
+  struct StagedParts {
+    std::size_t at[8], bytes[8], total;
+  };
+  static StagedParts staged_parts(const FlatScene& f);
+  static void stage_flat(const FlatScene& f, const StagedParts& p, unsigned char* dst);
+  // Allocates the scene's device block, queues its copy from `staged` (pinned,
+  // laid out by `p`) and registers the scene.
+  int register_flat(std::shared_ptr<const CompiledScene> scene, FlatScene flat, const StagedParts& p,
+                    const unsigned char* staged);
   // One of the two pinned upload buffers, grown to `bytes`, once its previous copy
   // is done; the caller records upload_ev_[b] after queuing its copy from it.
-  unsigned char* upload_staging(std::size_t bytes, int& b);
+  // want >= 0 picks that buffer instead of alternating (batch uploads use buffer 0,
+  // so only one buffer grows to a whole batch).
+  unsigned char* upload_staging(std::size_t bytes, int& b, int want = -1);
   void ensure_wave();
   GpuFrame make_frame(int w, int h);
   void free_frame(GpuFrame& f);
