@@ -125,6 +125,7 @@ struct Engine::Wave {
 Engine::Engine(int device) : device_(device) {
   CK(cudaSetDevice(device));
   CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&build_stream_, cudaStreamNonBlocking));
   CK(cudaEventCreate(&ev_begin_));
   CK(cudaEventCreate(&ev_end_));
   for (auto& e : upload_ev_) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -162,6 +163,8 @@ Engine::~Engine() {
     cudaEventDestroy(upload_ev_[b]);
     if (upload_host_[b]) cudaFreeHost(upload_host_[b]);
   }
+  cudaStreamSynchronize(build_stream_);
+  cudaStreamDestroy(build_stream_);
   cudaStreamDestroy(stream_);
   cudaMemPoolDestroy(pool_);
 }
@@ -399,15 +402,15 @@ int Engine::add_scene_gpu_bvh(std::shared_ptr<const CompiledScene> scene) {
 
   // Device copy of the inputs plus room for the slot -> primitive map.
   void* in_block = nullptr;
-  CK(cudaMallocFromPoolAsync(&in_block, staged + pad(np * sizeof(std::uint32_t)), pool_, stream_));
+  CK(cudaMallocFromPoolAsync(&in_block, staged + pad(np * sizeof(std::uint32_t)), pool_, build_stream_));
   struct FreeInput {
     void* p;
     cudaStream_t s;
     ~FreeInput() { cudaFreeAsync(p, s); }
-  } free_input{in_block, stream_};
+  } free_input{in_block, build_stream_};
   auto* dev_in = static_cast<unsigned char*>(in_block);
-  CK(cudaMemcpyAsync(dev_in, host, staged, cudaMemcpyHostToDevice, stream_));
-  CK(cudaEventRecord(upload_ev_[b], stream_));
+  CK(cudaMemcpyAsync(dev_in, host, staged, cudaMemcpyHostToDevice, build_stream_));
+  CK(cudaEventRecord(upload_ev_[b], build_stream_));
   upload_pending_[b] = true;
   auto* order = reinterpret_cast<std::uint32_t*>(dev_in + staged);
 
@@ -418,7 +421,7 @@ int Engine::add_scene_gpu_bvh(std::shared_ptr<const CompiledScene> scene) {
   in.normals = reinterpret_cast<const float4*>(dev_in + in_at[2]);
   in.material = reinterpret_cast<const std::uint32_t*>(dev_in + in_at[3]);
   in.items = reinterpret_cast<const std::uint32_t*>(dev_in + in_at[4]);
-  GpuBvhBuilder builder(stream_, pool_);
+  GpuBvhBuilder builder(build_stream_, pool_);
   const GpuBvhCounts c = builder.build(in);
 
   // The scene's arrays, in add_flat's order, in one allocation.
@@ -431,7 +434,7 @@ int Engine::add_scene_gpu_bvh(std::shared_ptr<const CompiledScene> scene) {
     total += pad(part_bytes[k]);
   }
   void* block = nullptr;
-  CK(cudaMallocFromPoolAsync(&block, total, pool_, stream_));
+  CK(cudaMallocFromPoolAsync(&block, total, pool_, build_stream_));
   auto* dst = static_cast<unsigned char*>(block);
   auto gs = std::make_unique<GpuScene>();
   gs->block = block;
@@ -445,11 +448,11 @@ int Engine::add_scene_gpu_bvh(std::shared_ptr<const CompiledScene> scene) {
   gs->lights = reinterpret_cast<DevLight*>(dst + at[7]);
   builder.emit(in, gs->nodes, gs->nodes4, gs->prims, gs->slot_material, gs->slot_normals, order);
   for (int k = 5; k < 8; ++k)
-    if (part_bytes[k]) CK(cudaMemcpyAsync(dst + at[k], dev_in + in_at[k], part_bytes[k], cudaMemcpyDeviceToDevice, stream_));
+    if (part_bytes[k]) CK(cudaMemcpyAsync(dst + at[k], dev_in + in_at[k], part_bytes[k], cudaMemcpyDeviceToDevice, build_stream_));
   gs->slot_prim.resize(n_items);
   if (n_items)
-    CK(cudaMemcpyAsync(gs->slot_prim.data(), order, n_items * sizeof(std::uint32_t), cudaMemcpyDeviceToHost, stream_));
-  CK(cudaStreamSynchronize(stream_));
+    CK(cudaMemcpyAsync(gs->slot_prim.data(), order, n_items * sizeof(std::uint32_t), cudaMemcpyDeviceToHost, build_stream_));
+  CK(cudaStreamSynchronize(build_stream_));
 
   gs->root = n_items ? c.root : kNoRoot;
   gs->root4 = n_items ? c.root4 : kNoRoot;

@@ -279,6 +279,9 @@ class Engine {
 
   int device_;
   cudaStream_t stream_ = nullptr;
+  // GPU BVH builds run here, beside the wavefront: their per-level
+  // synchronisation waits for the build alone, not for queued render iterations.
+  cudaStream_t build_stream_ = nullptr;
   cudaMemPool_t pool_ = nullptr;  // framebuffers and read-back staging
   // Pinned staging for scene uploads (two alternating buffers).
   unsigned char* upload_host_[2] = {nullptr, nullptr};

@@ -62,6 +62,35 @@ def test_request_in_a_mix_is_bit_identical_to_rendering_it_alone(ctx):
         ctx.release(sid)
 
 
+def test_scene_built_on_the_gpu_while_requests_render(ctx):
+    """A cold scene arrives while a request is rendering: its BVH is built on the
+    GPU (on the build stream, beside the wavefront), a preview of it is served, and
+    both requests still give exactly the images they give alone."""
+    busy = workloads.cornell(width=512, height=512, spp=2048)  # ~5e8 samples: still rendering
+    cold = workloads.mesh_stress(width=32, height=24, spp=4)
+    bs = ctx.load_json(json.dumps(busy))
+    bst = ctx.scene_settings(bs)
+    opts = rtg.RenderOptions(progressive=True, max_pass_spp=32)
+    ref_busy = alone(ctx, bs, bst, opts)
+    warm = ctx.upload(rtg.parse_scene(json.dumps(cold)))
+    cst = ctx.scene_settings(warm)
+    ref_cold = alone(ctx, warm, cst, opts)
+    ctx.release(warm)
+    rb = ctx.submit(bs, bst, opts, priority=1)
+    ctx.pump(20.0)
+    assert not ctx.request_progress(rb).finished
+    cs = ctx.upload(rtg.parse_scene(json.dumps(cold), defer_bvh=True))
+    assert ctx.scene_layout(cs, "roots")[0][3] == 1
+    rc = ctx.submit(cs, cst, opts, priority=0)
+    pump_until(ctx, lambda ev: ctx.request_progress(rb).finished and ctx.request_progress(rc).finished)
+    assert ctx.request_mean(rb, bst.width, bst.height).tobytes() == ref_busy[0].tobytes()
+    assert ctx.request_mean(rc, cst.width, cst.height).tobytes() == ref_cold[0].tobytes()
+    for r in (rb, rc):
+        ctx.release_request(r)
+    ctx.release(bs)
+    ctx.release(cs)
+
+
 def test_previews_overtake_a_final_already_rendering(ctx):
     final = workloads.cornell(width=512, height=512, spp=4096)  # ~1e9 samples: renders for a while
     preview = workloads.sphere_field(width=32, height=32, spp=2)
