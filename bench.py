@@ -429,6 +429,20 @@ def run_rtg(a, dist, scenes, desc):
 
         serve = serving.serve(ctx, sids[:32], seconds=a.serve_seconds, rate=200.0, preview_share=0.9, seed=2025)
         serve["scenes"] = min(32, len(sids))
+        # The same loop with 5% of arrivals being previews of the 32 other scenes of
+        # the mix, not resident: compiled on arrival, uploaded with the BVH built on
+        # the GPU or on the host.
+        if len(scenes) > 32:
+            cold_texts = [json.dumps(sc) for sc in scenes[32:]]
+            serve["cold"] = {"share": 0.05, "scenes": len(cold_texts)}
+            for arm, gpu_bvh in (("gpu_bvh", True), ("host_bvh", False)):
+                r = serving.serve(ctx, sids[:32], seconds=min(5.0, a.serve_seconds), rate=200.0, preview_share=0.9,
+                                  seed=2026, cold_texts=cold_texts, cold_share=0.05, cold_gpu_bvh=gpu_bvh)
+                serve["cold"][arm] = {"cold_preview": r.get("cold_preview"),
+                                      "preview_ttfp_ms_p50_p99": [r["preview"]["ttfp_ms_p50"],
+                                                                  r["preview"]["ttfp_ms_p99"]],
+                                      "msamples_per_s": r["msamples_per_s"],
+                                      "upload_calls": r["host_calls"].get("upload")}
 
     # Scenes that are not resident: the BVH built on the host or on the GPU.
     cold = None

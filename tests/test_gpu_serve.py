@@ -178,3 +178,24 @@ def test_poisson_request_loop_serves_every_preview(ctx):
     assert ctx.serve_footprint() == (0, 0, 0)
     for sid in sids:
         ctx.release(sid)
+
+
+def test_poisson_loop_with_cold_scene_previews(ctx):
+    """Previews of scenes that are not resident, compiled on arrival and uploaded
+    with the BVH built on the GPU: every one is served, and each cold scene is
+    released again when its request finishes."""
+    import serving
+
+    mix = workloads.batch_mix(8, seed=4)
+    sids = [ctx.load_json(json.dumps(s)) for s in mix[:4]]
+    cold = [json.dumps(s) for s in mix[4:]]
+    out = serving.serve(ctx, sids, seconds=1.0, rate=100.0, preview_share=0.9, seed=11, cold_texts=cold,
+                        cold_share=0.2, cold_gpu_bvh=True)
+    c = out["cold_preview"]
+    assert c["count"] > 5 and c["first_pass_on_host"] == c["count"] == c["finished"]
+    assert out["host_calls"]["upload"]["count"] == c["count"]
+    assert out["host_calls"]["release_scene"]["count"] == c["count"]
+    assert out["preview"]["first_pass_on_host"] == out["preview"]["count"]
+    assert ctx.serve_footprint() == (0, 0, 0)
+    for sid in sids:
+        ctx.release(sid)
