@@ -277,7 +277,7 @@ def cold_scene_ttfp(ctx, named_scenes, reps=3):
         runs = {"host_bvh": [], "gpu_bvh": []}
         prims = None
         for _ in range(reps):
-            for arm, defer in (("host_bvh", False), ("gpu_bvh", True)):
+            for arm, defer in (("host_bvh", False), ("gpu_bvh", "auto")):
                 t0 = time.perf_counter()
                 host = rtg.parse_scene(text, defer_bvh=defer)
                 t1 = time.perf_counter()

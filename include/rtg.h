@@ -116,8 +116,14 @@ typedef struct rtg_host_scene rtg_host_scene;
 int rtg_compile(const char* scene_json, const char* base_dir, rtg_host_scene** out, char* err, size_t err_cap);
 /* rtg_compile with flags. RTG_COMPILE_DEFER_BVH leaves the BVH out of the host
  * compile (Bvh::build, src/geometry/bvh.cpp:133-163, is skipped; the view below
- * then has no nodes): rtg_scene_upload builds the same tree on the GPU instead. */
+ * then has no nodes): rtg_scene_upload builds the same tree at upload, on the GPU
+ * for scenes of 32,768 primitives or more and on the host below that, where the
+ * host is faster. */
 #define RTG_COMPILE_DEFER_BVH 1u
+/* RTG_COMPILE_AUTO_BVH: the compile builds the tree itself for scenes under 32,768
+ * primitives and defers it to the GPU build for larger ones, so the host work stays
+ * on the compiling thread (not on the thread that uploads). */
+#define RTG_COMPILE_AUTO_BVH 2u
 int rtg_compile_flags(const char* scene_json, const char* base_dir, uint32_t flags, rtg_host_scene** out, char* err,
                       size_t err_cap);
 void rtg_host_scene_free(rtg_host_scene* scene);
@@ -165,8 +171,9 @@ int rtg_device_count(void);
 /* ---- scenes (Scene::compile, src/core/scene.cpp:31-137; load_scene / parse_scene,
  *      src/io/scene_io.cpp:480-502) ---- */
 
-/* Parse, validate, compile (host BVH build) and upload. base_dir resolves
- * relative OBJ paths (may be NULL). */
+/* Parse, validate, compile and upload. The BVH is built on the host for scenes under
+ * 32,768 primitives and on the GPU for larger ones (RTG_COMPILE_AUTO_BVH): the same
+ * tree either way. base_dir resolves relative OBJ paths (may be NULL). */
 int rtg_scene_load_json(rtg_context* ctx, const char* scene_json, const char* base_dir, rtg_scene_id* out);
 int rtg_scene_load_file(rtg_context* ctx, const char* path, rtg_scene_id* out);
 /* Flatten a host-compiled scene to the device layout and copy it to HBM. The
@@ -179,9 +186,10 @@ int rtg_scene_upload_batch(rtg_context* ctx, int32_t n, const rtg_host_scene* co
 /* Uploads a host scene with its BVH built on the GPU: the binned-SAH tree of
  * Bvh::build (src/geometry/bvh.cpp:28-163), node for node, and the device layout
  * derived from it there (byte-identical to what rtg_scene_upload makes from a host
- * build). Host scenes compiled with RTG_COMPILE_DEFER_BVH take this path in
+ * build). Large host scenes compiled with RTG_COMPILE_DEFER_BVH take this path in
  * rtg_scene_upload too. It replaces the host build for scenes that are not
- * resident yet, where that build dominates the time to the first pass. */
+ * resident yet, where that build dominates the time to the first pass. Builds run
+ * on their own high-priority stream, beside any render in flight. */
 int rtg_scene_upload_gpu_bvh(rtg_context* ctx, const rtg_host_scene* scene, rtg_scene_id* out);
 /* Reads back one part of a scene's device layout (tests and tools; no reference
  * counterpart). Copies min(cap, size) bytes to out (out may be NULL) and returns

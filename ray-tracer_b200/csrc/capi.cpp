@@ -257,7 +257,9 @@ int rtg_compile(const char* scene_json, const char* base_dir, rtg_host_scene** o
 
 int rtg_compile_flags(const char* scene_json, const char* base_dir, uint32_t flags, rtg_host_scene** out, char* err,
                       size_t err_cap) {
-  if (!scene_json || !out || (flags & ~uint32_t(RTG_COMPILE_DEFER_BVH))) return RTG_ERR_INVALID;
+  if (!scene_json || !out || (flags & ~uint32_t(RTG_COMPILE_DEFER_BVH | RTG_COMPILE_AUTO_BVH)) ||
+      (flags == (RTG_COMPILE_DEFER_BVH | RTG_COMPILE_AUTO_BVH)))
+    return RTG_ERR_INVALID;
   *out = nullptr;
   auto fail = [&](const char* msg) {
     if (err && err_cap) {
@@ -270,7 +272,10 @@ int rtg_compile_flags(const char* scene_json, const char* base_dir, uint32_t fla
     rtg::SceneDesc d = rtg::parse_scene(scene_json);
     if (base_dir) d.base_dir = base_dir;
     auto hs = std::make_unique<rtg_host_scene>();
-    hs->scene = std::make_shared<const rtg::CompiledScene>(rtg::compile_scene(d, !(flags & RTG_COMPILE_DEFER_BVH)));
+    const rtg::BvhBuild where = (flags & RTG_COMPILE_DEFER_BVH)  ? rtg::BvhBuild::Defer
+                                : (flags & RTG_COMPILE_AUTO_BVH) ? rtg::BvhBuild::Auto
+                                                                 : rtg::BvhBuild::Host;
+    hs->scene = std::make_shared<const rtg::CompiledScene>(rtg::compile_scene(d, where));
     *out = hs.release();
     return RTG_OK;
   } catch (const std::exception& e) {
@@ -432,7 +437,8 @@ int rtg_scene_load_json(rtg_context* ctx, const char* scene_json, const char* ba
     if (!scene_json || !out) throw std::invalid_argument("null argument");
     rtg::SceneDesc d = rtg::parse_scene(scene_json);
     if (base_dir) d.base_dir = base_dir;
-    *out = ctx->engine->add_scene(std::make_shared<const rtg::CompiledScene>(rtg::compile_scene(d)));
+    *out = ctx->engine->add_scene(
+        std::make_shared<const rtg::CompiledScene>(rtg::compile_scene(d, rtg::BvhBuild::Auto)));
     return RTG_OK;
   });
 }
@@ -441,7 +447,8 @@ int rtg_scene_load_file(rtg_context* ctx, const char* path, rtg_scene_id* out) {
   return guarded(ctx, [&]() {
     if (!path || !out) throw std::invalid_argument("null argument");
     const rtg::SceneDesc d = rtg::load_scene(path);
-    *out = ctx->engine->add_scene(std::make_shared<const rtg::CompiledScene>(rtg::compile_scene(d)));
+    *out = ctx->engine->add_scene(
+        std::make_shared<const rtg::CompiledScene>(rtg::compile_scene(d, rtg::BvhBuild::Auto)));
     return RTG_OK;
   });
 }

@@ -225,8 +225,10 @@ int main(int argc, char** argv) {
 
   char err[1024] = {0};
   rtg_host_scene* host = nullptr;
-  if (rtg_compile_flags(text.c_str(), base_dir.c_str(), gpu_bvh ? RTG_COMPILE_DEFER_BVH : 0u, &host, err,
-                        sizeof err) != RTG_OK)
+  // The tree is built where it is faster (host for small scenes, GPU for large);
+  // --gpu-bvh always builds it on the GPU.
+  if (rtg_compile_flags(text.c_str(), base_dir.c_str(), gpu_bvh ? RTG_COMPILE_DEFER_BVH : RTG_COMPILE_AUTO_BVH, &host,
+                        err, sizeof err) != RTG_OK)
     return scene_error(err);
   rtg_scene_view view{};
   rtg_host_scene_view(host, &view);
@@ -270,7 +272,7 @@ int main(int argc, char** argv) {
     return 2;
   }
   rtg_scene_id sid = 0;
-  if (rtg_scene_upload(ctx, host, &sid) != RTG_OK) {
+  if ((gpu_bvh ? rtg_scene_upload_gpu_bvh(ctx, host, &sid) : rtg_scene_upload(ctx, host, &sid)) != RTG_OK) {
     const std::string msg = rtg_last_error(ctx);
     rtg_context_destroy(ctx);
     rtg_host_scene_free(host);

@@ -1276,6 +1276,23 @@ int blocks_for(long long threads, int per_block) {
 
 }  // namespace
 
+void gpu_bvh_preload() {
+  cudaFuncAttributes a;
+  const void* kernels[] = {
+      reinterpret_cast<const void*>(k_init),       reinterpret_cast<const void*>(k_bounds),
+      reinterpret_cast<const void*>(k_bins),       reinterpret_cast<const void*>(k_decide),
+      reinterpret_cast<const void*>(k_pcount),     reinterpret_cast<const void*>(k_pscan),
+      reinterpret_cast<const void*>(k_pranks),     reinterpret_cast<const void*>(k_pswap),
+      reinterpret_cast<const void*>(k_small),      reinterpret_cast<const void*>(k_sizes),
+      reinterpret_cast<const void*>(k_dfs),        reinterpret_cast<const void*>(k_small_dfs),
+      reinterpret_cast<const void*>(k_finish),     reinterpret_cast<const void*>(k_wide_init),
+      reinterpret_cast<const void*>(k_wide),       reinterpret_cast<const void*>(k_scan_block),
+      reinterpret_cast<const void*>(k_scan_sums),  reinterpret_cast<const void*>(k_scan_add),
+      reinterpret_cast<const void*>(k_mark_last),  reinterpret_cast<const void*>(k_emit_nodes),
+      reinterpret_cast<const void*>(k_emit_slots), reinterpret_cast<const void*>(k_emit_wide)};
+  for (const void* k : kernels) BVH_CK(cudaFuncGetAttributes(&a, k));
+}
+
 GpuBvhBuilder::~GpuBvhBuilder() { release(); }
 
 void GpuBvhBuilder::release() {

@@ -47,6 +47,10 @@ struct GpuBvhCounts {
   float build_ms = 0;         // device time of the tree build (CUDA events)
 };
 
+// Loads the build kernels onto the current device now (they are otherwise loaded
+// on first launch, which would stall the first build by milliseconds).
+void gpu_bvh_preload();
+
 // Owns the scratch memory of one build (from `pool`, stream-ordered).
 class GpuBvhBuilder {
  public:

@@ -81,7 +81,7 @@ void parallel_for(std::size_t n, F&& body) {
 
 }  // namespace
 
-CompiledScene compile_scene(const SceneDesc& desc, bool build_bvh) {
+CompiledScene compile_scene(const SceneDesc& desc, BvhBuild where) {
   CompiledScene s;
   s.settings = desc.render;
   s.background = desc.background;
@@ -216,7 +216,7 @@ CompiledScene compile_scene(const SceneDesc& desc, bool build_bvh) {
       s.lights.push_back({LightEntry::kEmitter, static_cast<std::uint32_t>(i)});
   s.info.lights = s.lights.size();
 
-  if (!build_bvh) {
+  if (where == BvhBuild::Defer || (where == BvhBuild::Auto && s.prims.size() >= kGpuBuildMinPrims)) {
     s.bvh_built = false;
     return s;
   }

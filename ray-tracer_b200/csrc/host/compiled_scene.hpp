@@ -68,8 +68,14 @@ struct CompiledScene {
   BuildInfo info;
 };
 
-// build_bvh = false leaves `bvh` empty: the device build (bvh_gpu.h) makes the
-// same tree on the GPU when the scene is uploaded.
-CompiledScene compile_scene(const SceneDesc& desc, bool build_bvh = true);
+// Scenes from this many primitives up build their BVH faster on the GPU than on
+// the host (latency of the GPU build's level passes against the host build's work).
+constexpr std::size_t kGpuBuildMinPrims = 32768;
+
+// Where the BVH is built: in the compile (Host); at upload, on the GPU from
+// kGpuBuildMinPrims primitives up and on the host below (Defer: `bvh` stays empty
+// here); or chosen by size here (Auto: small scenes built now, large ones deferred).
+enum class BvhBuild { Host, Defer, Auto };
+CompiledScene compile_scene(const SceneDesc& desc, BvhBuild where = BvhBuild::Host);
 
 }  // namespace rtg

@@ -125,7 +125,11 @@ struct Engine::Wave {
 Engine::Engine(int device) : device_(device) {
   CK(cudaSetDevice(device));
   CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
-  CK(cudaStreamCreateWithFlags(&build_stream_, cudaStreamNonBlocking));
+  // Highest priority: a build's short kernels take SM slots ahead of the
+  // wavefront's queued blocks, so a cold scene does not wait behind renders.
+  int least = 0, greatest = 0;
+  CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+  CK(cudaStreamCreateWithPriority(&build_stream_, cudaStreamNonBlocking, greatest));
   CK(cudaEventCreate(&ev_begin_));
   CK(cudaEventCreate(&ev_end_));
   for (auto& e : upload_ev_) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -188,7 +192,20 @@ void Engine::reset_wave() {
 }
 
 int Engine::add_scene(std::shared_ptr<const CompiledScene> scene) {
-  if (!scene->bvh_built) return add_scene_gpu_bvh(std::move(scene));
+  if (!scene->bvh_built) {
+    if (scene->prims.size() >= kGpuBuildMinPrims) return add_scene_gpu_bvh(std::move(scene));
+    // Small scene: the host builds the same tree faster than the GPU build's
+    // level-by-level passes can start and finish.
+    auto built = std::make_shared<CompiledScene>(*scene);
+    std::vector<Box> boxes;
+    boxes.reserve(built->prims.size());
+    for (const Prim& p : built->prims) boxes.push_back(p.bounds());
+    built->bvh.build(boxes, 4);
+    built->info.bvh = built->bvh.stats;
+    built->bvh_built = true;
+    FlatScene flat = flatten(*built);
+    return add_flat(std::move(built), std::move(flat));
+  }
   FlatScene flat = flatten(*scene);
   return add_flat(std::move(scene), std::move(flat));
 }
@@ -1138,8 +1155,12 @@ void Engine::release_request(int request) {
 }
 
 void Engine::reserve_pool(std::size_t bytes) {
-  if (bytes <= pool_reserved_) return;
   CK(cudaSetDevice(device_));
+  if (!bvh_preloaded_) {
+    gpu_bvh_preload();
+    bvh_preloaded_ = true;
+  }
+  if (bytes <= pool_reserved_) return;
   void* p = nullptr;
   CK(cudaMallocFromPoolAsync(&p, bytes, pool_, stream_));
   CK(cudaFreeAsync(p, stream_));

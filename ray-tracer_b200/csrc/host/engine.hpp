@@ -132,8 +132,10 @@ class Engine {
   cudaStream_t stream() const { return stream_; }
   EngineConfig& config() { return cfg_; }
 
-  // Host-built scenes are flattened on the host; scenes compiled without a BVH
-  // (compile_scene(desc, false)) get it built on the GPU (add_scene_gpu_bvh).
+  // Host-built scenes are flattened on the host. Scenes compiled without a BVH
+  // (BvhBuild::Defer / Auto) get it built on the GPU (add_scene_gpu_bvh) from
+  // kGpuBuildMinPrims primitives up, and on the host below that; either way the tree
+  // is the same.
   int add_scene(std::shared_ptr<const CompiledScene> scene);
   // Builds the scene's BVH on the GPU (device/bvh_gpu.h), whether or not the host
   // compile holds one, and derives the device layout there.
@@ -290,6 +292,7 @@ class Engine {
   bool upload_pending_[2] = {false, false};
   int upload_next_ = 0;
   std::size_t pool_reserved_ = 0;
+  bool bvh_preloaded_ = false;
   cudaEvent_t ev_begin_ = nullptr, ev_end_ = nullptr;
   EngineConfig cfg_;
   std::unordered_map<int, std::unique_ptr<GpuScene>> scenes_;

@@ -323,6 +323,7 @@ class HostScene:
 
 
 COMPILE_DEFER_BVH = 1
+COMPILE_AUTO_BVH = 2
 # Parts of a scene's device layout (rtg_scene_layout): name -> (part, dtype, record width).
 LAYOUT_PARTS = {
     "nodes": (0, np.float32, 16), "nodes4": (1, np.float32, 32), "prims": (2, np.float32, 12),
@@ -332,14 +333,17 @@ LAYOUT_PARTS = {
 }
 
 
-def parse_scene(scene_json: str, base_dir: Optional[str] = None, defer_bvh: bool = False) -> HostScene:
+def parse_scene(scene_json: str, base_dir: Optional[str] = None, defer_bvh=False) -> HostScene:
     """Parse + validate + compile a scene (raises SceneError with the field path).
 
-    defer_bvh skips the host BVH build; uploading the scene then builds it on the GPU."""
+    defer_bvh=True skips the host BVH build: uploading the scene builds it (on the
+    GPU from 32,768 primitives up). defer_bvh="auto" builds small scenes' trees here
+    and defers only large ones."""
     h = C.c_void_p()
     err = C.create_string_buffer(1024)
+    flags = COMPILE_AUTO_BVH if defer_bvh == "auto" else (COMPILE_DEFER_BVH if defer_bvh else 0)
     rc = lib().rtg_compile_flags(scene_json.encode(), base_dir.encode() if base_dir else None,
-                                 COMPILE_DEFER_BVH if defer_bvh else 0, C.byref(h), err, 1024)
+                                 flags, C.byref(h), err, 1024)
     if rc != RTG_OK:
         raise SceneError(err.value.decode())
     return HostScene(h.value)

@@ -11,7 +11,8 @@ Cold previews (optional) are previews of scenes that are not resident: the scene
 JSON arrives with the request, a worker thread compiles it, the serving thread
 uploads it (with the BVH built on the GPU, or flattened from a host-built tree)
 and submits it; the scene is released when its request finishes. Their TTFP
-includes the compile and the upload.
+includes the compile and the upload. With the GPU build, scenes under 32,768
+primitives still get their tree on the worker (the host is faster there).
 """
 import collections
 import concurrent.futures
@@ -146,7 +147,9 @@ def serve(ctx: rtg.Context, scene_ids, seconds: float = 10.0, rate: float = 200.
         while pending and pending[0].arrival <= t:
             r = pending.popleft()
             if r.kind is COLD:
-                r.future = compiler.submit(lambda text: (rtg.parse_scene(text, None, cold_gpu_bvh), now()), r.text)
+                defer = "auto" if cold_gpu_bvh else False  # small scenes: host tree on the worker
+                r.future = compiler.submit(lambda text, defer=defer: (rtg.parse_scene(text, None, defer), now()),
+                                           r.text)
             waiting[r.kind.name].append(r)
         # Previews first (they may use the reserve), cold previews once compiled;
         # finals while the budget allows and only inside the arrival window.

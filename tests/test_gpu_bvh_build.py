@@ -139,16 +139,20 @@ def test_batched_mix_layouts_match_host_build(ctx):
             raise AssertionError(f"mix scene {k}: {e}") from e
 
 
-def test_deferred_compile_builds_on_the_gpu(ctx):
-    """A scene compiled without its BVH gets it built on the GPU by plain upload,
-    with the same layout as the host-built scene's."""
-    text = json.dumps(workloads.cornell())
-    deferred = rtg.parse_scene(text, defer_bvh=True)
-    assert len(deferred.view()["nodes"]) == 0
+@pytest.mark.parametrize("defer", [True, "auto"])
+@pytest.mark.parametrize("make,gpu", [(workloads.mesh_stress, True), (workloads.cornell, False)])
+def test_deferred_compile_builds_at_upload(ctx, make, gpu, defer):
+    """A scene compiled without its BVH gets it at plain upload: built on the GPU
+    from 32,768 primitives up (the mesh, 174k), on the host below (Cornell, 36),
+    with the same layout as the scene compiled with its tree either way. The
+    automatic mode builds small trees in the compile instead."""
+    text = json.dumps(make())
+    deferred = rtg.parse_scene(text, defer_bvh=defer)
+    assert (len(deferred.view()["nodes"]) == 0) == (defer is True or gpu)
     a = ctx.upload(rtg.parse_scene(text))
     b = ctx.upload(deferred)
     try:
-        assert ctx.scene_layout(b, "roots")[0][3] == 1
+        assert ctx.scene_layout(b, "roots")[0][3] == int(gpu)
         for part in PARTS:
             assert ctx.scene_layout(a, part).tobytes() == ctx.scene_layout(b, part).tobytes(), part
     finally:
