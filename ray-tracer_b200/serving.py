@@ -92,10 +92,10 @@ def serve(ctx: rtg.Context, scene_ids, seconds: float = 10.0, rate: float = 200.
     reqs = poisson_arrivals(scene_ids, seconds, rate, preview_share, seed, cold_texts, cold_share)
     ctx.serve_prepare()  # start-up, outside the timed loop
     if cold_texts:
-        # Start-up for cold scenes too: one upload of the largest maps the memory
-        # its build and staging need, as serve_prepare does for requests.
-        big = max(cold_texts, key=len)
-        ctx.release(ctx.upload(rtg.parse_scene(big, None, "auto" if cold_gpu_bvh else False)))
+        # Start-up for cold scenes too: uploading each once maps the memory their
+        # builds and staging need, as serve_prepare does for requests.
+        for text in cold_texts:
+            ctx.release(ctx.upload(rtg.parse_scene(text, None, "auto" if cold_gpu_bvh else False)))
     pending = collections.deque(reqs)
     waiting = {PREVIEW.name: collections.deque(), FINAL.name: collections.deque(), COLD.name: collections.deque()}
     compiler = concurrent.futures.ThreadPoolExecutor(max_workers=4) if cold_texts else None
