@@ -117,3 +117,42 @@ def test_reference_assets_round_trip_when_present():
         assert np.array_equal(a["prims"], b["prims"]) and np.array_equal(a["nodes"], b["nodes"]), name
         count += 1
     assert count >= 8
+
+
+def test_bvh_placement_flags():
+    """RTG_COMPILE_DEFER_BVH leaves the tree to the upload; RTG_COMPILE_AUTO_BVH
+    builds it in the compile below 32,768 primitives and defers it above. Whatever
+    the compile does, the scene itself (primitives, lights, materials) is the same."""
+    small = json.dumps(workloads.cornell())
+    large = json.dumps(workloads.mesh_stress())
+    assert len(rtg.parse_scene(small, defer_bvh=True).view()["nodes"]) == 0
+    assert len(rtg.parse_scene(small, defer_bvh="auto").view()["nodes"]) > 0
+    host = rtg.parse_scene(large).view()
+    auto = rtg.parse_scene(large, defer_bvh="auto").view()
+    assert len(host["nodes"]) > 0 and len(auto["nodes"]) == 0
+    for k in ("prims", "planes", "lights", "materials", "point_lights"):
+        assert np.array_equal(host[k], auto[k]), k
+
+
+def test_compile_flags_are_checked():
+    import ctypes as C
+
+    h = C.c_void_p()
+    err = C.create_string_buffer(256)
+    text = json.dumps(workloads.cornell()).encode()
+    lib = rtg.lib()
+    assert lib.rtg_compile_flags(text, None, 4, C.byref(h), err, 256) == rtg.RTG_ERR_INVALID
+    assert lib.rtg_compile_flags(text, None, rtg.COMPILE_DEFER_BVH | rtg.COMPILE_AUTO_BVH, C.byref(h), err,
+                                 256) == rtg.RTG_ERR_INVALID
+    assert lib.rtg_compile_flags(text, None, rtg.COMPILE_AUTO_BVH, C.byref(h), err, 256) == rtg.RTG_OK
+    lib.rtg_host_scene_free(h)
+
+
+def test_mis_setting_survives_dump_and_defaults_off():
+    scene = workloads.cornell()
+    assert '"mis"' not in rtg.dump_scene(json.dumps(scene))
+    scene["render"]["mis"] = True
+    dumped = json.loads(rtg.dump_scene(json.dumps(scene)))
+    assert dumped["render"]["mis"] is True
+    st = rtg.parse_scene(json.dumps(dumped)).view()["settings"]
+    assert st.mis and st.light_sampling
