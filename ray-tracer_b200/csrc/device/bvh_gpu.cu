@@ -10,7 +10,6 @@
 #include "device/bvh_gpu.h"
 
 #include <algorithm>
-#include <cstring>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -746,8 +745,9 @@ struct SmallArgs {
   Counters* counters;
 };
 
-// One warp's workspace: the subtree's primitives (position = lane), its bins and
-// its nodes in preorder, and the stack of nodes still to build.
+// One warp's workspace: the subtree's primitives (position = lane), its nodes in
+// preorder, and the stack of nodes still to build. Bins live in registers (one
+// lane per axis and bin).
 struct SmallWarp {
   double box[kSmallItems][6];
   double cen[kSmallItems][3];

@@ -12,13 +12,13 @@
 // layout that results (DevNode, DevNode4, slots) is byte-identical to
 // flatten()'s output for the same scene.
 //
-// Work is split by size. Nodes with more than kSmallItems primitives are built
-// level by level: warps reduce 256-primitive chunks into per-node bounds and
-// bins with atomics on order-preserving integer keys of the doubles, one thread
-// per node runs the SAH sweep, and the partition runs as count / scan / rank /
-// swap passes. A node with at most kSmallItems primitives is built whole, with
-// all its descendants, by one warp in shared memory. Depth-first numbering is
-// then derived from subtree sizes.
+// Work is split by size. Nodes with more than 32 primitives are built level by
+// level: warps reduce 256-primitive chunks into per-node bounds and bins with
+// atomics on order-preserving integer keys of the doubles, one warp per node runs
+// the SAH sweep (16 lanes per axis), and the partition runs as count / scan / rank
+// / swap passes. A node with at most 32 primitives is built whole, with all its
+// descendants, by one warp in shared memory. Depth-first numbering is then
+// derived from subtree sizes.
 #include <cstdint>
 
 #include <cuda_runtime.h>
