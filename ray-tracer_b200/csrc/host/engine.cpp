@@ -452,6 +452,14 @@ int Engine::add_scene_gpu_bvh(std::shared_ptr<const CompiledScene> scene) {
   }
   void* block = nullptr;
   CK(cudaMallocFromPoolAsync(&block, total, pool_, build_stream_));
+  // Freed again if anything below throws; handed to the scene at the end.
+  struct FreeBlock {
+    void* p;
+    cudaStream_t s;
+    ~FreeBlock() {
+      if (p) cudaFreeAsync(p, s);
+    }
+  } free_block{block, build_stream_};
   auto* dst = static_cast<unsigned char*>(block);
   auto gs = std::make_unique<GpuScene>();
   gs->block = block;
@@ -485,6 +493,7 @@ int Engine::add_scene_gpu_bvh(std::shared_ptr<const CompiledScene> scene) {
   gs->bvh.max_leaf = static_cast<std::size_t>(c.max_leaf);
   gs->bvh.build_ms = c.build_ms;
   gs->device_built = true;
+  free_block.p = nullptr;
   gs->host = std::move(scene);
   const int id = next_scene_++;
   scenes_[id] = std::move(gs);
