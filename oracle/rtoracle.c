@@ -16,6 +16,11 @@
  *   integrators    src/rendering/integrator.cpp:14-198
  *   sample loop    src/rendering/renderer.cpp:28-50
  *   tone map       src/rendering/tonemap.cpp:15-37
+ *
+ * One addition is not the reference's: multiple importance sampling
+ * (light_sampling == 2), the GPU renderer's opt-in estimator, restated here so
+ * that its weights can be checked sample by sample. With light_sampling 0 or 1
+ * the code paths are the reference's.
  */
 #include "rtoracle.h"
 
@@ -482,8 +487,11 @@ static v3 background(const ro_scene* s, v3 d) {
 /* ---------------------------------------------------------------- integrators */
 typedef struct { uint64_t rays, shadow, rr, invalid; } counters_t;
 
+/* pdf_out, wi_out (may be NULL): the solid-angle pdf of the sampled direction (0
+ * for a point light) and the direction itself, for the MIS extension's weights. */
 static v3 sample_one_light(const ro_scene* s, uint32_t li, const hit_t* rec, const double* mat, rng_t* rng,
-                           counters_t* st) {
+                           counters_t* st, double* pdf_out, v3* wi_out) {
+  double pdf_l = 0;
   const v3 p = rec->p;
   v3 wi;
   double dist = 0;
@@ -518,6 +526,7 @@ static v3 sample_one_light(const ro_scene* s, uint32_t li, const hit_t* rec, con
         if (cos_l < 1e-9) return V(0, 0, 0);
         const double area = 4 * PI * radius * radius;
         rad = scl(emission(lm), cos_l * area / dd2);
+        pdf_l = dd2 / (cos_l * area);
       } else {
         const double x = r2 / d2;
         const double omc = x / (1 + sqrt(1 - x));
@@ -530,6 +539,7 @@ static v3 sample_one_light(const ro_scene* s, uint32_t li, const hit_t* rec, con
         dist = th;
         const double pdf = 1 / (2 * PI * omc);
         rad = dvs(emission(lm), pdf);
+        pdf_l = pdf;
       }
     } else {
       double b1, b2;
@@ -549,8 +559,11 @@ static v3 sample_one_light(const ro_scene* s, uint32_t li, const hit_t* rec, con
       const double area = 0.5 * len(cross(sub(v1, v0), sub(v2, v0)));
       const double pdf = d2 / (cos_l * area);
       rad = dvs(emission(lm), pdf);
+      pdf_l = pdf;
     }
   }
+  if (pdf_out) *pdf_out = pdf_l;
+  if (wi_out) *wi_out = wi;
   const v3 f = eval_brdf_cos(mat, rec, wi);
   if (is_zero(f) || is_zero(rad)) return V(0, 0, 0);
   const v3 origin = offset_origin(p, rec->gn, wi);
@@ -568,9 +581,35 @@ static int is_sampled_light(const ro_scene* s, const hit_t* rec) {
   return !is_zero(emission(MAT(s, (uint32_t)PRIM(s, rec->prim)[1])));
 }
 
+/* MIS extension: power heuristic (Veach, beta = 2) of pdf a against pdf b. */
+static double power_heuristic(double a, double b) {
+  const double a2 = a * a, b2 = b * b;
+  return a2 + b2 > 0 ? a2 / (a2 + b2) : 0;
+}
+
+/* MIS extension: the solid-angle pdf with which light sampling would have chosen
+ * direction ray.d from ray.o toward the emitter that `rec` hit. */
+static double light_pdf_of_hit(const ro_scene* s, const ray_t* ray, const hit_t* rec) {
+  const double* pr = PRIM(s, rec->prim);
+  const double cos_l = fabs(dot(rec->gn, ray->d));
+  if (pr[0] == 0) {
+    const double r = pr[6], r2 = r * r;
+    const v3 oc = sub(at(pr + 3), ray->o);
+    const double d2 = len2(oc);
+    if (d2 <= r2) return cos_l > 0 ? rec->t * rec->t / (cos_l * 4 * PI * r2) : 0;
+    const double x = r2 / d2;
+    return 1 / (2 * PI * (x / (1 + sqrt(1 - x))));
+  }
+  const v3 v0 = at(pr + 3), v1 = at(pr + 6), v2 = at(pr + 9);
+  const double area = 0.5 * len(cross(sub(v1, v0), sub(v2, v0)));
+  return cos_l > 0 && area > 0 ? rec->t * rec->t / (cos_l * area) : 0;
+}
+
 static v3 path_trace(const ro_scene* s, ray_t ray, rng_t* rng, counters_t* st) {
   v3 L = V(0, 0, 0), beta = V(1, 1, 1);
   int specular_bounce = 1;
+  const int mis = s->light_sampling == 2;
+  double pdf_prev = 0; /* MIS: cosine pdf of the direction the last diffuse bounce sampled */
   for (int depth = 0; depth < s->max_depth; ++depth) {
     hit_t rec;
     st->rays++;
@@ -580,14 +619,25 @@ static v3 path_trace(const ro_scene* s, ray_t ray, rng_t* rng, counters_t* st) {
     }
     const double* mat = MAT(s, rec.material);
     const v3 le = emitted(mat, rec.front);
-    if (!is_zero(le) && (specular_bounce || !s->light_sampling || !is_sampled_light(s, &rec))) L = add(L, mul(beta, le));
+    if (!is_zero(le) && (specular_bounce || !s->light_sampling || !is_sampled_light(s, &rec))) {
+      L = add(L, mul(beta, le));
+    } else if (!is_zero(le) && mis) {
+      const double w = power_heuristic(pdf_prev, light_pdf_of_hit(s, &ray, &rec) / (double)s->n_lights);
+      L = add(L, scl(mul(beta, le), w));
+    }
     scatter_t sr;
     if (!scatter(mat, &ray, &rec, rng, &sr)) break;
     if (s->light_sampling && !sr.specular && s->n_lights > 0) {
       const uint32_t n = (uint32_t)s->n_lights;
       const uint32_t li = below(rng, n);
-      L = add(L, scl(mul(beta, sample_one_light(s, li, &rec, mat, rng, st)), (double)n));
+      double pdf_l = 0;
+      v3 wi = V(0, 0, 0);
+      const v3 c = sample_one_light(s, li, &rec, mat, rng, st, &pdf_l, &wi);
+      double w = 1; /* a point light (pdf 0) cannot be hit by BSDF sampling */
+      if (mis && pdf_l > 0) w = power_heuristic(pdf_l / (double)n, dot(rec.normal, wi) * INV_PI);
+      L = add(L, scl(mul(beta, c), (double)n * w));
     }
+    if (mis && !sr.specular) pdf_prev = dot(rec.normal, sr.dir) * INV_PI;
     beta = mul(beta, sr.weight);
     specular_bounce = sr.specular;
     if (is_zero(beta)) break;
@@ -615,7 +665,8 @@ static v3 direct_trace(const ro_scene* s, ray_t ray, rng_t* rng, counters_t* st,
   if (depth >= s->max_depth) return L;
   const int kind = (int)mat[0];
   if (kind == 0) {
-    for (uint32_t li = 0; li < s->n_lights; ++li) L = add(L, sample_one_light(s, li, &rec, mat, rng, st));
+    for (uint32_t li = 0; li < s->n_lights; ++li)
+      L = add(L, sample_one_light(s, li, &rec, mat, rng, st, NULL, NULL));
     return L;
   }
   if (kind == 1) {

@@ -27,6 +27,7 @@ typedef struct ro_scene {
   const double* materials;    /* 16 per material */
   double camera[19];
   double background[8];
+  /* light_sampling: 0 off, 1 NEE (the reference), 2 NEE with MIS (the GPU's opt-in extension) */
   int32_t width, height, spp, max_depth, rr_min_depth, integrator, light_sampling, use_bvh;
   uint64_t seed;
 } ro_scene;

@@ -89,7 +89,8 @@ class OracleScene:
         s.width, s.height, s.spp = st.width, st.height, st.spp
         s.max_depth, s.rr_min_depth = st.max_depth, st.rr_min_depth
         s.integrator = {"path": 0, "direct": 1, "normals": 2}[st.integrator]
-        s.light_sampling = int(st.light_sampling)
+        # 2: the MIS extension (the GPU's opt-in estimator), 1: the reference's NEE.
+        s.light_sampling = (2 if getattr(st, "mis", False) else 1) if st.light_sampling else 0
         s.use_bvh = int(st.use_bvh)
         s.seed = st.seed
         self.c = s
