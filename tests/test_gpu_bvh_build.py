@@ -175,3 +175,21 @@ def test_gpu_built_scene_renders_identically(ctx):
     finally:
         ctx.release(a)
         ctx.release(b)
+
+
+def test_ray_queries_on_a_gpu_built_scene(ctx):
+    """The ray API maps slots back to primitive ids through the slot map the GPU
+    build read back: closest and any hits on the GPU-built mesh equal the
+    host-built scene's, ray for ray."""
+    host = rtg.parse_scene(json.dumps(workloads.mesh_stress()))
+    rays = workloads.random_rays(host.view(), 100_000, seed=5)
+    a, b = ctx.upload(host), ctx.upload_gpu_bvh(host)
+    try:
+        ra, rb = ctx.trace_closest(a, rays), ctx.trace_closest(b, rays)
+        for x, y in zip(ra, rb):
+            assert np.array_equal(x, y)
+        assert np.array_equal(ctx.trace_any(a, rays), ctx.trace_any(b, rays))
+        assert (ra[1] >= 0).mean() > 0.05
+    finally:
+        ctx.release(a)
+        ctx.release(b)
