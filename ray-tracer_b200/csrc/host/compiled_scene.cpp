@@ -182,11 +182,17 @@ CompiledScene compile_scene(const SceneDesc& desc, BvhBuild where) {
       const std::size_t nf = mesh.faces.size();
       const std::size_t chunks = std::min<std::size_t>(64, (nf + 4095) / 4096);
       std::vector<std::size_t> kept(chunks + 1, 0);
+      std::vector<std::uint8_t> keep(nf);
       auto chunk_range = [&](std::size_t c) { return std::pair{nf * c / chunks, nf * (c + 1) / chunks}; };
       parallel_for(chunks, [&](std::size_t c0, std::size_t c1) {
         for (std::size_t c = c0; c < c1; ++c) {
           const auto [f0, f1] = chunk_range(c);
-          for (std::size_t i = f0; i < f1; ++i) kept[c + 1] += face_prim(mesh.faces[i]).area() >= kMinTriangleArea;
+          for (std::size_t i = f0; i < f1; ++i) {
+            // Prim::area() of the face, from the placed vertices.
+            const auto& f = mesh.faces[i];
+            keep[i] = 0.5 * len(cross(pos[f[1]] - pos[f[0]], pos[f[2]] - pos[f[0]])) >= kMinTriangleArea;
+            kept[c + 1] += keep[i];
+          }
         }
       });
       for (std::size_t c = 0; c < chunks; ++c) kept[c + 1] += kept[c];
@@ -196,10 +202,8 @@ CompiledScene compile_scene(const SceneDesc& desc, BvhBuild where) {
         for (std::size_t c = c0; c < c1; ++c) {
           const auto [f0, f1] = chunk_range(c);
           std::size_t at = base + kept[c];
-          for (std::size_t i = f0; i < f1; ++i) {
-            const Prim t = face_prim(mesh.faces[i]);
-            if (t.area() >= kMinTriangleArea) s.prims[at++] = t;
-          }
+          for (std::size_t i = f0; i < f1; ++i)
+            if (keep[i]) s.prims[at++] = face_prim(mesh.faces[i]);
         }
       });
       s.info.triangles += kept[chunks];
