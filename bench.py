@@ -415,6 +415,10 @@ def run_rtg(a, dist, scenes, desc):
         "kernel": "k_extend (closest-hit BVH traversal + camera-path generation)",
         "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
         "traffic": traffic, "traffic_source": traffic_src, "peak_source": peak_src,
+        # The same launches measured by DRAM bytes (ncu) instead of algorithmic bytes:
+        # node and primitive fetches are mostly L1/L2 hits, so this is far lower.
+        "dram_achieved": traffic / (avg_ms / 1e3) / 1e9 if traffic else None,
+        "dram_frac": traffic / (avg_ms / 1e3) / 1e9 / peak if traffic else None,
         "bytes_per_launch": ext_bytes / launches_ext, "avg_launch_ms": avg_ms, "launches": launches_ext,
         "share_of_kernel_time": t_st["extend_ms"] / kernel_total if kernel_total else None,
         "per_ray": {"nodes": c_st["node_visits"] / max(1, c_st["rays"]),
