@@ -60,11 +60,12 @@ namespace {
 
 constexpr double kMinTriangleArea = 1e-14;  // smaller triangles are dropped as degenerate
 
-// Runs body(begin, end) over [0, n) in contiguous chunks on the host cores.
+// Runs body(begin, end) over [0, n) in contiguous chunks on the host cores, with
+// at least `grain` items per worker.
 template <class F>
-void parallel_for(std::size_t n, F&& body) {
+void parallel_for(std::size_t n, F&& body, std::size_t grain = 1024) {
   const std::size_t workers = std::min<std::size_t>({16, std::max(1u, std::thread::hardware_concurrency()),
-                                                     (n + 1023) / 1024});
+                                                     (n + grain - 1) / grain});
   if (workers <= 1) {
     body(std::size_t(0), n);
     return;
@@ -194,7 +195,7 @@ CompiledScene compile_scene(const SceneDesc& desc, BvhBuild where) {
             kept[c + 1] += keep[i];
           }
         }
-      });
+      }, 1);
       for (std::size_t c = 0; c < chunks; ++c) kept[c + 1] += kept[c];
       const std::size_t base = s.prims.size();
       s.prims.resize(base + kept[chunks]);
@@ -205,7 +206,7 @@ CompiledScene compile_scene(const SceneDesc& desc, BvhBuild where) {
           for (std::size_t i = f0; i < f1; ++i)
             if (keep[i]) s.prims[at++] = face_prim(mesh.faces[i]);
         }
-      });
+      }, 1);
       s.info.triangles += kept[chunks];
       s.info.degenerate_skipped += nf - kept[chunks];
     }
