@@ -1,300 +1,687 @@
+// Scene JSON <-> SceneDesc, driven by one declarative schema.
+//
+// Each record of a scene file (camera, render, background, the four material
+// kinds, the six object kinds, a point light) is described by a table of its
+// fields: JSON key, value kind, whether it is required, and how the value goes
+// into and out of the description. Reading walks a table in order, so the first
+// bad field in table order is the one reported; writing walks the same table
+// (or a record's own write order) and skips fields whose `written` test fails.
+// Validation is a second table per record: range checks with their messages,
+// finiteness and colour checks of vector fields, evaluated over a SceneDesc (the
+// CLI validates again after its command-line overrides).
+//
+// The schema itself — keys, defaults, kinds, ranges, the order problems are
+// found in and every message — is the reference's contract for scene files
+// (src/io/scene_io.cpp:101-473, include/raytracer/core/scene_desc.hpp:20-102), so
+// that the same files are accepted and rejected with the same words.
+// tests/test_scene_schema.py holds the reference CLI's own answers for a corpus
+// of scenes and checks them byte for byte.
 #include "host/scene_io.hpp"
 
 #include <cmath>
 #include <filesystem>
 #include <fstream>
+#include <span>
 #include <sstream>
+#include <utility>
 
 namespace rtg {
 
-const char* integrator_name(Integrator i) {
-  switch (i) {
-    case Integrator::Direct: return "direct";
-    case Integrator::Normals: return "normals";
-    default: return "path";
-  }
-}
-const char* tone_map_name(ToneMap t) {
-  switch (t) {
-    case ToneMap::Clamp: return "clamp";
-    case ToneMap::Reinhard: return "reinhard";
-    default: return "aces";
-  }
-}
-
 namespace {
 
-// Typed field access on one JSON object; errors carry the dotted field path.
-class Fields {
- public:
-  Fields(const JsonValue& v, std::string where) : v_(v), where_(std::move(where)) {
-    if (!v_.is_map()) throw SceneError((where_.empty() ? std::string("scene") : where_) + ": expected an object");
-  }
-  std::string path(const std::string& key) const { return where_.empty() ? key : where_ + "." + key; }
-  const JsonValue* find(const std::string& key) const { return v_.get(key); }
+// ---------------------------------------------------------------------------
+// Values
 
-  double num(const std::string& key, double fallback) const {
-    const JsonValue* f = find(key);
-    if (!f) return fallback;
-    if (!f->is_number()) throw SceneError(path(key) + ": expected a number");
-    return f->number();
-  }
-  int integer(const std::string& key, int fallback) const {
-    const JsonValue* f = find(key);
-    if (!f) return fallback;
-    if (!f->is_number()) throw SceneError(path(key) + ": expected an integer");
-    const double d = f->number();
-    if (d != std::floor(d) || std::fabs(d) > 2e9) throw SceneError(path(key) + ": expected an integer");
-    return static_cast<int>(d);
-  }
-  bool flag(const std::string& key, bool fallback) const {
-    const JsonValue* f = find(key);
-    if (!f) return fallback;
-    if (!f->is_bool()) throw SceneError(path(key) + ": expected true/false");
-    return f->boolean();
-  }
-  std::string text(const std::string& key, const std::string& fallback) const {
-    const JsonValue* f = find(key);
-    if (!f) return fallback;
-    if (!f->is_string()) throw SceneError(path(key) + ": expected a string");
-    return f->str();
-  }
-  std::string required_text(const std::string& key) const {
-    if (!find(key)) throw SceneError(path(key) + ": required");
-    return text(key, "");
-  }
-  // [x, y, z], or a scalar s meaning [s, s, s].
-  D3 vec(const std::string& key, D3 fallback) const {
-    const JsonValue* f = find(key);
-    if (!f) return fallback;
-    if (f->is_number()) return D3{f->number()};
-    if (!f->is_list() || f->list().size() != 3) throw SceneError(path(key) + ": expected [x, y, z]");
-    D3 out;
-    for (int i = 0; i < 3; ++i) {
-      const JsonValue& e = f->list()[static_cast<std::size_t>(i)];
-      if (!e.is_number()) throw SceneError(path(key) + ": expected [x, y, z] of numbers");
-      out.at(i) = e.number();
-    }
-    return out;
-  }
-  D3 required_vec(const std::string& key) const {
-    if (!find(key)) throw SceneError(path(key) + ": required");
-    return vec(key, {});
-  }
+enum class Kind : std::uint8_t { Number, Integer, Flag, Text, Vector };
 
- private:
-  const JsonValue& v_;
-  std::string where_;
+struct Value {
+  double num = 0;
+  int integer = 0;
+  bool flag = false;
+  std::string text;
+  D3 vec;
 };
 
-JsonValue vjson(D3 v) { return JsonList{v.x, v.y, v.z}; }
-
-Material material_from(const Fields& f) {
-  const std::string type = f.required_text("type");
-  if (type == "lambertian" || type == "diffuse") {
-    Lambertian m;
-    m.albedo.a = f.vec("albedo", D3{0.5});
-    m.albedo.b = f.vec("albedo2", m.albedo.a);
-    m.albedo.checker_scale = f.num("checker_scale", 0);
-    return m;
-  }
-  if (type == "metal") return Metal{f.vec("albedo", D3{0.9}), f.num("roughness", 0)};
-  if (type == "dielectric" || type == "glass") return Dielectric{f.num("ior", 1.5), f.vec("tint", D3{1})};
-  if (type == "emissive" || type == "light")
-    return Emissive{f.vec("color", D3{1}), f.num("intensity", 1), f.flag("two_sided", false)};
-  throw SceneError(f.path("type") + ": unknown material type '" + type + "'");
+std::string field_path(const std::string& at, const char* key) {
+  return at.empty() ? std::string(key) : at + "." + key;
 }
 
-JsonValue material_to(const Material& m) {
-  JsonValue j;
-  if (const auto* l = std::get_if<Lambertian>(&m)) {
-    j["type"] = "lambertian";
-    j["albedo"] = vjson(l->albedo.a);
-    if (l->albedo.checker_scale > 0) {
-      j["albedo2"] = vjson(l->albedo.b);
-      j["checker_scale"] = l->albedo.checker_scale;
+[[noreturn]] void reject(const std::string& at, const std::string& what) {
+  throw SceneError((at.empty() ? std::string("scene") : at) + ": " + what);
+}
+
+// Decodes a present JSON value as `kind`; `at` is its field path.
+Value decode(const JsonValue& v, Kind kind, const std::string& at) {
+  Value out;
+  switch (kind) {
+    case Kind::Number:
+      if (!v.is_number()) reject(at, "expected a number");
+      out.num = v.number();
+      break;
+    case Kind::Integer: {
+      if (!v.is_number()) reject(at, "expected an integer");
+      const double d = v.number();
+      if (d != std::floor(d) || std::fabs(d) > 2e9) reject(at, "expected an integer");
+      out.integer = static_cast<int>(d);
+      break;
     }
-  } else if (const auto* me = std::get_if<Metal>(&m)) {
-    j["type"] = "metal";
-    j["albedo"] = vjson(me->albedo);
-    j["roughness"] = me->roughness;
-  } else if (const auto* d = std::get_if<Dielectric>(&m)) {
-    j["type"] = "dielectric";
-    j["ior"] = d->ior;
-    j["tint"] = vjson(d->tint);
-  } else {
-    const auto& e = std::get<Emissive>(m);
-    j["type"] = "emissive";
-    j["color"] = vjson(e.color);
-    j["intensity"] = e.intensity;
-    if (e.two_sided) j["two_sided"] = true;
+    case Kind::Flag:
+      if (!v.is_bool()) reject(at, "expected true/false");
+      out.flag = v.boolean();
+      break;
+    case Kind::Text:
+      if (!v.is_string()) reject(at, "expected a string");
+      out.text = v.str();
+      break;
+    case Kind::Vector:
+      if (v.is_number()) {  // a scalar s stands for [s, s, s]
+        out.vec = D3{v.number()};
+        break;
+      }
+      if (!v.is_list() || v.list().size() != 3) reject(at, "expected [x, y, z]");
+      for (int k = 0; k < 3; ++k) {
+        const JsonValue& e = v.list()[static_cast<std::size_t>(k)];
+        if (!e.is_number()) reject(at, "expected [x, y, z] of numbers");
+        out.vec.at(k) = e.number();
+      }
+      break;
   }
+  return out;
+}
+
+JsonValue vec_json(D3 v) { return JsonList{v.x, v.y, v.z}; }
+
+// Named choices of an enumerated text field: "expected a, b or c" when unknown.
+template <class E>
+struct Choice {
+  const char* name;
+  E value;
+};
+
+template <class E, std::size_t N>
+E choose(const Choice<E> (&options)[N], const std::string& text, const std::string& at) {
+  for (const auto& o : options)
+    if (text == o.name) return o.value;
+  std::string list;
+  for (std::size_t i = 0; i < N; ++i) list += (i == 0 ? "" : (i + 1 == N ? " or " : ", ")) + std::string(options[i].name);
+  reject(at, "expected " + list);
+}
+
+template <class E, std::size_t N>
+const char* choice_name(const Choice<E> (&options)[N], E value) {
+  for (const auto& o : options)
+    if (o.value == value) return o.name;
+  return options[0].name;
+}
+
+constexpr Choice<Integrator> kIntegrators[] = {
+    {"path", Integrator::Path}, {"direct", Integrator::Direct}, {"normals", Integrator::Normals}};
+constexpr Choice<ToneMap> kToneMaps[] = {
+    {"clamp", ToneMap::Clamp}, {"reinhard", ToneMap::Reinhard}, {"aces", ToneMap::Aces}};
+constexpr Choice<Background::Kind> kBackgrounds[] = {
+    {"gradient", Background::Kind::Gradient}, {"solid", Background::Kind::Solid}};
+constexpr Choice<MeshDesc::Source> kMeshSources[] = {
+    {"icosphere", MeshDesc::Source::Icosphere}, {"torus", MeshDesc::Source::Torus}, {"obj", MeshDesc::Source::ObjFile}};
+
+// ---------------------------------------------------------------------------
+// Field tables
+
+// One field of record type R. `put` stores a decoded value (`at` is the field's
+// path, for enumeration errors); `get` gives it back for writing. `read_if` and
+// `written` gate the field on the record's other fields (null: always).
+template <class R>
+struct Field {
+  const char* key;
+  Kind kind;
+  bool required;
+  void (*put)(R&, Value&&, const std::string& at);
+  JsonValue (*get)(const R&);
+  bool (*read_if)(const R&) = nullptr;
+  bool (*written)(const R&) = nullptr;
+};
+
+// Reads the fields of `table` from `j` (a map) into `rec`, in table order.
+template <class R>
+void read_fields(std::span<const Field<R>> table, const JsonValue& j, const std::string& at, R& rec) {
+  for (const Field<R>& f : table) {
+    if (f.read_if && !f.read_if(rec)) continue;
+    const std::string where = field_path(at, f.key);
+    const JsonValue* v = j.get(f.key);
+    if (!v) {
+      if (f.required) reject(where, "required");
+      continue;
+    }
+    f.put(rec, decode(*v, f.kind, where), where);
+  }
+}
+
+template <class R>
+void write_fields(std::span<const Field<R>> table, const R& rec, JsonValue& j) {
+  for (const Field<R>& f : table)
+    if (!f.written || f.written(rec)) j[f.key] = f.get(rec);
+}
+
+// A map record: rejects anything else with "<path>: expected an object".
+const JsonValue& record(const JsonValue& j, const std::string& at) {
+  if (!j.is_map()) reject(at, "expected an object");
   return j;
 }
 
-ObjectDesc object_from(const Fields& f) {
-  ObjectDesc o;
-  const std::string type = f.required_text("type");
-  o.name = f.text("name", type);
-  o.material = f.required_text("material");
-  if (type == "sphere") {
-    o.shape = SphereDesc{f.required_vec("center"), f.num("radius", 1)};
-  } else if (type == "plane") {
-    o.shape = PlaneDesc{f.vec("point", {}), f.vec("normal", {0, 1, 0})};
-  } else if (type == "triangle") {
-    o.shape = TriangleDesc{f.required_vec("v0"), f.required_vec("v1"), f.required_vec("v2")};
-  } else if (type == "quad") {
-    o.shape = QuadDesc{f.required_vec("corner"), f.required_vec("u"), f.required_vec("v")};
-  } else if (type == "box") {
-    o.shape = BoxDesc{f.required_vec("min"), f.required_vec("max"), f.num("rotate_y", 0)};
-  } else if (type == "mesh") {
-    MeshDesc m;
-    const std::string src = f.text("source", "icosphere");
-    if (src == "icosphere") m.source = MeshDesc::Source::Icosphere;
-    else if (src == "torus") m.source = MeshDesc::Source::Torus;
-    else if (src == "obj") m.source = MeshDesc::Source::ObjFile;
-    else throw SceneError(f.path("source") + ": expected icosphere, torus or obj");
-    m.subdivisions = f.integer("subdivisions", m.subdivisions);
-    m.major_radius = f.num("major_radius", m.major_radius);
-    m.minor_radius = f.num("minor_radius", m.minor_radius);
-    m.segments = f.integer("segments", m.segments);
-    m.segments_v = f.integer("segments_v", 0);
-    m.path = f.text("path", "");
-    m.smooth = f.flag("smooth", true);
-    m.scale = f.vec("scale", {1, 1, 1});
-    m.rotate_y = f.num("rotate_y", 0);
-    m.translate = f.vec("translate", {0, 0, 0});
-    o.shape = m;
-  } else {
-    throw SceneError(f.path("type") + ": unknown object type '" + type + "'");
+const Field<CameraDesc> kCameraFields[] = {
+    {"look_from", Kind::Vector, false, [](CameraDesc& c, Value&& v, const std::string&) { c.look_from = v.vec; },
+     [](const CameraDesc& c) { return vec_json(c.look_from); }},
+    {"look_at", Kind::Vector, false, [](CameraDesc& c, Value&& v, const std::string&) { c.look_at = v.vec; },
+     [](const CameraDesc& c) { return vec_json(c.look_at); }},
+    {"vup", Kind::Vector, false, [](CameraDesc& c, Value&& v, const std::string&) { c.vup = v.vec; },
+     [](const CameraDesc& c) { return vec_json(c.vup); }},
+    {"vfov", Kind::Number, false, [](CameraDesc& c, Value&& v, const std::string&) { c.vfov_deg = v.num; },
+     [](const CameraDesc& c) { return JsonValue(c.vfov_deg); }},
+    {"aperture", Kind::Number, false, [](CameraDesc& c, Value&& v, const std::string&) { c.aperture = v.num; },
+     [](const CameraDesc& c) { return JsonValue(c.aperture); }},
+    {"focus_dist", Kind::Number, false, [](CameraDesc& c, Value&& v, const std::string&) { c.focus_dist = v.num; },
+     [](const CameraDesc& c) { return JsonValue(c.focus_dist); }},
+};
+
+const Field<RenderSettings> kRenderFields[] = {
+    {"width", Kind::Integer, false, [](RenderSettings& r, Value&& v, const std::string&) { r.width = v.integer; },
+     [](const RenderSettings& r) { return JsonValue(r.width); }},
+    {"height", Kind::Integer, false, [](RenderSettings& r, Value&& v, const std::string&) { r.height = v.integer; },
+     [](const RenderSettings& r) { return JsonValue(r.height); }},
+    {"spp", Kind::Integer, false, [](RenderSettings& r, Value&& v, const std::string&) { r.spp = v.integer; },
+     [](const RenderSettings& r) { return JsonValue(r.spp); }},
+    {"max_depth", Kind::Integer, false, [](RenderSettings& r, Value&& v, const std::string&) { r.max_depth = v.integer; },
+     [](const RenderSettings& r) { return JsonValue(r.max_depth); }},
+    {"rr_min_depth", Kind::Integer, false,
+     [](RenderSettings& r, Value&& v, const std::string&) { r.rr_min_depth = v.integer; },
+     [](const RenderSettings& r) { return JsonValue(r.rr_min_depth); }},
+    {"light_sampling", Kind::Flag, false,
+     [](RenderSettings& r, Value&& v, const std::string&) { r.light_sampling = v.flag; },
+     [](const RenderSettings& r) { return JsonValue(r.light_sampling); }},
+    // Schema extension (no reference counterpart): written only when set.
+    {"mis", Kind::Flag, false, [](RenderSettings& r, Value&& v, const std::string&) { r.mis = v.flag; },
+     [](const RenderSettings&) { return JsonValue(true); }, nullptr, [](const RenderSettings& r) { return r.mis; }},
+    // The seed is read as a 32-bit integer (and sign-extended), as the reference's loader reads it.
+    {"seed", Kind::Integer, false,
+     [](RenderSettings& r, Value&& v, const std::string&) { r.seed = static_cast<std::uint64_t>(v.integer); },
+     [](const RenderSettings& r) { return JsonValue(r.seed); }},
+    {"exposure", Kind::Number, false, [](RenderSettings& r, Value&& v, const std::string&) { r.exposure = v.num; },
+     [](const RenderSettings& r) { return JsonValue(r.exposure); }},
+    {"threads", Kind::Integer, false, [](RenderSettings& r, Value&& v, const std::string&) { r.threads = v.integer; },
+     [](const RenderSettings& r) { return JsonValue(r.threads); }},
+    {"tile_size", Kind::Integer, false,
+     [](RenderSettings& r, Value&& v, const std::string&) { r.tile_size = v.integer; },
+     [](const RenderSettings& r) { return JsonValue(r.tile_size); }},
+    {"use_bvh", Kind::Flag, false, [](RenderSettings& r, Value&& v, const std::string&) { r.use_bvh = v.flag; },
+     [](const RenderSettings& r) { return JsonValue(r.use_bvh); }},
+    {"integrator", Kind::Text, false,
+     [](RenderSettings& r, Value&& v, const std::string& at) { r.integrator = choose(kIntegrators, v.text, at); },
+     [](const RenderSettings& r) { return JsonValue(choice_name(kIntegrators, r.integrator)); }},
+    {"tone_map", Kind::Text, false,
+     [](RenderSettings& r, Value&& v, const std::string& at) { r.tone_map = choose(kToneMaps, v.text, at); },
+     [](const RenderSettings& r) { return JsonValue(choice_name(kToneMaps, r.tone_map)); }},
+};
+// The normalised file lists the render block in this order.
+constexpr const char* kRenderWriteOrder[] = {"width", "height", "spp", "max_depth", "rr_min_depth", "integrator",
+                                             "light_sampling", "mis", "seed", "tone_map", "exposure", "threads",
+                                             "tile_size", "use_bvh"};
+
+bool is_solid(const Background& b) { return b.kind == Background::Kind::Solid; }
+
+// A solid background keeps its colour in `top` and reads it from "color".
+const Field<Background> kBackgroundFields[] = {
+    {"type", Kind::Text, false,
+     [](Background& b, Value&& v, const std::string& at) { b.kind = choose(kBackgrounds, v.text, at); },
+     [](const Background& b) { return JsonValue(choice_name(kBackgrounds, b.kind)); }},
+    {"color", Kind::Vector, false, [](Background& b, Value&& v, const std::string&) { b.top = v.vec; },
+     [](const Background& b) { return vec_json(b.top); }, is_solid, is_solid},
+    {"top", Kind::Vector, false, [](Background& b, Value&& v, const std::string&) { b.top = v.vec; },
+     [](const Background& b) { return vec_json(b.top); }, [](const Background& b) { return !is_solid(b); },
+     [](const Background& b) { return !is_solid(b); }},
+    {"bottom", Kind::Vector, false, [](Background& b, Value&& v, const std::string&) { b.bottom = v.vec; },
+     [](const Background& b) { return vec_json(b.bottom); }, nullptr, [](const Background& b) { return !is_solid(b); }},
+    {"intensity", Kind::Number, false, [](Background& b, Value&& v, const std::string&) { b.intensity = v.num; },
+     [](const Background& b) { return JsonValue(b.intensity); }},
+};
+
+const Field<PointLightDesc> kLightFields[] = {
+    {"name", Kind::Text, false, [](PointLightDesc& l, Value&& v, const std::string&) { l.name = std::move(v.text); },
+     [](const PointLightDesc& l) { return JsonValue(l.name); }},
+    {"position", Kind::Vector, true, [](PointLightDesc& l, Value&& v, const std::string&) { l.position = v.vec; },
+     [](const PointLightDesc& l) { return vec_json(l.position); }},
+    {"intensity", Kind::Vector, false, [](PointLightDesc& l, Value&& v, const std::string&) { l.intensity = v.vec; },
+     [](const PointLightDesc& l) { return vec_json(l.intensity); }},
+};
+
+// ---------------------------------------------------------------------------
+// Kinds of a variant: the schema of each alternative (its type names, fields
+// and validation rules) is a specialisation of Schema<T>.
+
+template <class T>
+struct Schema;
+
+// Validation rule of record type R. Check: `ok` must hold, else `message`.
+// Finite: the vector must be finite. Colour: finite, and no component below 0.
+template <class R>
+struct Rule {
+  enum Kind : std::uint8_t { Check, Finite, Colour } kind;
+  const char* field;  // appended to the record's path; "" names the record itself
+  const char* message = nullptr;
+  bool (*ok)(const R&) = nullptr;
+  D3 (*vec)(const R&) = nullptr;
+};
+
+template <class R>
+Rule<R> check(const char* field, const char* message, bool (*ok)(const R&)) {
+  return Rule<R>{Rule<R>::Check, field, message, ok, nullptr};
+}
+template <class R>
+Rule<R> finite(const char* field, D3 (*vec)(const R&)) {
+  return Rule<R>{Rule<R>::Finite, field, nullptr, nullptr, vec};
+}
+template <class R>
+Rule<R> colour(const char* field, D3 (*vec)(const R&)) {
+  return Rule<R>{Rule<R>::Colour, field, nullptr, nullptr, vec};
+}
+
+// Appends every problem of `rec` (at path `at`) to `out`, in rule order.
+template <class R>
+void apply_rules(std::span<const Rule<R>> rules, const R& rec, const std::string& at, std::vector<std::string>& out) {
+  for (const Rule<R>& r : rules) {
+    const std::string where = *r.field ? field_path(at, r.field) : at;
+    if (r.kind == Rule<R>::Check) {
+      if (!r.ok(rec)) out.push_back(where + ": " + r.message);
+      continue;
+    }
+    const D3 v = r.vec(rec);
+    if (!v.finite()) out.push_back(where + ": must be finite");
+    if (r.kind == Rule<R>::Colour && (v.x < 0 || v.y < 0 || v.z < 0))
+      out.push_back(where + ": colour components must be >= 0");
   }
+}
+
+bool finite_positive(double x) { return x > 0 && std::isfinite(x); }
+
+template <>
+struct Schema<Lambertian> {
+  static constexpr const char* names[] = {"lambertian", "diffuse"};
+  static inline const Field<Lambertian> fields[] = {
+      {"albedo", Kind::Vector, false,
+       [](Lambertian& m, Value&& v, const std::string&) { m.albedo.a = m.albedo.b = v.vec; },
+       [](const Lambertian& m) { return vec_json(m.albedo.a); }},
+      // Absent: the second checker colour is the first (set together above).
+      {"albedo2", Kind::Vector, false, [](Lambertian& m, Value&& v, const std::string&) { m.albedo.b = v.vec; },
+       [](const Lambertian& m) { return vec_json(m.albedo.b); }, nullptr,
+       [](const Lambertian& m) { return m.albedo.checker_scale > 0; }},
+      {"checker_scale", Kind::Number, false,
+       [](Lambertian& m, Value&& v, const std::string&) { m.albedo.checker_scale = v.num; },
+       [](const Lambertian& m) { return JsonValue(m.albedo.checker_scale); }, nullptr,
+       [](const Lambertian& m) { return m.albedo.checker_scale > 0; }},
+  };
+  static inline const Rule<Lambertian> rules[] = {
+      colour<Lambertian>("albedo", [](const Lambertian& m) { return m.albedo.a; }),
+      colour<Lambertian>("albedo2", [](const Lambertian& m) { return m.albedo.b; }),
+      check<Lambertian>("checker_scale", "must be >= 0", [](const Lambertian& m) { return !(m.albedo.checker_scale < 0); }),
+  };
+};
+
+template <>
+struct Schema<Metal> {
+  static constexpr const char* names[] = {"metal"};
+  static inline const Field<Metal> fields[] = {
+      {"albedo", Kind::Vector, false, [](Metal& m, Value&& v, const std::string&) { m.albedo = v.vec; },
+       [](const Metal& m) { return vec_json(m.albedo); }},
+      {"roughness", Kind::Number, false, [](Metal& m, Value&& v, const std::string&) { m.roughness = v.num; },
+       [](const Metal& m) { return JsonValue(m.roughness); }},
+  };
+  static inline const Rule<Metal> rules[] = {
+      colour<Metal>("albedo", [](const Metal& m) { return m.albedo; }),
+      check<Metal>("roughness", "must be in [0, 1]", [](const Metal& m) { return !(m.roughness < 0 || m.roughness > 1); }),
+  };
+};
+
+template <>
+struct Schema<Dielectric> {
+  static constexpr const char* names[] = {"dielectric", "glass"};
+  static inline const Field<Dielectric> fields[] = {
+      {"ior", Kind::Number, false, [](Dielectric& m, Value&& v, const std::string&) { m.ior = v.num; },
+       [](const Dielectric& m) { return JsonValue(m.ior); }},
+      {"tint", Kind::Vector, false, [](Dielectric& m, Value&& v, const std::string&) { m.tint = v.vec; },
+       [](const Dielectric& m) { return vec_json(m.tint); }},
+  };
+  static inline const Rule<Dielectric> rules[] = {
+      check<Dielectric>("ior", "must be in [1, 4]", [](const Dielectric& m) { return m.ior >= 1.0 && m.ior <= 4.0; }),
+      colour<Dielectric>("tint", [](const Dielectric& m) { return m.tint; }),
+  };
+};
+
+template <>
+struct Schema<Emissive> {
+  static constexpr const char* names[] = {"emissive", "light"};
+  static inline const Field<Emissive> fields[] = {
+      {"color", Kind::Vector, false, [](Emissive& m, Value&& v, const std::string&) { m.color = v.vec; },
+       [](const Emissive& m) { return vec_json(m.color); }},
+      {"intensity", Kind::Number, false, [](Emissive& m, Value&& v, const std::string&) { m.intensity = v.num; },
+       [](const Emissive& m) { return JsonValue(m.intensity); }},
+      {"two_sided", Kind::Flag, false, [](Emissive& m, Value&& v, const std::string&) { m.two_sided = v.flag; },
+       [](const Emissive&) { return JsonValue(true); }, nullptr, [](const Emissive& m) { return m.two_sided; }},
+  };
+  static inline const Rule<Emissive> rules[] = {
+      colour<Emissive>("color", [](const Emissive& m) { return m.color; }),
+      check<Emissive>("intensity", "must be >= 0", [](const Emissive& m) { return m.intensity >= 0 && std::isfinite(m.intensity); }),
+  };
+};
+
+template <>
+struct Schema<SphereDesc> {
+  static constexpr const char* names[] = {"sphere"};
+  static inline const Field<SphereDesc> fields[] = {
+      {"center", Kind::Vector, true, [](SphereDesc& s, Value&& v, const std::string&) { s.center = v.vec; },
+       [](const SphereDesc& s) { return vec_json(s.center); }},
+      {"radius", Kind::Number, false, [](SphereDesc& s, Value&& v, const std::string&) { s.radius = v.num; },
+       [](const SphereDesc& s) { return JsonValue(s.radius); }},
+  };
+  static inline const Rule<SphereDesc> rules[] = {
+      finite<SphereDesc>("center", [](const SphereDesc& s) { return s.center; }),
+      check<SphereDesc>("radius", "must be > 0", [](const SphereDesc& s) { return finite_positive(s.radius); }),
+  };
+};
+
+template <>
+struct Schema<PlaneDesc> {
+  static constexpr const char* names[] = {"plane"};
+  static inline const Field<PlaneDesc> fields[] = {
+      {"point", Kind::Vector, false, [](PlaneDesc& p, Value&& v, const std::string&) { p.point = v.vec; },
+       [](const PlaneDesc& p) { return vec_json(p.point); }},
+      {"normal", Kind::Vector, false, [](PlaneDesc& p, Value&& v, const std::string&) { p.normal = v.vec; },
+       [](const PlaneDesc& p) { return vec_json(p.normal); }},
+  };
+  static inline const Rule<PlaneDesc> rules[] = {
+      finite<PlaneDesc>("point", [](const PlaneDesc& p) { return p.point; }),
+      finite<PlaneDesc>("normal", [](const PlaneDesc& p) { return p.normal; }),
+      check<PlaneDesc>("normal", "must be non-zero", [](const PlaneDesc& p) { return !(len(p.normal) < 1e-9); }),
+  };
+};
+
+template <>
+struct Schema<TriangleDesc> {
+  static constexpr const char* names[] = {"triangle"};
+  static inline const Field<TriangleDesc> fields[] = {
+      {"v0", Kind::Vector, true, [](TriangleDesc& t, Value&& v, const std::string&) { t.v0 = v.vec; },
+       [](const TriangleDesc& t) { return vec_json(t.v0); }},
+      {"v1", Kind::Vector, true, [](TriangleDesc& t, Value&& v, const std::string&) { t.v1 = v.vec; },
+       [](const TriangleDesc& t) { return vec_json(t.v1); }},
+      {"v2", Kind::Vector, true, [](TriangleDesc& t, Value&& v, const std::string&) { t.v2 = v.vec; },
+       [](const TriangleDesc& t) { return vec_json(t.v2); }},
+  };
+  static inline const Rule<TriangleDesc> rules[] = {
+      finite<TriangleDesc>("v0", [](const TriangleDesc& t) { return t.v0; }),
+      finite<TriangleDesc>("v1", [](const TriangleDesc& t) { return t.v1; }),
+      finite<TriangleDesc>("v2", [](const TriangleDesc& t) { return t.v2; }),
+      check<TriangleDesc>("", "triangle is degenerate",
+                          [](const TriangleDesc& t) { return !(len(cross(t.v1 - t.v0, t.v2 - t.v0)) < 1e-12); }),
+  };
+};
+
+template <>
+struct Schema<QuadDesc> {
+  static constexpr const char* names[] = {"quad"};
+  static inline const Field<QuadDesc> fields[] = {
+      {"corner", Kind::Vector, true, [](QuadDesc& q, Value&& v, const std::string&) { q.corner = v.vec; },
+       [](const QuadDesc& q) { return vec_json(q.corner); }},
+      {"u", Kind::Vector, true, [](QuadDesc& q, Value&& v, const std::string&) { q.u = v.vec; },
+       [](const QuadDesc& q) { return vec_json(q.u); }},
+      {"v", Kind::Vector, true, [](QuadDesc& q, Value&& v, const std::string&) { q.v = v.vec; },
+       [](const QuadDesc& q) { return vec_json(q.v); }},
+  };
+  static inline const Rule<QuadDesc> rules[] = {
+      finite<QuadDesc>("corner", [](const QuadDesc& q) { return q.corner; }),
+      finite<QuadDesc>("u", [](const QuadDesc& q) { return q.u; }),
+      finite<QuadDesc>("v", [](const QuadDesc& q) { return q.v; }),
+      check<QuadDesc>("", "quad is degenerate (u parallel to v)",
+                      [](const QuadDesc& q) { return !(len(cross(q.u, q.v)) < 1e-12); }),
+  };
+};
+
+template <>
+struct Schema<BoxDesc> {
+  static constexpr const char* names[] = {"box"};
+  static inline const Field<BoxDesc> fields[] = {
+      {"min", Kind::Vector, true, [](BoxDesc& b, Value&& v, const std::string&) { b.min = v.vec; },
+       [](const BoxDesc& b) { return vec_json(b.min); }},
+      {"max", Kind::Vector, true, [](BoxDesc& b, Value&& v, const std::string&) { b.max = v.vec; },
+       [](const BoxDesc& b) { return vec_json(b.max); }},
+      {"rotate_y", Kind::Number, false, [](BoxDesc& b, Value&& v, const std::string&) { b.rotate_y = v.num; },
+       [](const BoxDesc& b) { return JsonValue(b.rotate_y); }},
+  };
+  static inline const Rule<BoxDesc> rules[] = {
+      finite<BoxDesc>("min", [](const BoxDesc& b) { return b.min; }),
+      finite<BoxDesc>("max", [](const BoxDesc& b) { return b.max; }),
+      check<BoxDesc>("", "box max must exceed min on every axis",
+                     [](const BoxDesc& b) { return b.max.x > b.min.x && b.max.y > b.min.y && b.max.z > b.min.z; }),
+  };
+};
+
+bool mesh_is(const MeshDesc& m, MeshDesc::Source s) { return m.source == s; }
+
+template <>
+struct Schema<MeshDesc> {
+  static constexpr const char* names[] = {"mesh"};
+  static inline const Field<MeshDesc> fields[] = {
+      {"source", Kind::Text, false,
+       [](MeshDesc& m, Value&& v, const std::string& at) { m.source = choose(kMeshSources, v.text, at); },
+       [](const MeshDesc& m) { return JsonValue(choice_name(kMeshSources, m.source)); }},
+      {"subdivisions", Kind::Integer, false, [](MeshDesc& m, Value&& v, const std::string&) { m.subdivisions = v.integer; },
+       [](const MeshDesc& m) { return JsonValue(m.subdivisions); }, nullptr,
+       [](const MeshDesc& m) { return mesh_is(m, MeshDesc::Source::Icosphere); }},
+      {"major_radius", Kind::Number, false, [](MeshDesc& m, Value&& v, const std::string&) { m.major_radius = v.num; },
+       [](const MeshDesc& m) { return JsonValue(m.major_radius); }, nullptr,
+       [](const MeshDesc& m) { return mesh_is(m, MeshDesc::Source::Torus); }},
+      {"minor_radius", Kind::Number, false, [](MeshDesc& m, Value&& v, const std::string&) { m.minor_radius = v.num; },
+       [](const MeshDesc& m) { return JsonValue(m.minor_radius); }, nullptr,
+       [](const MeshDesc& m) { return mesh_is(m, MeshDesc::Source::Torus); }},
+      {"segments", Kind::Integer, false, [](MeshDesc& m, Value&& v, const std::string&) { m.segments = v.integer; },
+       [](const MeshDesc& m) { return JsonValue(m.segments); }, nullptr,
+       [](const MeshDesc& m) { return mesh_is(m, MeshDesc::Source::Torus); }},
+      // Schema extension: the torus's minor segment count (0 keeps segments / 2).
+      {"segments_v", Kind::Integer, false, [](MeshDesc& m, Value&& v, const std::string&) { m.segments_v = v.integer; },
+       [](const MeshDesc& m) { return JsonValue(m.segments_v); }, nullptr,
+       [](const MeshDesc& m) { return mesh_is(m, MeshDesc::Source::Torus) && m.segments_v > 0; }},
+      {"path", Kind::Text, false, [](MeshDesc& m, Value&& v, const std::string&) { m.path = std::move(v.text); },
+       [](const MeshDesc& m) { return JsonValue(m.path); }, nullptr,
+       [](const MeshDesc& m) { return mesh_is(m, MeshDesc::Source::ObjFile); }},
+      {"smooth", Kind::Flag, false, [](MeshDesc& m, Value&& v, const std::string&) { m.smooth = v.flag; },
+       [](const MeshDesc& m) { return JsonValue(m.smooth); }},
+      {"scale", Kind::Vector, false, [](MeshDesc& m, Value&& v, const std::string&) { m.scale = v.vec; },
+       [](const MeshDesc& m) { return vec_json(m.scale); }},
+      {"rotate_y", Kind::Number, false, [](MeshDesc& m, Value&& v, const std::string&) { m.rotate_y = v.num; },
+       [](const MeshDesc& m) { return JsonValue(m.rotate_y); }},
+      {"translate", Kind::Vector, false, [](MeshDesc& m, Value&& v, const std::string&) { m.translate = v.vec; },
+       [](const MeshDesc& m) { return vec_json(m.translate); }},
+  };
+  static inline const Rule<MeshDesc> rules[] = {
+      check<MeshDesc>("subdivisions", "must be in [0, 7]",
+                      [](const MeshDesc& m) { return m.subdivisions >= 0 && m.subdivisions <= 7; }),
+      check<MeshDesc>("segments", "must be in [3, 2048]", [](const MeshDesc& m) { return m.segments >= 3 && m.segments <= 2048; }),
+      check<MeshDesc>("segments_v", "must be in [3, 2048]",
+                      [](const MeshDesc& m) { return m.segments_v == 0 || (m.segments_v >= 3 && m.segments_v <= 2048); }),
+      check<MeshDesc>("", "torus radii must be > 0", [](const MeshDesc& m) { return m.major_radius > 0 && m.minor_radius > 0; }),
+      check<MeshDesc>("path", "required for obj meshes",
+                      [](const MeshDesc& m) { return !(m.source == MeshDesc::Source::ObjFile && m.path.empty()); }),
+      finite<MeshDesc>("scale", [](const MeshDesc& m) { return m.scale; }),
+      finite<MeshDesc>("translate", [](const MeshDesc& m) { return m.translate; }),
+      check<MeshDesc>("scale", "components must be non-zero",
+                      [](const MeshDesc& m) { return !(std::fabs(m.scale.x * m.scale.y * m.scale.z) < 1e-12); }),
+  };
+};
+
+template <class T>
+bool named(const std::string& type) {
+  for (const char* n : Schema<T>::names)
+    if (type == n) return true;
+  return false;
+}
+
+// Reads the alternative of variant V named `type` (false if none is).
+template <class V, std::size_t I = 0>
+bool read_kind(const std::string& type, const JsonValue& j, const std::string& at, V& out) {
+  if constexpr (I == std::variant_size_v<V>) {
+    return false;
+  } else {
+    using T = std::variant_alternative_t<I, V>;
+    if (!named<T>(type)) return read_kind<V, I + 1>(type, j, at, out);
+    T rec;
+    read_fields<T>(Schema<T>::fields, j, at, rec);
+    out = std::move(rec);
+    return true;
+  }
+}
+
+template <class V>
+void write_kind(const V& v, JsonValue& j) {
+  std::visit([&](const auto& rec) {
+    using T = std::decay_t<decltype(rec)>;
+    j["type"] = Schema<T>::names[0];
+    write_fields<T>(Schema<T>::fields, rec, j);
+  }, v);
+}
+
+template <class V>
+void check_kind(const V& v, const std::string& at, std::vector<std::string>& out) {
+  std::visit([&](const auto& rec) {
+    using T = std::decay_t<decltype(rec)>;
+    apply_rules<T>(Schema<T>::rules, rec, at, out);
+  }, v);
+}
+
+// ---------------------------------------------------------------------------
+// Records with their own framing
+
+Material read_material(const JsonValue& j, const std::string& at) {
+  record(j, at);
+  const std::string where = field_path(at, "type");
+  const JsonValue* t = j.get("type");
+  if (!t) reject(where, "required");
+  const std::string type = decode(*t, Kind::Text, where).text;
+  Material m;
+  if (!read_kind(type, j, at, m)) reject(where, "unknown material type '" + type + "'");
+  return m;
+}
+
+// Objects read type, name and material before their shape's fields, and write
+// the material last.
+ObjectDesc read_object(const JsonValue& j, const std::string& at) {
+  record(j, at);
+  auto text = [&](const char* key, bool required, const std::string& fallback) {
+    const std::string where = field_path(at, key);
+    const JsonValue* v = j.get(key);
+    if (!v) {
+      if (required) reject(where, "required");
+      return fallback;
+    }
+    return decode(*v, Kind::Text, where).text;
+  };
+  ObjectDesc o;
+  const std::string type = text("type", true, "");
+  o.name = text("name", false, type);
+  o.material = text("material", true, "");
+  if (!read_kind(type, j, at, o.shape)) reject(field_path(at, "type"), "unknown object type '" + type + "'");
   return o;
 }
 
-JsonValue object_to(const ObjectDesc& o) {
+JsonValue write_object(const ObjectDesc& o) {
   JsonValue j;
-  if (const auto* s = std::get_if<SphereDesc>(&o.shape)) {
-    j["type"] = "sphere"; j["name"] = o.name; j["center"] = vjson(s->center); j["radius"] = s->radius;
-  } else if (const auto* p = std::get_if<PlaneDesc>(&o.shape)) {
-    j["type"] = "plane"; j["name"] = o.name; j["point"] = vjson(p->point); j["normal"] = vjson(p->normal);
-  } else if (const auto* t = std::get_if<TriangleDesc>(&o.shape)) {
-    j["type"] = "triangle"; j["name"] = o.name;
-    j["v0"] = vjson(t->v0); j["v1"] = vjson(t->v1); j["v2"] = vjson(t->v2);
-  } else if (const auto* q = std::get_if<QuadDesc>(&o.shape)) {
-    j["type"] = "quad"; j["name"] = o.name;
-    j["corner"] = vjson(q->corner); j["u"] = vjson(q->u); j["v"] = vjson(q->v);
-  } else if (const auto* b = std::get_if<BoxDesc>(&o.shape)) {
-    j["type"] = "box"; j["name"] = o.name;
-    j["min"] = vjson(b->min); j["max"] = vjson(b->max); j["rotate_y"] = b->rotate_y;
-  } else {
-    const auto& m = std::get<MeshDesc>(o.shape);
-    j["type"] = "mesh"; j["name"] = o.name;
-    if (m.source == MeshDesc::Source::Icosphere) {
-      j["source"] = "icosphere"; j["subdivisions"] = m.subdivisions;
-    } else if (m.source == MeshDesc::Source::Torus) {
-      j["source"] = "torus"; j["major_radius"] = m.major_radius; j["minor_radius"] = m.minor_radius;
-      j["segments"] = m.segments;
-      if (m.segments_v > 0) j["segments_v"] = m.segments_v;
-    } else {
-      j["source"] = "obj"; j["path"] = m.path;
-    }
-    j["smooth"] = m.smooth;
-    j["scale"] = vjson(m.scale);
-    j["rotate_y"] = m.rotate_y;
-    j["translate"] = vjson(m.translate);
-  }
+  std::visit([&](const auto& rec) {
+    using T = std::decay_t<decltype(rec)>;
+    j["type"] = Schema<T>::names[0];
+    j["name"] = o.name;
+    write_fields<T>(Schema<T>::fields, rec, j);
+  }, o.shape);
   j["material"] = o.material;
   return j;
 }
 
+PointLightDesc read_light(const JsonValue& j, const std::string& at, std::size_t index) {
+  record(j, at);
+  const std::string where = field_path(at, "type");
+  if (const JsonValue* t = j.get("type"); t && decode(*t, Kind::Text, where).text != "point")
+    reject(where, "only 'point' lights are supported (use emissive materials for area lights)");
+  PointLightDesc l;
+  l.name = "light" + std::to_string(index);
+  read_fields<PointLightDesc>(kLightFields, j, at, l);
+  return l;
+}
+
+// ---------------------------------------------------------------------------
+// Whole-scene validation rules
+
+const Rule<RenderSettings> kRenderRules[] = {
+    check<RenderSettings>("width", "must be in [1, 8192]", [](const RenderSettings& r) { return r.width >= 1 && r.width <= 8192; }),
+    check<RenderSettings>("height", "must be in [1, 8192]", [](const RenderSettings& r) { return r.height >= 1 && r.height <= 8192; }),
+    check<RenderSettings>("spp", "must be in [1, 1000000]", [](const RenderSettings& r) { return r.spp >= 1 && r.spp <= 1'000'000; }),
+    check<RenderSettings>("max_depth", "must be in [1, 1000]",
+                          [](const RenderSettings& r) { return r.max_depth >= 1 && r.max_depth <= 1000; }),
+    check<RenderSettings>("rr_min_depth", "must be >= 0", [](const RenderSettings& r) { return r.rr_min_depth >= 0; }),
+    check<RenderSettings>("threads", "must be in [0, 1024]", [](const RenderSettings& r) { return r.threads >= 0 && r.threads <= 1024; }),
+    check<RenderSettings>("tile_size", "must be in [1, 1024]",
+                          [](const RenderSettings& r) { return r.tile_size >= 1 && r.tile_size <= 1024; }),
+    check<RenderSettings>("exposure", "must be > 0", [](const RenderSettings& r) { return finite_positive(r.exposure); }),
+};
+
+const Rule<CameraDesc> kCameraRules[] = {
+    finite<CameraDesc>("look_from", [](const CameraDesc& c) { return c.look_from; }),
+    finite<CameraDesc>("look_at", [](const CameraDesc& c) { return c.look_at; }),
+    check<CameraDesc>("", "look_from and look_at must differ",
+                      [](const CameraDesc& c) { return !(len(c.look_at - c.look_from) < 1e-9); }),
+    check<CameraDesc>("vfov", "must be in (0, 180)", [](const CameraDesc& c) { return c.vfov_deg > 0 && c.vfov_deg < 180; }),
+    check<CameraDesc>("aperture", "must be >= 0", [](const CameraDesc& c) { return !(c.aperture < 0); }),
+    check<CameraDesc>("focus_dist", "must be >= 0", [](const CameraDesc& c) { return !(c.focus_dist < 0); }),
+};
+
+const Rule<Background> kBackgroundRules[] = {
+    colour<Background>("top", [](const Background& b) { return b.top; }),
+    colour<Background>("bottom", [](const Background& b) { return b.bottom; }),
+};
+
+const Rule<PointLightDesc> kLightRules[] = {
+    finite<PointLightDesc>("position", [](const PointLightDesc& l) { return l.position; }),
+    colour<PointLightDesc>("intensity", [](const PointLightDesc& l) { return l.intensity; }),
+};
+
+constexpr const char* kTopLevelKeys[] = {"name", "camera", "render", "background", "materials",
+                                         "objects", "lights", "$schema", "description"};
+
 }  // namespace
 
+const char* integrator_name(Integrator i) { return choice_name(kIntegrators, i); }
+const char* tone_map_name(ToneMap t) { return choice_name(kToneMaps, t); }
+
 SceneDesc scene_from_json(const JsonValue& root) {
-  SceneDesc s;
-  const Fields top(root, "");
-  static const char* const kTopKeys[] = {"name", "camera", "render", "background", "materials",
-                                         "objects", "lights", "$schema", "description"};
+  record(root, "");
   for (const auto& kv : root.map()) {
     bool known = false;
-    for (const char* k : kTopKeys) known = known || kv.first == k;
-    if (!known) throw SceneError("scene: unknown top-level key '" + kv.first + "'");
+    for (const char* k : kTopLevelKeys) known = known || kv.first == k;
+    if (!known) reject("", "unknown top-level key '" + kv.first + "'");
   }
-  s.name = top.text("name", s.name);
-
-  if (const JsonValue* cj = top.find("camera")) {
-    const Fields c(*cj, "camera");
-    s.camera.look_from = c.vec("look_from", s.camera.look_from);
-    s.camera.look_at = c.vec("look_at", s.camera.look_at);
-    s.camera.vup = c.vec("vup", s.camera.vup);
-    s.camera.vfov_deg = c.num("vfov", s.camera.vfov_deg);
-    s.camera.aperture = c.num("aperture", 0);
-    s.camera.focus_dist = c.num("focus_dist", 0);
+  SceneDesc s;
+  if (const JsonValue* v = root.get("name")) s.name = decode(*v, Kind::Text, "name").text;
+  if (const JsonValue* v = root.get("camera")) read_fields<CameraDesc>(kCameraFields, record(*v, "camera"), "camera", s.camera);
+  if (const JsonValue* v = root.get("render")) read_fields<RenderSettings>(kRenderFields, record(*v, "render"), "render", s.render);
+  if (const JsonValue* v = root.get("background"))
+    read_fields<Background>(kBackgroundFields, record(*v, "background"), "background", s.background);
+  if (const JsonValue* v = root.get("materials")) {
+    if (!v->is_map()) reject("materials", "expected an object of name -> material");
+    for (const auto& kv : v->map()) s.materials.push_back({kv.first, read_material(kv.second, "materials." + kv.first)});
   }
-
-  if (const JsonValue* rj = top.find("render")) {
-    const Fields c(*rj, "render");
-    RenderSettings& R = s.render;
-    R.width = c.integer("width", R.width);
-    R.height = c.integer("height", R.height);
-    R.spp = c.integer("spp", R.spp);
-    R.max_depth = c.integer("max_depth", R.max_depth);
-    R.rr_min_depth = c.integer("rr_min_depth", R.rr_min_depth);
-    R.light_sampling = c.flag("light_sampling", R.light_sampling);
-    R.mis = c.flag("mis", R.mis);  // schema extension (no reference counterpart)
-    // The seed goes through a 32-bit integer read, as in the reference loader.
-    R.seed = static_cast<std::uint64_t>(c.integer("seed", static_cast<int>(R.seed)));
-    R.exposure = c.num("exposure", R.exposure);
-    R.threads = c.integer("threads", R.threads);
-    R.tile_size = c.integer("tile_size", R.tile_size);
-    R.use_bvh = c.flag("use_bvh", R.use_bvh);
-    const std::string integ = c.text("integrator", integrator_name(R.integrator));
-    if (integ == "path") R.integrator = Integrator::Path;
-    else if (integ == "direct") R.integrator = Integrator::Direct;
-    else if (integ == "normals") R.integrator = Integrator::Normals;
-    else throw SceneError("render.integrator: expected path, direct or normals");
-    const std::string tm = c.text("tone_map", tone_map_name(R.tone_map));
-    if (tm == "clamp") R.tone_map = ToneMap::Clamp;
-    else if (tm == "reinhard") R.tone_map = ToneMap::Reinhard;
-    else if (tm == "aces") R.tone_map = ToneMap::Aces;
-    else throw SceneError("render.tone_map: expected clamp, reinhard or aces");
+  if (const JsonValue* v = root.get("objects")) {
+    if (!v->is_list()) reject("objects", "expected an array");
+    for (std::size_t i = 0; i < v->list().size(); ++i)
+      s.objects.push_back(read_object(v->list()[i], "objects[" + std::to_string(i) + "]"));
   }
-
-  if (const JsonValue* bj = top.find("background")) {
-    const Fields b(*bj, "background");
-    const std::string kind = b.text("type", "gradient");
-    if (kind == "gradient") s.background.kind = Background::Kind::Gradient;
-    else if (kind == "solid") s.background.kind = Background::Kind::Solid;
-    else throw SceneError("background.type: expected gradient or solid");
-    s.background.top = b.vec(kind == "solid" ? "color" : "top", s.background.top);
-    s.background.bottom = b.vec("bottom", s.background.bottom);
-    s.background.intensity = b.num("intensity", 1);
+  if (const JsonValue* v = root.get("lights")) {
+    if (!v->is_list()) reject("lights", "expected an array");
+    for (std::size_t i = 0; i < v->list().size(); ++i)
+      s.lights.push_back(read_light(v->list()[i], "lights[" + std::to_string(i) + "]", i));
   }
-
-  if (const JsonValue* mj = top.find("materials")) {
-    if (!mj->is_map()) throw SceneError("materials: expected an object of name -> material");
-    for (const auto& kv : mj->map())
-      s.materials.push_back({kv.first, material_from(Fields(kv.second, "materials." + kv.first))});
-  }
-
-  if (const JsonValue* oj = top.find("objects")) {
-    if (!oj->is_list()) throw SceneError("objects: expected an array");
-    const auto& l = oj->list();
-    for (std::size_t i = 0; i < l.size(); ++i)
-      s.objects.push_back(object_from(Fields(l[i], "objects[" + std::to_string(i) + "]")));
-  }
-
-  if (const JsonValue* lj = top.find("lights")) {
-    if (!lj->is_list()) throw SceneError("lights: expected an array");
-    const auto& l = lj->list();
-    for (std::size_t i = 0; i < l.size(); ++i) {
-      const Fields f(l[i], "lights[" + std::to_string(i) + "]");
-      if (f.text("type", "point") != "point")
-        throw SceneError(f.path("type") + ": only 'point' lights are supported (use emissive materials for area lights)");
-      s.lights.push_back({f.text("name", "light" + std::to_string(i)), f.required_vec("position"),
-                          f.vec("intensity", D3{10})});
-    }
-  }
-
   const std::vector<std::string> problems = validate_scene(s);
   if (!problems.empty()) {
     std::string msg = problems.front();
@@ -307,57 +694,23 @@ SceneDesc scene_from_json(const JsonValue& root) {
 JsonValue scene_to_json(const SceneDesc& s) {
   JsonValue j;
   j["name"] = s.name;
-  JsonValue& c = j["camera"];
-  c["look_from"] = vjson(s.camera.look_from);
-  c["look_at"] = vjson(s.camera.look_at);
-  c["vup"] = vjson(s.camera.vup);
-  c["vfov"] = s.camera.vfov_deg;
-  c["aperture"] = s.camera.aperture;
-  c["focus_dist"] = s.camera.focus_dist;
-
+  write_fields<CameraDesc>(kCameraFields, s.camera, j["camera"]);
   JsonValue& r = j["render"];
-  const RenderSettings& R = s.render;
-  r["width"] = R.width;
-  r["height"] = R.height;
-  r["spp"] = R.spp;
-  r["max_depth"] = R.max_depth;
-  r["rr_min_depth"] = R.rr_min_depth;
-  r["integrator"] = integrator_name(R.integrator);
-  r["light_sampling"] = R.light_sampling;
-  if (R.mis) r["mis"] = true;
-  r["seed"] = R.seed;
-  r["tone_map"] = tone_map_name(R.tone_map);
-  r["exposure"] = R.exposure;
-  r["threads"] = R.threads;
-  r["tile_size"] = R.tile_size;
-  r["use_bvh"] = R.use_bvh;
-
-  JsonValue& b = j["background"];
-  if (s.background.kind == Background::Kind::Solid) {
-    b["type"] = "solid";
-    b["color"] = vjson(s.background.top);
-  } else {
-    b["type"] = "gradient";
-    b["top"] = vjson(s.background.top);
-    b["bottom"] = vjson(s.background.bottom);
-  }
-  b["intensity"] = s.background.intensity;
-
+  for (const char* key : kRenderWriteOrder)
+    for (const Field<RenderSettings>& f : kRenderFields)
+      if (std::string(f.key) == key && (!f.written || f.written(s.render))) r[key] = f.get(s.render);
+  write_fields<Background>(kBackgroundFields, s.background, j["background"]);
   JsonValue mats = JsonMap{};
-  for (const auto& m : s.materials) mats[m.name] = material_to(m.material);
+  for (const auto& m : s.materials) write_kind(m.material, mats[m.name]);
   j["materials"] = std::move(mats);
-
   JsonList objs;
-  for (const auto& o : s.objects) objs.push_back(object_to(o));
+  for (const auto& o : s.objects) objs.push_back(write_object(o));
   j["objects"] = std::move(objs);
-
   JsonList lights;
   for (const auto& l : s.lights) {
     JsonValue lj;
     lj["type"] = "point";
-    lj["name"] = l.name;
-    lj["position"] = vjson(l.position);
-    lj["intensity"] = vjson(l.intensity);
+    write_fields<PointLightDesc>(kLightFields, l, lj);
     lights.push_back(std::move(lj));
   }
   j["lights"] = std::move(lights);
@@ -366,111 +719,30 @@ JsonValue scene_to_json(const SceneDesc& s) {
 
 std::vector<std::string> validate_scene(const SceneDesc& s) {
   std::vector<std::string> out;
-  auto finite = [&](D3 v, const std::string& where) {
-    if (!v.finite()) out.push_back(where + ": must be finite");
-  };
-  auto colour = [&](D3 v, const std::string& where) {
-    finite(v, where);
-    if (v.x < 0 || v.y < 0 || v.z < 0) out.push_back(where + ": colour components must be >= 0");
-  };
-  const RenderSettings& R = s.render;
-  if (R.width < 1 || R.width > 8192) out.push_back("render.width: must be in [1, 8192]");
-  if (R.height < 1 || R.height > 8192) out.push_back("render.height: must be in [1, 8192]");
-  if (R.spp < 1 || R.spp > 1'000'000) out.push_back("render.spp: must be in [1, 1000000]");
-  if (R.max_depth < 1 || R.max_depth > 1000) out.push_back("render.max_depth: must be in [1, 1000]");
-  if (R.rr_min_depth < 0) out.push_back("render.rr_min_depth: must be >= 0");
-  if (R.threads < 0 || R.threads > 1024) out.push_back("render.threads: must be in [0, 1024]");
-  if (R.tile_size < 1 || R.tile_size > 1024) out.push_back("render.tile_size: must be in [1, 1024]");
-  if (!(R.exposure > 0) || !std::isfinite(R.exposure)) out.push_back("render.exposure: must be > 0");
-
-  finite(s.camera.look_from, "camera.look_from");
-  finite(s.camera.look_at, "camera.look_at");
-  if (len(s.camera.look_at - s.camera.look_from) < 1e-9) out.push_back("camera: look_from and look_at must differ");
-  if (!(s.camera.vfov_deg > 0 && s.camera.vfov_deg < 180)) out.push_back("camera.vfov: must be in (0, 180)");
-  if (s.camera.aperture < 0) out.push_back("camera.aperture: must be >= 0");
-  if (s.camera.focus_dist < 0) out.push_back("camera.focus_dist: must be >= 0");
-  colour(s.background.top, "background.top");
-  colour(s.background.bottom, "background.bottom");
-
+  apply_rules<RenderSettings>(kRenderRules, s.render, "render", out);
+  apply_rules<CameraDesc>(kCameraRules, s.camera, "camera", out);
+  apply_rules<Background>(kBackgroundRules, s.background, "background", out);
   for (std::size_t i = 0; i < s.materials.size(); ++i) {
-    const NamedMaterial& nm = s.materials[i];
-    const std::string at = "materials." + nm.name;
-    if (nm.name.empty()) out.push_back("materials: material names must be non-empty");
+    const std::string at = "materials." + s.materials[i].name;
+    if (s.materials[i].name.empty()) out.push_back("materials: material names must be non-empty");
     for (std::size_t k = 0; k < i; ++k)
-      if (s.materials[k].name == nm.name) out.push_back(at + ": duplicate material name");
-    if (const auto* l = std::get_if<Lambertian>(&nm.material)) {
-      colour(l->albedo.a, at + ".albedo");
-      colour(l->albedo.b, at + ".albedo2");
-      if (l->albedo.checker_scale < 0) out.push_back(at + ".checker_scale: must be >= 0");
-    } else if (const auto* m = std::get_if<Metal>(&nm.material)) {
-      colour(m->albedo, at + ".albedo");
-      if (m->roughness < 0 || m->roughness > 1) out.push_back(at + ".roughness: must be in [0, 1]");
-    } else if (const auto* d = std::get_if<Dielectric>(&nm.material)) {
-      if (!(d->ior >= 1.0 && d->ior <= 4.0)) out.push_back(at + ".ior: must be in [1, 4]");
-      colour(d->tint, at + ".tint");
-    } else {
-      const auto& e = std::get<Emissive>(nm.material);
-      colour(e.color, at + ".color");
-      if (!(e.intensity >= 0) || !std::isfinite(e.intensity)) out.push_back(at + ".intensity: must be >= 0");
-    }
+      if (s.materials[k].name == s.materials[i].name) out.push_back(at + ": duplicate material name");
+    check_kind(s.materials[i].material, at, out);
   }
-
   for (std::size_t i = 0; i < s.objects.size(); ++i) {
-    const ObjectDesc& o = s.objects[i];
     const std::string at = "objects[" + std::to_string(i) + "]";
-    if (!s.find_material(o.material)) out.push_back(at + ".material: unknown material '" + o.material + "'");
-    if (const auto* sp = std::get_if<SphereDesc>(&o.shape)) {
-      finite(sp->center, at + ".center");
-      if (!(sp->radius > 0) || !std::isfinite(sp->radius)) out.push_back(at + ".radius: must be > 0");
-    } else if (const auto* pl = std::get_if<PlaneDesc>(&o.shape)) {
-      finite(pl->point, at + ".point");
-      finite(pl->normal, at + ".normal");
-      if (len(pl->normal) < 1e-9) out.push_back(at + ".normal: must be non-zero");
-    } else if (const auto* t = std::get_if<TriangleDesc>(&o.shape)) {
-      finite(t->v0, at + ".v0");
-      finite(t->v1, at + ".v1");
-      finite(t->v2, at + ".v2");
-      if (len(cross(t->v1 - t->v0, t->v2 - t->v0)) < 1e-12) out.push_back(at + ": triangle is degenerate");
-    } else if (const auto* q = std::get_if<QuadDesc>(&o.shape)) {
-      finite(q->corner, at + ".corner");
-      finite(q->u, at + ".u");
-      finite(q->v, at + ".v");
-      if (len(cross(q->u, q->v)) < 1e-12) out.push_back(at + ": quad is degenerate (u parallel to v)");
-    } else if (const auto* b = std::get_if<BoxDesc>(&o.shape)) {
-      finite(b->min, at + ".min");
-      finite(b->max, at + ".max");
-      if (!(b->max.x > b->min.x && b->max.y > b->min.y && b->max.z > b->min.z))
-        out.push_back(at + ": box max must exceed min on every axis");
-    } else {
-      const auto& m = std::get<MeshDesc>(o.shape);
-      if (m.subdivisions < 0 || m.subdivisions > 7) out.push_back(at + ".subdivisions: must be in [0, 7]");
-      if (m.segments < 3 || m.segments > 2048) out.push_back(at + ".segments: must be in [3, 2048]");
-      if (m.segments_v != 0 && (m.segments_v < 3 || m.segments_v > 2048))
-        out.push_back(at + ".segments_v: must be in [3, 2048]");
-      if (!(m.major_radius > 0) || !(m.minor_radius > 0)) out.push_back(at + ": torus radii must be > 0");
-      if (m.source == MeshDesc::Source::ObjFile && m.path.empty()) out.push_back(at + ".path: required for obj meshes");
-      finite(m.scale, at + ".scale");
-      finite(m.translate, at + ".translate");
-      if (std::fabs(m.scale.x * m.scale.y * m.scale.z) < 1e-12) out.push_back(at + ".scale: components must be non-zero");
-    }
+    if (!s.find_material(s.objects[i].material))
+      out.push_back(at + ".material: unknown material '" + s.objects[i].material + "'");
+    check_kind(s.objects[i].shape, at, out);
   }
-
-  for (std::size_t i = 0; i < s.lights.size(); ++i) {
-    finite(s.lights[i].position, "lights[" + std::to_string(i) + "].position");
-    colour(s.lights[i].intensity, "lights[" + std::to_string(i) + "].intensity");
-  }
+  for (std::size_t i = 0; i < s.lights.size(); ++i)
+    apply_rules<PointLightDesc>(kLightRules, s.lights[i], "lights[" + std::to_string(i) + "]", out);
   return out;
 }
 
 SceneDesc parse_scene(const std::string& text) {
-  JsonValue j;
   try {
-    j = JsonValue::parse(text);
-  } catch (const JsonError& e) {
-    throw SceneError(e.what());
-  }
-  try {
-    return scene_from_json(j);
+    return scene_from_json(JsonValue::parse(text));
   } catch (const JsonError& e) {
     throw SceneError(e.what());
   }
@@ -479,9 +751,9 @@ SceneDesc parse_scene(const std::string& text) {
 SceneDesc load_scene(const std::string& path) {
   std::ifstream f(path, std::ios::binary);
   if (!f) throw SceneError("cannot open scene file: " + path);
-  std::stringstream ss;
-  ss << f.rdbuf();
-  SceneDesc s = parse_scene(ss.str());
+  std::stringstream text;
+  text << f.rdbuf();
+  SceneDesc s = parse_scene(text.str());
   s.base_dir = std::filesystem::path(path).parent_path().string();
   return s;
 }
