@@ -249,20 +249,27 @@ int rtg_trace_any(rtg_context* ctx, rtg_scene_id scene, const float* rays, uint6
 
 /* No counterpart in the reference. rtg_trace_closest for callers that must not
  * allocate device memory during the call: a loop sharing the GPU with other
- * streams (freeing device memory synchronises the whole device), a host that
- * pre-reserves all device memory in its own pool, or code that issues work while
- * a stream is being captured, where allocation calls are refused. Same arguments
- * and results; at most RTG_NOALLOC_MAX_RAYS rays per call (RTG_ERR_LIMIT beyond).
- * Its rays and results pass through one static device array of about 13 MiB that
- * the library reserves on every GPU it runs on until the process exits. The first
- * call on a device sets that array up (make it before any stream capture). All
- * calls share the array, so calls whose GPU work overlaps (other streams or
- * contexts on the same device) race. t is refined in double only when the
- * scene's double-precision copy is already resident (after an rtg_trace_closest
- * call on the same scene); this entry point never uploads it itself. */
+ * streams (freeing device memory synchronises the whole device), or a host that
+ * pre-reserves all device memory in its own pool. Same arguments; at most
+ * RTG_NOALLOC_MAX_RAYS rays per call (RTG_ERR_LIMIT beyond). The call makes the
+ * context's GPU current (it stays current afterwards). Its rays and results pass
+ * through one static device array of about 13 MiB that the library reserves on
+ * every GPU it runs on until the process exits. The first call on a device sets
+ * that array up (make it before any stream capture). All calls share the array,
+ * so calls whose GPU work overlaps (other streams or contexts on the same
+ * device) race. Ids and planes are those of rtg_trace_closest. t is refined in
+ * double only when the scene's double-precision copy is already resident (after
+ * an rtg_trace_closest call on the same scene with refine_hits on); otherwise it
+ * is the fp32 traversal's own t, as with refine_hits = 0, since this entry point
+ * never uploads that copy itself. */
 #define RTG_NOALLOC_MAX_RAYS 262144
 int rtg_trace_closest_noalloc(rtg_context* ctx, rtg_scene_id scene, const float* rays, uint64_t n, int32_t brute,
                               float* t, int32_t* prim, int32_t* is_plane, float* bary);
+
+/* No counterpart in the reference. How many memory allocations (device, pooled
+ * and pinned host) the library has asked CUDA for in this process so far: a
+ * diagnostic for callers that must not allocate, to check an entry point. */
+uint64_t rtg_allocation_count(void);
 
 /* ---- engine tuning (no reference counterpart) ---- */
 typedef struct rtg_tuning {
@@ -276,6 +283,10 @@ typedef struct rtg_tuning {
   uint32_t chained;          /* programmatic dependent launch between wavefront kernels (default 1) */
   uint64_t serve_budget_bytes; /* admission limit of the open requests' device footprint */
   uint64_t serve_reserve_bytes; /* part of that budget only priority-0 requests (previews) may use */
+  int32_t refine_hits;       /* ray queries report t recomputed in double for the winning primitive
+                              * (default 1); 0: the fp32 traversal's own t, the value the renderer's
+                              * closest-hit stage hands to shading */
+  int32_t reserved;
 } rtg_tuning;
 int rtg_get_tuning(rtg_context* ctx, rtg_tuning* out);
 int rtg_set_tuning(rtg_context* ctx, const rtg_tuning* in);

@@ -18,6 +18,7 @@
 #include <string>
 
 #include "device/noalloc.h"
+#include "host/alloc_count.hpp"
 #include "host/autotune.hpp"
 #include "host/engine.hpp"
 #include "host/scene_io.hpp"
@@ -664,6 +665,8 @@ int rtg_trace_closest_noalloc(rtg_context* ctx, rtg_scene_id scene, const float*
   });
 }
 
+uint64_t rtg_allocation_count(void) { return rtg::allocation_count(); }
+
 int rtg_get_tuning(rtg_context* ctx, rtg_tuning* out) {
   return guarded(ctx, [&]() {
     if (!out) throw std::invalid_argument("null argument");
@@ -681,6 +684,7 @@ int rtg_get_tuning(rtg_context* ctx, rtg_tuning* out) {
     out->chained = c.shape.chained ? 1 : 0;
     out->serve_budget_bytes = ctx->serve_budget;
     out->serve_reserve_bytes = ctx->serve_reserve;
+    out->refine_hits = c.refine_hits ? 1 : 0;
     return RTG_OK;
   });
 }
@@ -709,6 +713,7 @@ int rtg_set_tuning(rtg_context* ctx, const rtg_tuning* in) {
     c.count_traversal = in->count_traversal != 0;
     c.backlog_pools = in->backlog_pools;
     c.shape.chained = in->chained != 0;
+    c.refine_hits = in->refine_hits != 0;
     if (in->serve_budget_bytes) ctx->serve_budget = in->serve_budget_bytes;
     if (in->serve_reserve_bytes > ctx->serve_budget) throw std::invalid_argument("serve_reserve_bytes exceeds the budget");
     ctx->serve_reserve = in->serve_reserve_bytes;

@@ -8,6 +8,7 @@
 // split is cheaper), depth cap 60, the middle split when every centroid
 // coincides or a partition leaves one side empty, and std::partition.
 #include "device/bvh_gpu.h"
+#include "host/alloc_count.hpp"
 
 #include <algorithm>
 #include <stdexcept>
@@ -1306,6 +1307,7 @@ void* GpuBvhBuilder::alloc(std::size_t bytes) {
   if (n_blocks_ >= static_cast<int>(sizeof(blocks_) / sizeof(blocks_[0])))
     throw std::logic_error("bvh build: too many scratch blocks");
   void* p = nullptr;
+  count_allocation();
   BVH_CK(cudaMallocFromPoolAsync(&p, std::max<std::size_t>(bytes, 256), pool_, stream_));
   blocks_[n_blocks_++] = p;
   return p;

@@ -3,21 +3,28 @@
 // rtg_trace_closest stages its rays, its results and the scene descriptor in
 // buffers it cudaMallocs and cudaFrees on every call. Some callers cannot do
 // that: a render loop sharing the GPU with other streams (cudaFree synchronises
-// the whole device), a host that reserves all device memory up front in its own
-// pool and forbids further allocations, or code issuing work while a stream is
-// being captured, where allocation calls are refused. This variant keeps every
-// byte it needs in one file-scope device array, sized for kNoAllocMaxRays rays,
-// that the CUDA module reserves on each GPU where it is loaded (with lazy module
-// loading: at this file's first use on that GPU) and that stays until the process
-// exits.
+// the whole device), or a host that reserves all device memory up front in its
+// own pool and forbids further allocations. This variant keeps every byte it
+// needs in one file-scope device array, sized for kNoAllocMaxRays rays, that the
+// CUDA module reserves on each GPU where it is loaded (with lazy module loading:
+// at this file's first use on that GPU) and that stays until the process exits.
+// It makes no allocation and no free during a call; it does copy from pageable
+// host memory and waits for the context's stream before returning.
 //
-// Set-up: the first call on a device (with that device current) looks up the
-// array's device address with cudaGetSymbolAddress, once per device; make that
-// first call before starting any stream capture. Every call, on every context,
-// shares the one array and leaves its contents behind: a call copies its rays in
-// and writes every result slot it reads back, so nothing has to start at zero,
-// but two calls whose work overlaps on the GPU (different streams or contexts
-// on the same device) race on the array and corrupt each other's results.
+// Set-up: every call first makes its context's device current (cudaSetDevice;
+// the device stays current after the call returns). The first call on a device
+// then looks up the array's device address there with cudaGetSymbolAddress and
+// caches it for that device; make that first call before starting any stream
+// capture. Every call, on every context, shares the one array and leaves its
+// contents behind: a call copies its rays in and writes every result slot it
+// reads back, so nothing has to start at zero, but two calls whose work overlaps
+// on the GPU (different streams or contexts on the same device) race on the
+// array and corrupt each other's results.
+//
+// The reported distance is the fp32 traversal's own unless the scene's
+// double-precision copy is already resident (uploaded by an earlier
+// rtg_trace_closest call with distance refinement on); this call never uploads
+// that copy itself, since that would allocate.
 #include <mutex>
 
 #include "device/noalloc.h"
@@ -43,11 +50,16 @@ constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
 unsigned char* g_scratch_addr[kMaxDevices] = {};
 
-// Device address of g_scratch on `device` (which must be current).
+// Device address of g_scratch on `device`. The symbol lookup answers for the
+// current device, so the cache entry is only written when `device` is current.
 cudaError_t scratch_address(int device, unsigned char** out) {
   if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
   std::lock_guard<std::mutex> lock(g_setup_mutex);
   if (!g_scratch_addr[device]) {
+    int current = -1;
+    const cudaError_t ge = cudaGetDevice(&current);
+    if (ge != cudaSuccess) return ge;
+    if (current != device) return cudaErrorInvalidDevice;
     void* p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
     if (e != cudaSuccess) return e;
@@ -89,8 +101,12 @@ cudaError_t noalloc_trace_closest(int device, const RtgSceneDev& job, const floa
                                   cudaStream_t stream) {
   if (n > kNoAllocMaxRays) return cudaErrorInvalidValue;
   if (n == 0) return cudaSuccess;
+  // The scratch address, the kernel launch and the copies all belong to the
+  // context's device: make it current first (it stays current after the call).
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) return e;
   unsigned char* s = nullptr;
-  cudaError_t e = scratch_address(device, &s);
+  e = scratch_address(device, &s);
   if (e != cudaSuccess) return e;
   if ((e = cudaMemcpyAsync(s, &job, sizeof(job), cudaMemcpyHostToDevice, stream)) != cudaSuccess) return e;
   if ((e = cudaMemcpyAsync(s + kRaysOff, rays, n * 32, cudaMemcpyHostToDevice, stream)) != cudaSuccess) return e;

@@ -1,5 +1,7 @@
 #include "host/engine.hpp"
 
+#include "host/alloc_count.hpp"
+
 #include "device/bvh_gpu.h"
 
 #include <cuda_runtime.h>
@@ -17,6 +19,13 @@
 namespace rtg {
 
 namespace {
+std::atomic<std::uint64_t> g_allocations{0};
+}  // namespace
+
+void count_allocation() { g_allocations.fetch_add(1, std::memory_order_relaxed); }
+std::uint64_t allocation_count() { return g_allocations.load(std::memory_order_relaxed); }
+
+namespace {
 
 void check(cudaError_t e, const char* what) {
   if (e != cudaSuccess) throw CudaFailure(std::string(what) + ": " + cudaGetErrorString(e));
@@ -26,6 +35,7 @@ void check(cudaError_t e, const char* what) {
 template <class T>
 T* dev_alloc(std::size_t n) {
   void* p = nullptr;
+  count_allocation();
   CK(cudaMalloc(&p, std::max<std::size_t>(n, 1) * sizeof(T)));
   return static_cast<T*>(p);
 }
@@ -35,6 +45,7 @@ T* dev_alloc(std::size_t n) {
 template <class T>
 T* dev_alloc_async(std::size_t n, cudaMemPool_t pool, cudaStream_t s) {
   void* p = nullptr;
+  count_allocation();
   CK(cudaMallocFromPoolAsync(&p, std::max<std::size_t>(n, 1) * sizeof(T), pool, s));
   return static_cast<T*>(p);
 }
@@ -320,6 +331,7 @@ int Engine::register_flat(std::shared_ptr<const CompiledScene> scene, FlatScene 
   gs->n_interior = static_cast<std::int32_t>(flat.nodes.size());
   gs->n_wide = static_cast<std::int32_t>(flat.nodes4.size());
   void* block = nullptr;
+  count_allocation();
   CK(cudaMallocFromPoolAsync(&block, p.total, pool_, stream_));
   CK(cudaMemcpyAsync(block, staged, p.total, cudaMemcpyHostToDevice, stream_));
   auto at = [&](int k) { return static_cast<void*>(static_cast<unsigned char*>(block) + p.at[k]); };
@@ -354,6 +366,7 @@ unsigned char* Engine::upload_staging(std::size_t bytes, int& b, int want) {
     if (upload_host_[b]) CK(cudaFreeHost(upload_host_[b]));
     upload_host_[b] = nullptr;
     upload_cap_[b] = 0;
+    count_allocation();
     CK(cudaMallocHost(reinterpret_cast<void**>(&upload_host_[b]), bytes));
     upload_cap_[b] = bytes;
   }
@@ -419,6 +432,7 @@ int Engine::add_scene_gpu_bvh(std::shared_ptr<const CompiledScene> scene) {
 
   // Device copy of the inputs plus room for the slot -> primitive map.
   void* in_block = nullptr;
+  count_allocation();
   CK(cudaMallocFromPoolAsync(&in_block, staged + pad(np * sizeof(std::uint32_t)), pool_, build_stream_));
   struct FreeInput {
     void* p;
@@ -451,6 +465,7 @@ int Engine::add_scene_gpu_bvh(std::shared_ptr<const CompiledScene> scene) {
     total += pad(part_bytes[k]);
   }
   void* block = nullptr;
+  count_allocation();
   CK(cudaMallocFromPoolAsync(&block, total, pool_, build_stream_));
   // Freed again if anything below throws; handed to the scene at the end.
   struct FreeBlock {
@@ -548,9 +563,11 @@ void Engine::ensure_wave() {
   CK(cudaMemset(W.prog_dev, 0, sizeof(SegmentProgress) * kMaxSegments));
   CK(cudaMemset(W.gen_dev, 0, sizeof(GenTable)));
   CK(cudaMemset(W.plan_dev, 0, sizeof(GenPlan)));
+  count_allocation();
   CK(cudaHostAlloc(reinterpret_cast<void**>(&W.ring), sizeof(WaveSnapshot) * kRing, cudaHostAllocMapped));
   WaveSnapshot* ring_dev = nullptr;
   CK(cudaHostGetDevicePointer(reinterpret_cast<void**>(&ring_dev), W.ring, 0));
+  count_allocation();
   CK(cudaMallocHost(reinterpret_cast<void**>(&W.staging), kStageBytes * kRing));
   for (auto& e : W.plan_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   for (auto& e : W.tev) CK(cudaEventCreate(&e));
@@ -1171,6 +1188,7 @@ void Engine::reserve_pool(std::size_t bytes) {
   }
   if (bytes <= pool_reserved_) return;
   void* p = nullptr;
+  count_allocation();
   CK(cudaMallocFromPoolAsync(&p, bytes, pool_, stream_));
   CK(cudaFreeAsync(p, stream_));
   CK(cudaStreamSynchronize(stream_));
@@ -1247,7 +1265,7 @@ void Engine::trace_closest(int scene_id, const float* rays, std::uint64_t n, boo
   GpuScene& sc = scene(scene_id);
   if (n == 0) return;
   if (n > 0xFFFFFFFFull) throw std::invalid_argument("too many rays in one call");
-  if (!sc.prims64) {
+  if (!sc.prims64 && cfg_.refine_hits) {
     // Double originals in slot order, for the reported distance only.
     std::vector<double> g(std::max<std::size_t>(1, sc.slot_prim.size()) * 9, 0.0);
     for (std::size_t k = 0; k < sc.slot_prim.size(); ++k) {
@@ -1272,7 +1290,8 @@ void Engine::trace_closest(int scene_id, const float* rays, std::uint64_t n, boo
   }
   RenderSettings s = sc.host->settings;
   s.use_bvh = !brute;
-  const RtgSceneDev d = job_descriptor(sc, s, GpuFrame{});
+  RtgSceneDev d = job_descriptor(sc, s, GpuFrame{});
+  if (!cfg_.refine_hits) d.prims64 = d.planes64 = nullptr;
   RtgSceneDev* dd = dev_alloc<RtgSceneDev>(1);
   float4* in = dev_alloc<float4>(2 * n);
   float4* out = dev_alloc<float4>(n);
@@ -1331,7 +1350,9 @@ RtgSceneDev Engine::query_descriptor(int scene_id, bool brute) {
   GpuScene& sc = scene(scene_id);
   RenderSettings s = sc.host->settings;
   s.use_bvh = !brute;
-  return job_descriptor(sc, s, GpuFrame{});
+  RtgSceneDev d = job_descriptor(sc, s, GpuFrame{});
+  if (!cfg_.refine_hits) d.prims64 = d.planes64 = nullptr;
+  return d;
 }
 
 }  // namespace rtg

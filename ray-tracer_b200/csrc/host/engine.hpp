@@ -108,6 +108,10 @@ struct EngineConfig {
   LaunchShape shape;
   bool time_kernels = false;                    // CUDA events around every launch
   bool count_traversal = false;                 // node / primitive counters
+  // Ray queries (trace_closest and the no-alloc variant) report the winning
+  // primitive's distance recomputed in double; off: the fp32 traversal's own t,
+  // exactly what the wavefront's closest-hit stage hands to shading.
+  bool refine_hits = true;
 };
 
 // A render request for the scheduler.

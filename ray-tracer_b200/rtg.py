@@ -104,6 +104,7 @@ class _Tuning(C.Structure):
         ("extend_blocks", C.c_int32), ("shade_blocks", C.c_int32), ("shadow_blocks", C.c_int32),
         ("time_kernels", C.c_int32), ("count_traversal", C.c_int32), ("backlog_pools", C.c_uint32),
         ("chained", C.c_uint32), ("serve_budget_bytes", C.c_uint64), ("serve_reserve_bytes", C.c_uint64),
+        ("refine_hits", C.c_int32), ("reserved", C.c_int32),
     ]
 
 
@@ -152,6 +153,7 @@ _SIGNATURES = {
     "rtg_trace_closest_noalloc": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_float), C.c_uint64, C.c_int32,
                                             C.POINTER(C.c_float), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                             C.POINTER(C.c_float)]),
+    "rtg_allocation_count": (C.c_uint64, []),
     "rtg_get_tuning": (C.c_int, [C.c_void_p, C.POINTER(_Tuning)]),
     "rtg_set_tuning": (C.c_int, [C.c_void_p, C.POINTER(_Tuning)]),
     "rtg_request_submit": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(_Settings), C.POINTER(_Options), C.c_int32,
@@ -360,6 +362,12 @@ def load_scene(path: str) -> HostScene:
 
 def device_count() -> int:
     return lib().rtg_device_count()
+
+
+def allocation_count() -> int:
+    """Memory allocations (device, pooled, pinned host) the library has asked
+    CUDA for in this process so far."""
+    return int(lib().rtg_allocation_count())
 
 
 class Context:

@@ -22,7 +22,7 @@ import rtg  # noqa: E402  (host-side parse and dump only)
 
 OUT = os.path.dirname(os.path.abspath(__file__))
 HARNESS = os.path.join(ROOT, "oracle", "_ref", "rt_harness")
-ASSETS = "/root/reference/assets/scenes"
+ASSETS = os.path.join(os.environ.get("REF_DIR", "/root/reference"), "assets", "scenes")
 W, H = 64, 36
 REF_SPP, CPU_SPP, REF_SEED = 8192, 64, 9001
 

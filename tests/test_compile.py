@@ -102,7 +102,7 @@ def test_procedural_meshes_are_closed_and_outward():
 def test_reference_assets_round_trip_when_present():
     """Every shipped scene parses, validates, compiles and round-trips (reads the
     reference checkout only where it exists)."""
-    d = "/root/reference/assets/scenes"
+    d = os.path.join(os.environ.get("REF_DIR", "/root/reference"), "assets", "scenes")
     if not os.path.isdir(d):
         pytest.skip("reference checkout not present")
     count = 0

@@ -10,11 +10,46 @@ import rtg
 import rtoracle
 import workloads
 from conftest import GOLDEN
-from parity import hit_parity
+from parity import hit_parity, t_share
 
 pytestmark = pytest.mark.gpu
 
 CONFIGS = {"cornell": workloads.cornell, "spheres": workloads.sphere_field, "mesh": workloads.mesh_stress}
+
+
+# Distance modes of the ray-query API: "refined" recomputes the winning
+# primitive's t in double; "fp32" reports the traversal's own t, the value the
+# renderer's closest-hit stage hands to shading.
+MODES = ["refined", "fp32"]
+# Share of hits whose fp32 t is within 1e-5 of the reference's double t. With
+# world coordinates stored in fp32, a hit at distance t from an origin at |o|
+# carries an error of about 2^-24 |o| / t, so short hits far from the world
+# origin miss 1e-5: the random-origin sets of the 555-unit Cornell room and the
+# sphere field keep about 99.8%. The mesh scene's 1M-ray set meets 99.99%.
+FP32_T_SHARE = {"cornell": 0.997, "spheres": 0.997, "mesh": 0.9999}
+
+
+@pytest.fixture
+def mode(ctx, request):
+    ctx.set_tuning(refine_hits=1 if request.param == "refined" else 0)
+    yield request.param
+    ctx.set_tuning(refine_hits=1)
+
+
+def check_parity(mode, cfg, t, prim, plane, r_t, r_prim, r_plane, bar=0.9999):
+    """Refined: ids identical (or an exact tie) and t within 1e-5 on >= bar.
+    fp32: ids as before, with ties judged at 1e-4; t within 1e-5 on the share
+    FP32_T_SHARE[cfg] of hits."""
+    if mode == "refined":
+        p = hit_parity(t, prim, plane, r_t, r_prim, r_plane)
+        assert p["accepted"] >= bar, p
+        return p
+    p = hit_parity(t, prim, plane, r_t, r_prim, r_plane, t_rel=1e-4)
+    share = t_share(t, prim, r_t, r_prim)
+    print(cfg, "fp32 t within 1e-5:", share, {k: v for k, v in p.items() if k != "fail_idx"})
+    assert p["accepted"] >= bar, p
+    assert share >= FP32_T_SHARE[cfg], share
+    return p
 
 
 @pytest.fixture(scope="module")
@@ -26,52 +61,53 @@ def scenes(ctx):
     return out
 
 
+@pytest.mark.parametrize("mode", MODES, indirect=True)
 @pytest.mark.parametrize("cfg", list(CONFIGS))
-def test_closest_hit_matches_reference_fixture(ctx, scenes, cfg):
+def test_closest_hit_matches_reference_fixture(ctx, scenes, cfg, mode):
     g = np.load(os.path.join(GOLDEN, f"rays_{cfg}.npz"))
     _, _, sid = scenes[cfg]
     t, prim, plane, _ = ctx.trace_closest(sid, g["rays"])
     ref_t = np.where(g["hit"] == 1, g["t"], 0.0)
-    p = hit_parity(t, prim, plane, ref_t, g["prim"], g["is_plane"])
+    p = check_parity(mode, cfg, t, prim, plane, ref_t, g["prim"], g["is_plane"])
     assert p["hit_rate"] > 0.1
-    assert p["accepted"] >= 0.999, p
     # Brute-force kernel against the reference's intersect_brute.
     tb, pb, plb, _ = ctx.trace_closest(sid, g["rays"], brute=True)
-    pbr = hit_parity(tb, pb, plb, np.where(g["brute_hit"] == 1, g["brute_t"], 0.0), g["brute_prim"], g["brute_plane"])
-    assert pbr["accepted"] >= 0.999, pbr
+    check_parity(mode, cfg, tb, pb, plb, np.where(g["brute_hit"] == 1, g["brute_t"], 0.0), g["brute_prim"],
+                 g["brute_plane"])
 
 
+@pytest.mark.parametrize("mode", MODES, indirect=True)
 @pytest.mark.parametrize("cfg", ["cornell", "spheres"])
-def test_closest_hit_200k_rays_vs_oracle(ctx, scenes, cfg):
+def test_closest_hit_200k_rays_vs_oracle(ctx, scenes, cfg, mode):
     _, view, sid = scenes[cfg]
     rays = workloads.random_rays(view, 200_000, seed=202)
     t, prim, plane, _ = ctx.trace_closest(sid, rays)
     ot, op, opl, _ = rtoracle.OracleScene(view).closest_parallel(rays.astype(np.float64))
-    p = hit_parity(t, prim, plane, ot, op, opl)
-    print(cfg, {k: v for k, v in p.items() if k != "fail_idx"})
-    assert p["accepted"] >= 0.9999, p
+    p = check_parity(mode, cfg, t, prim, plane, ot, op, opl)
+    print(cfg, mode, {k: v for k, v in p.items() if k != "fail_idx"})
 
 
-def test_mesh_1m_rays_vs_oracle_and_brute_force(ctx, scenes):
+@pytest.mark.parametrize("mode", MODES, indirect=True)
+def test_mesh_1m_rays_vs_oracle_and_brute_force(ctx, scenes, mode):
     """Config 3's fixed set: 1M seeded fp32 rays against the 174k-triangle scene.
     GPU BVH vs CPU BVH (oracle, all 1M), GPU BVH vs GPU brute force (all 1M),
-    GPU vs CPU brute force (10k subset)."""
+    GPU vs CPU brute force (10k subset). In fp32 mode the distances are the
+    traversal's own and must meet 1e-5 on 99.99% of hits."""
     _, view, sid = scenes["mesh"]
     rays = workloads.random_rays(view, 1_000_000, seed=1)
     t, prim, plane, _ = ctx.trace_closest(sid, rays)
     oracle = rtoracle.OracleScene(view)
     ot, op, opl, _ = oracle.closest_parallel(rays.astype(np.float64))
-    p = hit_parity(t, prim, plane, ot, op, opl)
-    print("mesh 1M vs oracle BVH", {k: v for k, v in p.items() if k != "fail_idx"})
-    assert p["accepted"] >= 0.9999 and p["strict"] >= 0.999, p
+    p = check_parity(mode, "mesh", t, prim, plane, ot, op, opl)
+    print("mesh 1M vs oracle BVH", mode, {k: v for k, v in p.items() if k != "fail_idx"})
+    assert p["strict"] >= 0.999, p
     tb, pb, plb, _ = ctx.trace_closest(sid, rays, brute=True)
     pg = hit_parity(t, prim, plane, tb, pb, plb)
     print("mesh 1M GPU BVH vs GPU brute", {k: v for k, v in pg.items() if k != "fail_idx"})
     assert pg["accepted"] >= 0.9999, pg
     sub = rays[:10_000].astype(np.float64)
     ct, cp, cpl, _ = oracle.closest_parallel(sub, brute=True)
-    ps = hit_parity(t[:10_000], prim[:10_000], plane[:10_000], ct, cp, cpl)
-    assert ps["accepted"] >= 0.999, ps
+    check_parity(mode, "mesh", t[:10_000], prim[:10_000], plane[:10_000], ct, cp, cpl)
 
 
 @pytest.mark.parametrize("cfg", list(CONFIGS))
