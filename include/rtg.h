@@ -271,6 +271,17 @@ int rtg_trace_closest_noalloc(rtg_context* ctx, rtg_scene_id scene, const float*
  * diagnostic for callers that must not allocate, to check an entry point. */
 uint64_t rtg_allocation_count(void);
 
+/* No counterpart in the reference. Measures read bandwidth on the context's GPU:
+ * a zero-filled buffer of `bytes` (allocated for the call) is read `reps` times
+ * per launch with 16-byte loads by a grid that fills every SM; *gbs receives the
+ * best of five launches in GB/s. l1 = 0: loads bypass L1 and the grid shares the
+ * buffer (>= 1 MiB); well under the L2 size (126 MB on B200) that is the L2 read
+ * bandwidth, far above it the HBM read bandwidth. l1 = 1: L1-cached loads, every
+ * block reads the whole buffer (4 KiB to 128 KiB), so it is the aggregate L1 read
+ * bandwidth. BVH traversal's node and primitive fetches are served from L1 and
+ * L2, so these bound it, not HBM. */
+int rtg_probe_read_bandwidth(rtg_context* ctx, uint64_t bytes, int32_t reps, int32_t l1, double* gbs);
+
 /* ---- engine tuning (no reference counterpart) ---- */
 typedef struct rtg_tuning {
   uint32_t pool_paths;       /* wavefront path slots (default 1 << 20) */

@@ -18,6 +18,7 @@
 #include <string>
 
 #include "device/noalloc.h"
+#include "device/probe.h"
 #include "host/alloc_count.hpp"
 #include "host/autotune.hpp"
 #include "host/engine.hpp"
@@ -666,6 +667,20 @@ int rtg_trace_closest_noalloc(rtg_context* ctx, rtg_scene_id scene, const float*
 }
 
 uint64_t rtg_allocation_count(void) { return rtg::allocation_count(); }
+
+int rtg_probe_read_bandwidth(rtg_context* ctx, uint64_t bytes, int32_t reps, int32_t l1, double* gbs) {
+  return guarded(ctx, [&]() {
+    if (!gbs) throw std::invalid_argument("null argument");
+    if (reps < 1) throw std::invalid_argument("reps must be >= 1");
+    if (l1 && (bytes < 4096 || bytes > (128u << 10))) throw std::invalid_argument("l1: bytes must be in [4 KiB, 128 KiB]");
+    if (!l1 && bytes < (1u << 20)) throw std::invalid_argument("bytes must be >= 1 MiB");
+    if (ctx->busy) return RTG_ERR_BUSY;
+    cudaError_t e = cudaSetDevice(ctx->engine->device());
+    if (e == cudaSuccess) e = rtg::probe_read_bandwidth(bytes, reps, l1 != 0, ctx->engine->stream(), gbs);
+    if (e != cudaSuccess) throw rtg::CudaFailure(std::string("rtg_probe_read_bandwidth: ") + cudaGetErrorString(e));
+    return RTG_OK;
+  });
+}
 
 int rtg_get_tuning(rtg_context* ctx, rtg_tuning* out) {
   return guarded(ctx, [&]() {

@@ -154,6 +154,7 @@ _SIGNATURES = {
                                             C.POINTER(C.c_float), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                             C.POINTER(C.c_float)]),
     "rtg_allocation_count": (C.c_uint64, []),
+    "rtg_probe_read_bandwidth": (C.c_int, [C.c_void_p, C.c_uint64, C.c_int32, C.c_int32, C.POINTER(C.c_double)]),
     "rtg_get_tuning": (C.c_int, [C.c_void_p, C.POINTER(_Tuning)]),
     "rtg_set_tuning": (C.c_int, [C.c_void_p, C.POINTER(_Tuning)]),
     "rtg_request_submit": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(_Settings), C.POINTER(_Options), C.c_int32,
@@ -531,6 +532,14 @@ class Context:
                                             _ptr(t, C.c_float), _ptr(prim, C.c_int32), _ptr(plane, C.c_int32),
                                             _ptr(bary, C.c_float)))
         return t, prim, plane, bary
+
+    def probe_read_bandwidth(self, nbytes: int, reps: int = 8, l1: bool = False) -> float:
+        """Read bandwidth (GB/s) over a buffer of nbytes on this context's GPU:
+        L2 when nbytes is well under the L2 size, HBM when far above it; with l1,
+        every block reads its own copy of a small buffer (aggregate L1)."""
+        g = C.c_double()
+        self._check(lib().rtg_probe_read_bandwidth(self._h, int(nbytes), int(reps), int(bool(l1)), C.byref(g)))
+        return g.value
 
     def trace_closest_noalloc(self, scene_id: int, rays: np.ndarray, brute: bool = False):
         """trace_closest through the entry point that allocates no device memory
