@@ -115,7 +115,8 @@ def test_matches_oracle_statistics_on_the_same_samples(ctx):
     assert abs(stats["rays"] - cst["rays"]) <= 0.02 * cst["rays"]
 
 
-@pytest.mark.parametrize("make,depth", [(workloads.cornell, 8), (workloads.sphere_field, 16)])
+@pytest.mark.parametrize("make,depth", [(workloads.cornell, 8), (workloads.sphere_field, 16),
+                                        (workloads.mesh_stress, 12)])
 def test_samples_match_the_oracle_one_by_one(ctx, make, depth):
     """Same RNG streams, same draws: the GPU's fp32 radiance of each sample equals
     the oracle's double radiance (the reference's path_trace restated), sample by
@@ -224,6 +225,33 @@ def test_cancellation_stops_quickly_and_leaves_a_consistent_buffer(ctx):
     assert prog2.finished and not prog2.cancelled
 
 
+@pytest.mark.parametrize("integ", ["direct", "normals"])
+@pytest.mark.parametrize("make", [workloads.cornell, workloads.mesh_stress])
+def test_direct_and_normals_samples_match_the_oracle_one_by_one(ctx, make, integ):
+    """The direct (Whitted) and normals integrators sample by sample against the
+    oracle's restatement of the reference (src/rendering/integrator.cpp:141-198),
+    with the same RNG streams: at 1 spp each pixel holds one sample. The mesh
+    scene has a point light and an emissive sphere (cone sampling), rough metal
+    (recursion with a fuzz draw) and glass (the deterministic Fresnel split).
+    Normals must agree to 1e-4 except where a primary ray meets two surfaces at
+    the same distance (a box edge), which decides by rounding."""
+    scene = make(width=32, height=32, spp=1)
+    scene["render"]["integrator"] = integ
+    _, s, _, n, stats = render(ctx, scene, rtg.RenderOptions(progressive=False))
+    o = rtoracle.OracleScene(rtg.parse_scene(json.dumps(scene)).view())
+    cs, _, _ = o.render()
+    if integ == "normals":
+        close = np.abs(s - cs).max(-1) <= 1e-4
+        bar = 0.998
+    else:
+        err = np.abs(s - cs).max(axis=-1) / np.maximum(1.0, np.abs(cs).max(axis=-1))
+        close = err <= 1e-3
+        bar = 0.99
+    print(make.__name__, integ, "samples that agree:", int(close.sum()), "of", close.size)
+    assert close.mean() >= bar
+    assert stats["invalid_samples"] == 0
+
+
 def test_normals_and_direct_integrators_match_oracle(ctx):
     for integ in ("normals", "direct"):
         scene = workloads.cornell(width=32, height=32, spp=4)
@@ -280,3 +308,39 @@ def test_batch_upload_renders_like_single_uploads(ctx):
         assert ra.tobytes() == rb.tobytes()
     for i in single + many:
         ctx.release(i)
+
+
+def _invalid_scene(kind: str, intensity: float) -> dict:
+    """Every camera path ends on an emitter whose fp32 emission overflows to inf
+    (intensity 1e38 times colour 10): seen directly ("inf") or through a red
+    mirror ("nan": inf times the zero green and blue throughput)."""
+    scene = {"camera": {"look_from": [0, 0, 0], "look_at": [0, 0, -1], "vfov": 30},
+             "render": {"width": 16, "height": 12, "spp": 3, "max_depth": 4},
+             "background": {"type": "solid", "color": [0, 0, 0]},
+             "materials": {"hot": {"type": "emissive", "color": 10, "intensity": intensity, "two_sided": True},
+                           "red_mirror": {"type": "metal", "albedo": [1, 0, 0], "roughness": 0}},
+             "objects": [{"type": "sphere", "center": [0, 0, 0], "radius": 50, "material": "hot"}]}
+    if kind == "nan":
+        scene["objects"].append({"type": "quad", "corner": [-20, -20, -2], "u": [40, 0, 0], "v": [0, 40, 0],
+                                 "material": "red_mirror"})
+    return scene
+
+
+@pytest.mark.parametrize("integ", ["path", "direct"])
+@pytest.mark.parametrize("kind", ["inf", "nan"])
+def test_invalid_samples_are_counted_and_recorded_black(ctx, kind, integ):
+    """The reference's invalid-sample rule (src/rendering/renderer.cpp:39-44): a
+    non-finite or negative sample is counted in invalid_samples and added as
+    black, so the pixel keeps its sample count and stays finite. Here every
+    sample is non-finite on the GPU, through the path and the direct integrator."""
+    scene = _invalid_scene(kind, 1e38)
+    scene["render"]["integrator"] = integ
+    prog, s, q, n, stats = render(ctx, scene)
+    w, h, spp = 16, 12, 3
+    assert prog.finished
+    assert stats["invalid_samples"] == w * h * spp
+    assert (n == spp).all() and np.isfinite(s).all() and np.isfinite(q).all()
+    assert (s == 0).all()
+    # The same scene with a finite emission: no invalid sample, every pixel lit.
+    prog, s, q, n, stats = render(ctx, _invalid_scene(kind, 1e30))
+    assert stats["invalid_samples"] == 0 and np.isfinite(s).all() and (s[..., 0] > 0).all()
