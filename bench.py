@@ -82,6 +82,10 @@ def args(argv=None):
     p.add_argument("--no-autotune", action="store_true", help="keep the default pool and block size")
     p.add_argument("--pool", type=int, default=0, help="path slots (implies --no-autotune)")
     p.add_argument("--block", type=int, default=0, help="threads per block: 64, 128, 256 (implies --no-autotune)")
+    p.add_argument("--closest-tree", type=int, choices=[2, 8], default=0,
+                   help="closest-hit walk: 8 compressed eight-wide tree, 2 binary tree (default: the library's)")
+    p.add_argument("--shadow-tree", type=int, choices=[4, 8], default=0,
+                   help="any-hit walk: 4 four-wide tree, 8 compressed eight-wide tree (default: the library's)")
     return p.parse_args(argv)
 
 
@@ -569,6 +573,9 @@ def run_rtg(a, dist, scenes, desc):
 
     dev = dist.local
     ctx = rtg.Context(dev)
+    if a.closest_tree or a.shadow_tree:
+        ctx.set_tuning(**({"closest_tree": a.closest_tree} if a.closest_tree else {}),
+                       **({"shadow_tree": a.shadow_tree} if a.shadow_tree else {}))
     peaks = measured_peaks(ctx)
     opts = rtg.RenderOptions(progressive=not a.single_pass, max_pass_spp=32)
     hosts = [rtg.parse_scene(json.dumps(s)) for s in scenes]

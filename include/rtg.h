@@ -204,9 +204,18 @@ enum {
   RTG_LAYOUT_MATERIALS = 6,
   RTG_LAYOUT_LIGHTS = 7,
   RTG_LAYOUT_SLOT_PRIM = 8,     /* uint32 per slot: primitive id */
-  RTG_LAYOUT_ROOTS = 9          /* int32[4]: root link, four-wide root link, slots, built on the GPU */
+  RTG_LAYOUT_ROOTS = 9,         /* int32[5]: root link, four-wide root link, slots, built on the GPU,
+                                 * eight-wide root link */
+  RTG_LAYOUT_NODES8 = 10        /* DevNode8, 80 B each (compressed eight-wide nodes, breadth-first) */
 };
 int64_t rtg_scene_layout(rtg_context* ctx, rtg_scene_id scene, int32_t part, void* out, uint64_t cap);
+/* No counterpart in the reference. The device layout a host-compiled scene gets
+ * at upload, computed on the host without a GPU (tests and tools): the same parts
+ * and record formats as rtg_scene_layout (the built-on-GPU flag of ROOTS is 0).
+ * Copies min(cap, size) bytes to out (out may be NULL) and returns the part's full
+ * size in bytes; RTG_ERR_INVALID for an unknown part or a scene compiled without
+ * its BVH. */
+int64_t rtg_host_scene_layout(const rtg_host_scene* scene, int32_t part, void* out, uint64_t cap);
 /* The scene file's own render settings. */
 int rtg_scene_settings(rtg_context* ctx, rtg_scene_id scene, rtg_settings* out);
 int rtg_scene_get_info(rtg_context* ctx, rtg_scene_id scene, rtg_scene_info* out);
@@ -297,6 +306,8 @@ typedef struct rtg_tuning {
   int32_t refine_hits;       /* ray queries report t recomputed in double for the winning primitive
                               * (default 1); 0: the fp32 traversal's own t, the value the renderer's
                               * closest-hit stage hands to shading */
+  int32_t closest_tree;      /* closest-hit walk: 8 the compressed eight-wide tree (default), 2 the binary tree */
+  int32_t shadow_tree;       /* any-hit walk: 4 the four-wide tree (default), 8 the compressed eight-wide tree */
   int32_t reserved;
 } rtg_tuning;
 int rtg_get_tuning(rtg_context* ctx, rtg_tuning* out);

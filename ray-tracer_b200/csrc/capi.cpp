@@ -23,6 +23,7 @@
 #include "host/autotune.hpp"
 #include "host/engine.hpp"
 #include "host/scene_io.hpp"
+#include "host/flatten.hpp"
 
 namespace rtg {
 std::vector<std::uint8_t> encode_png(const std::uint8_t* rgb, int width, int height);
@@ -288,6 +289,35 @@ int rtg_compile_flags(const char* scene_json, const char* base_dir, uint32_t fla
 
 void rtg_host_scene_free(rtg_host_scene* scene) { delete scene; }
 
+int64_t rtg_host_scene_layout(const rtg_host_scene* hs, int32_t part, void* out, uint64_t cap) {
+  if (!hs) return RTG_ERR_INVALID;
+  try {
+    if (!hs->scene->bvh_built) return RTG_ERR_INVALID;
+    const rtg::FlatScene f = rtg::flatten(*hs->scene);
+    const std::int32_t roots[5] = {f.root, f.root4, static_cast<std::int32_t>(f.slot_prim.size()), 0, f.root8};
+    const void* src = nullptr;
+    std::size_t bytes = 0;
+    switch (part) {
+      case RTG_LAYOUT_NODES: src = f.nodes.data(); bytes = f.nodes.size() * sizeof(rtg::DevNode); break;
+      case RTG_LAYOUT_NODES4: src = f.nodes4.data(); bytes = f.nodes4.size() * sizeof(rtg::DevNode4); break;
+      case RTG_LAYOUT_NODES8: src = f.nodes8.data(); bytes = f.nodes8.size() * sizeof(rtg::DevNode8); break;
+      case RTG_LAYOUT_PRIMS: src = f.prims.data(); bytes = f.prims.size() * sizeof(float4); break;
+      case RTG_LAYOUT_SLOT_MATERIAL: src = f.slot_material.data(); bytes = f.slot_material.size() * 4; break;
+      case RTG_LAYOUT_SLOT_NORMALS: src = f.slot_normals.data(); bytes = f.slot_normals.size() * sizeof(float4); break;
+      case RTG_LAYOUT_PLANES: src = f.planes.data(); bytes = f.planes.size() * sizeof(rtg::DevPlane); break;
+      case RTG_LAYOUT_MATERIALS: src = f.materials.data(); bytes = f.materials.size() * sizeof(rtg::DevMaterial); break;
+      case RTG_LAYOUT_LIGHTS: src = f.lights.data(); bytes = f.lights.size() * sizeof(rtg::DevLight); break;
+      case RTG_LAYOUT_SLOT_PRIM: src = f.slot_prim.data(); bytes = f.slot_prim.size() * 4; break;
+      case RTG_LAYOUT_ROOTS: src = roots; bytes = sizeof(roots); break;
+      default: return RTG_ERR_INVALID;
+    }
+    if (out && bytes) std::memcpy(out, src, std::min<std::size_t>(bytes, cap));
+    return static_cast<int64_t>(bytes);
+  } catch (const std::exception&) {
+    return RTG_ERR_INVALID;
+  }
+}
+
 int rtg_host_scene_view(const rtg_host_scene* hs, rtg_scene_view* out) {
   if (!hs || !out) return RTG_ERR_INVALID;
   std::call_once(hs->view_once, [hs] { build_view_arrays(*hs); });
@@ -349,13 +379,14 @@ int64_t rtg_scene_layout(rtg_context* ctx, rtg_scene_id scene, int32_t part, voi
   const int rc = guarded(ctx, [&]() {
     if (ctx->busy) return RTG_ERR_BUSY;
     const rtg::GpuScene& g = ctx->engine->scene(scene);
-    const std::int32_t roots[4] = {g.root, g.root4, g.n_slots, g.device_built ? 1 : 0};
+    const std::int32_t roots[5] = {g.root, g.root4, g.n_slots, g.device_built ? 1 : 0, g.root8};
     const void* src = nullptr;
     bool on_device = true;
     const int64_t slots = g.n_slots;
     switch (part) {
       case RTG_LAYOUT_NODES: src = g.nodes; bytes = int64_t(g.n_interior) * int64_t(sizeof(rtg::DevNode)); break;
       case RTG_LAYOUT_NODES4: src = g.nodes4; bytes = int64_t(g.n_wide) * int64_t(sizeof(rtg::DevNode4)); break;
+      case RTG_LAYOUT_NODES8: src = g.nodes8; bytes = int64_t(g.n_wide8) * int64_t(sizeof(rtg::DevNode8)); break;
       case RTG_LAYOUT_PRIMS: src = g.prims; bytes = slots * 3 * int64_t(sizeof(float4)); break;
       case RTG_LAYOUT_SLOT_MATERIAL: src = g.slot_material; bytes = slots * int64_t(sizeof(uint32_t)); break;
       case RTG_LAYOUT_SLOT_NORMALS: src = g.slot_normals; bytes = slots * 3 * int64_t(sizeof(float4)); break;
@@ -659,7 +690,8 @@ int rtg_trace_closest_noalloc(rtg_context* ctx, rtg_scene_id scene, const float*
       return RTG_ERR_LIMIT;
     }
     const rtg::RtgSceneDev d = ctx->engine->query_descriptor(scene, brute != 0);
-    const cudaError_t e = rtg::noalloc_trace_closest(ctx->engine->device(), d, rays, n, brute, t, prim, is_plane,
+    const cudaError_t e = rtg::noalloc_trace_closest(ctx->engine->device(), d, rays, n, brute,
+                                                     ctx->engine->config().shape.closest_tree, t, prim, is_plane,
                                                      bary, ctx->engine->stream());
     if (e != cudaSuccess) throw rtg::CudaFailure(std::string("rtg_trace_closest_noalloc: ") + cudaGetErrorString(e));
     return RTG_OK;
@@ -700,6 +732,8 @@ int rtg_get_tuning(rtg_context* ctx, rtg_tuning* out) {
     out->serve_budget_bytes = ctx->serve_budget;
     out->serve_reserve_bytes = ctx->serve_reserve;
     out->refine_hits = c.refine_hits ? 1 : 0;
+    out->closest_tree = c.shape.closest_tree;
+    out->shadow_tree = c.shape.shadow_tree;
     return RTG_OK;
   });
 }
@@ -729,6 +763,10 @@ int rtg_set_tuning(rtg_context* ctx, const rtg_tuning* in) {
     c.backlog_pools = in->backlog_pools;
     c.shape.chained = in->chained != 0;
     c.refine_hits = in->refine_hits != 0;
+    if (in->closest_tree != 2 && in->closest_tree != 8) throw std::invalid_argument("closest_tree must be 2 or 8");
+    if (in->shadow_tree != 4 && in->shadow_tree != 8) throw std::invalid_argument("shadow_tree must be 4 or 8");
+    c.shape.closest_tree = in->closest_tree;
+    c.shape.shadow_tree = in->shadow_tree;
     if (in->serve_budget_bytes) ctx->serve_budget = in->serve_budget_bytes;
     if (in->serve_reserve_bytes > ctx->serve_budget) throw std::invalid_argument("serve_reserve_bytes exceeds the budget");
     ctx->serve_reserve = in->serve_reserve_bytes;

@@ -1584,4 +1584,65 @@ void GpuBvhBuilder::emit(const GpuBvhInput& in, DevNode* nodes, DevNode4* nodes4
   BVH_CK(cudaGetLastError());
 }
 
+// ---------------------------------------------------------------------------
+// Slot order of the eight-wide tree
+
+namespace {
+
+__device__ __forceinline__ std::int32_t remap_leaf(std::int32_t link, const std::uint32_t* new_of, std::uint32_t n) {
+  if (link >= 0 || link == INT32_MIN) return link;
+  const std::uint32_t old = static_cast<std::uint32_t>(~link);
+  return old < n ? ~static_cast<std::int32_t>(new_of[old]) : link;
+}
+
+__global__ void k_gather_slots(const std::uint32_t* old_of, std::uint32_t n, const float4* prims_in,
+                               const float4* normals_in, const std::uint32_t* material_in, float4* prims,
+                               float4* normals, std::uint32_t* material) {
+  const std::uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const std::uint32_t o = old_of[k];
+  if (o >= n) return;
+  for (int r = 0; r < 3; ++r) {
+    prims[3 * k + r] = prims_in[3 * o + r];
+    normals[3 * k + r] = normals_in[3 * o + r];
+  }
+  material[k] = material_in[o];
+}
+
+__global__ void k_remap_links(const std::uint32_t* new_of, std::uint32_t n, DevNode* nodes, std::int32_t n_nodes,
+                              DevNode4* nodes4, std::int32_t n_wide) {
+  const std::int32_t i = static_cast<std::int32_t>(blockIdx.x * blockDim.x + threadIdx.x);
+  if (i < n_nodes) {
+    int4 l = nodes[i].link;
+    l.x = remap_leaf(l.x, new_of, n);
+    l.y = remap_leaf(l.y, new_of, n);
+    nodes[i].link = l;
+  }
+  if (i < n_wide) {
+    int4 l = nodes4[i].link;
+    l.x = remap_leaf(l.x, new_of, n);
+    l.y = remap_leaf(l.y, new_of, n);
+    l.z = remap_leaf(l.z, new_of, n);
+    l.w = remap_leaf(l.w, new_of, n);
+    nodes4[i].link = l;
+  }
+}
+
+}  // namespace
+
+cudaError_t apply_slot_order(const std::uint32_t* old_of, const std::uint32_t* new_of, std::uint32_t n_slots,
+                             const float4* prims_in, const float4* normals_in, const std::uint32_t* material_in,
+                             float4* prims, float4* normals, std::uint32_t* material, DevNode* nodes,
+                             std::int32_t n_nodes, DevNode4* nodes4, std::int32_t n_wide, cudaStream_t stream) {
+  if (n_slots) {
+    k_gather_slots<<<(n_slots + 255) / 256, 256, 0, stream>>>(old_of, n_slots, prims_in, normals_in, material_in,
+                                                              prims, normals, material);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  const std::int32_t n = n_nodes > n_wide ? n_nodes : n_wide;
+  if (n > 0) k_remap_links<<<(n + 255) / 256, 256, 0, stream>>>(new_of, n_slots, nodes, n_nodes, nodes4, n_wide);
+  return cudaGetLastError();
+}
+
 }  // namespace rtg

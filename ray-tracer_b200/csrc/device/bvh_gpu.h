@@ -52,6 +52,16 @@ struct GpuBvhCounts {
 void gpu_bvh_preload();
 
 // Owns the scratch memory of one build (from `pool`, stream-ordered).
+// Moves an emitted layout to another slot order (the one the compressed
+// eight-wide tree needs, wide8.hpp): slot k of the output takes old slot
+// old_of[k] of the inputs (prims and normals 3 rows per slot, material 1 word),
+// and the leaf links of `nodes` (n_nodes DevNode) and `nodes4` (n_wide DevNode4)
+// become ~new_of[old start]. Indices are range-checked; stream-ordered.
+cudaError_t apply_slot_order(const std::uint32_t* old_of, const std::uint32_t* new_of, std::uint32_t n_slots,
+                             const float4* prims_in, const float4* normals_in, const std::uint32_t* material_in,
+                             float4* prims, float4* normals, std::uint32_t* material, DevNode* nodes,
+                             std::int32_t n_nodes, DevNode4* nodes4, std::int32_t n_wide, cudaStream_t stream);
+
 class GpuBvhBuilder {
  public:
   GpuBvhBuilder(cudaStream_t stream, cudaMemPool_t pool) : stream_(stream), pool_(pool) {}

@@ -29,6 +29,7 @@
 // WaveCounters (Aila & Laine, "Understanding the Efficiency of Ray Traversal on
 // GPUs", HPG 2009), so uneven traversal costs balance across SMs.
 #include <cfloat>
+#include <type_traits>
 
 #include "device/shade.cuh"
 #include "device/wave.h"
@@ -184,9 +185,33 @@ __global__ void __launch_bounds__(kMaxGen) k_plan(WaveBuffers wb, int par) {
 }
 
 // ---------------------------------------------------------------------------
-template <int kBlock, bool kCount>
+// Closest hit of one ray: the eight-wide tree (kWide8) or the binary tree, or
+// brute force when the job asks for it.
+template <int kBlock, bool kCount, bool kWide8, class Stack>
+__device__ __forceinline__ RayHit trace_closest(const RtgSceneDev& J, float3 o, float3 d, float tmin, Stack* stack,
+                                                TraceCount& tc) {
+  if (!J.use_bvh) return closest_brute<kCount>(J, o, d, tmin, FLT_MAX, tc);
+  if constexpr (kWide8) return closest_hit8<kStackSmem, kBlock, kCount>(J, o, d, tmin, FLT_MAX, stack, tc);
+  else return closest_hit<kStackSmem, kBlock, kCount>(J, o, d, tmin, FLT_MAX, stack, tc);
+}
+
+// Any hit of one shadow ray below tmax: the eight-wide or the four-wide tree.
+template <int kBlock, bool kCount, bool kWide8, class Stack>
+__device__ __forceinline__ bool trace_any(const RtgSceneDev& J, float3 o, float3 d, float tmin, float tmax,
+                                          Stack* stack, TraceCount& tc) {
+  if (!J.use_bvh) return any_brute(J, o, d, tmin, tmax);
+  if constexpr (kWide8) return any_hit8<kStackSmem, kBlock, kCount>(J, o, d, tmin, tmax, stack, tc);
+  else return any_hit4<kStackSmem, kBlock, kCount>(J, o, d, tmin, tmax, stack, tc);
+}
+
+// Per-thread traversal stack entries in shared memory: groups (two words) for
+// the eight-wide walk, node links for the binary and four-wide walks.
+template <bool kWide8>
+using StackEntry = std::conditional_t<kWide8, uint2, int>;
+
+template <int kBlock, bool kCount, bool kWide8>
 __global__ void __launch_bounds__(kBlock) k_extend(WaveBuffers wb, int par) {
-  __shared__ int stack[kStackSmem * kBlock];
+  __shared__ StackEntry<kWide8> stack[kStackSmem * kBlock];
   chain_to_previous_grid();
   WaveCounters* C = wb.cnt;
   const std::uint32_t live = C->live[par];
@@ -234,8 +259,7 @@ __global__ void __launch_bounds__(kBlock) k_extend(WaveBuffers wb, int par) {
       job = __float_as_uint(b.w) >> kMetaSceneShift;
     }
     const RtgSceneDev& J = wb.jobs[job];
-    const RayHit h = J.use_bvh ? closest_hit<kStackSmem, kBlock, kCount>(J, o, d, kRayTMin, FLT_MAX, stack, tc)
-                               : closest_brute<kCount>(J, o, d, kRayTMin, FLT_MAX, tc);
+    const RayHit h = trace_closest<kBlock, kCount, kWide8>(J, o, d, kRayTMin, stack, tc);
     __stcs(&wb.hits[i], make_float4(h.t, __uint_as_float(h.word), h.b1, h.b2));
     ++rays;
   }
@@ -408,9 +432,9 @@ __global__ void __launch_bounds__(kBlock, 1024 / kBlock) k_shade(WaveBuffers wb,
 }
 
 // ---------------------------------------------------------------------------
-template <int kBlock, bool kCount>
+template <int kBlock, bool kCount, bool kWide8>
 __global__ void __launch_bounds__(kBlock) k_shadow(WaveBuffers wb) {
-  __shared__ int stack[kStackSmem * kBlock];
+  __shared__ StackEntry<kWide8> stack[kStackSmem * kBlock];
   chain_to_previous_grid();
   WaveCounters* C = wb.cnt;
   const std::uint32_t n = C->n_shadow;
@@ -424,8 +448,7 @@ __global__ void __launch_bounds__(kBlock) k_shadow(WaveBuffers wb) {
     const float4 a = __ldcs(&wb.sh_a[i]), b = __ldcs(&wb.sh_b[i]), c = __ldcs(&wb.sh_c[i]);
     const RtgSceneDev& J = wb.jobs[__float_as_uint(c.w)];
     const float3 o = f3(a), d = f3(b);
-    const bool blocked = J.use_bvh ? any_hit4<kStackSmem, kBlock, kCount>(J, o, d, kRayTMin, b.w, stack, tc)
-                                   : any_brute(J, o, d, kRayTMin, b.w);
+    const bool blocked = trace_any<kBlock, kCount, kWide8>(J, o, d, kRayTMin, b.w, stack, tc);
     ++rays;
     if (!blocked) {
       float4* const slot = &wb.radiance[__float_as_uint(a.w)];
@@ -453,9 +476,10 @@ struct Pending {
   int depth;
 };
 
-template <int kBlock>
+template <int kBlock, bool kWide8>
 __device__ __forceinline__ float3 direct_light_all(const RtgSceneDev& J, const DevMaterial& m, const Surface& s,
-                                                   Pcg& rng, int* stack, TraceCount& tc, std::uint64_t& shadow_rays) {
+                                                   Pcg& rng, StackEntry<kWide8>* stack, TraceCount& tc,
+                                                   std::uint64_t& shadow_rays) {
   float3 sum = f3(0.f, 0.f, 0.f);
   for (int li = 0; li < J.n_lights; ++li) {
     const LightSample ls = sample_light(J.lights + li, s, rng);
@@ -464,17 +488,16 @@ __device__ __forceinline__ float3 direct_light_all(const RtgSceneDev& J, const D
     if (is_zero3(f) || is_zero3(ls.li_over_pdf)) continue;
     const ShadowRay sr = shadow_ray(s, ls);
     ++shadow_rays;
-    const bool blocked = J.use_bvh ? any_hit4<kStackSmem, kBlock, false>(J, sr.o, sr.d, kRayTMin, sr.tmax, stack, tc)
-                                   : any_brute(J, sr.o, sr.d, kRayTMin, sr.tmax);
+    const bool blocked = trace_any<kBlock, false, kWide8>(J, sr.o, sr.d, kRayTMin, sr.tmax, stack, tc);
     if (!blocked) sum = sum + f * ls.li_over_pdf;
   }
   return sum;
 }
 
-template <int kBlock>
+template <int kBlock, bool kWide8>
 __global__ void __launch_bounds__(kBlock) k_direct(const RtgSceneDev* __restrict__ job, DevSegment seg, float4* radiance,
                                                    WaveCounters* C) {
-  __shared__ int stack[kStackSmem * kBlock];
+  __shared__ StackEntry<kWide8> stack[kStackSmem * kBlock];
   TraceCount tc;
   std::uint64_t rays = 0, shadow_rays = 0;
   const RtgSceneDev& J = *job;
@@ -488,8 +511,7 @@ __global__ void __launch_bounds__(kBlock) k_direct(const RtgSceneDev* __restrict
     bool overflow = false;
     while (true) {
       ++rays;
-      const RayHit h = J.use_bvh ? closest_hit<kStackSmem, kBlock, false>(J, cur.o, cur.d, kRayTMin, FLT_MAX, stack, tc)
-                                 : closest_brute<false>(J, cur.o, cur.d, kRayTMin, FLT_MAX, tc);
+      const RayHit h = trace_closest<kBlock, false, kWide8>(J, cur.o, cur.d, kRayTMin, stack, tc);
       bool next = false;
       if (h.word == kHitMiss) {
         L = L + cur.w * background(J, cur.d);
@@ -500,7 +522,7 @@ __global__ void __launch_bounds__(kBlock) k_direct(const RtgSceneDev* __restrict
         if (cur.depth < J.max_depth) {
           const std::uint32_t kind = kind_of(m);
           if (kind == kLambertian) {
-            L = L + cur.w * direct_light_all<kBlock>(J, m, s, cs.rng, stack, tc, shadow_rays);
+            L = L + cur.w * direct_light_all<kBlock, kWide8>(J, m, s, cs.rng, stack, tc, shadow_rays);
           } else if (kind == kMetal) {
             Scatter sr;
             if (scatter(m, cur.d, s, cs.rng, sr)) {
@@ -613,30 +635,36 @@ __global__ void k_resolve(const double* __restrict__ fb_sum, const std::uint32_t
 }
 
 // ---------------------------------------------------------------------------
+// `tree` picks the walk: 8 the eight-wide tree; otherwise the binary tree
+// (closest hit) or the four-wide tree (any hit).
 template <int kBlock>
 __global__ void __launch_bounds__(kBlock) k_ray_closest(const RtgSceneDev* __restrict__ job, const float4* __restrict__ rays,
-                                                        std::uint32_t n, float4* out, int brute) {
-  __shared__ int stack[kStackSmem * kBlock];
+                                                        std::uint32_t n, float4* out, int brute, int tree) {
+  __shared__ uint2 stack[kStackSmem * kBlock];
   const std::uint32_t i = blockIdx.x * kBlock + threadIdx.x;
   if (i >= n) return;
   const float4 a = rays[2 * i], b = rays[2 * i + 1];
   TraceCount tc;
-  RayHit h = brute ? closest_brute<false>(*job, f3(a), f3(b), a.w, b.w, tc)
-                   : closest_hit<kStackSmem, kBlock, false>(*job, f3(a), f3(b), a.w, b.w, stack, tc);
+  RayHit h;
+  if (brute) h = closest_brute<false>(*job, f3(a), f3(b), a.w, b.w, tc);
+  else if (tree == 8) h = closest_hit8<kStackSmem, kBlock, false>(*job, f3(a), f3(b), a.w, b.w, stack, tc);
+  else h = closest_hit<kStackSmem, kBlock, false>(*job, f3(a), f3(b), a.w, b.w, reinterpret_cast<int*>(stack), tc);
   refine_hit(*job, f3(a), f3(b), h);
   out[i] = make_float4(h.t, __uint_as_float(h.word), h.b1, h.b2);
 }
 
 template <int kBlock>
 __global__ void __launch_bounds__(kBlock) k_ray_any(const RtgSceneDev* __restrict__ job, const float4* __restrict__ rays,
-                                                    std::uint32_t n, std::uint32_t* out, int brute) {
-  __shared__ int stack[kStackSmem * kBlock];
+                                                    std::uint32_t n, std::uint32_t* out, int brute, int tree) {
+  __shared__ uint2 stack[kStackSmem * kBlock];
   const std::uint32_t i = blockIdx.x * kBlock + threadIdx.x;
   if (i >= n) return;
   const float4 a = rays[2 * i], b = rays[2 * i + 1];
   TraceCount tc;
-  const bool hit = brute ? any_brute(*job, f3(a), f3(b), a.w, b.w)
-                         : any_hit4<kStackSmem, kBlock, false>(*job, f3(a), f3(b), a.w, b.w, stack, tc);
+  bool hit;
+  if (brute) hit = any_brute(*job, f3(a), f3(b), a.w, b.w);
+  else if (tree == 8) hit = any_hit8<kStackSmem, kBlock, false>(*job, f3(a), f3(b), a.w, b.w, stack, tc);
+  else hit = any_hit4<kStackSmem, kBlock, false>(*job, f3(a), f3(b), a.w, b.w, reinterpret_cast<int*>(stack), tc);
   out[i] = hit ? 1u : 0u;
 }
 
@@ -651,20 +679,25 @@ int persistent_blocks(K kernel, int block) {
   return sms * per_sm;
 }
 
+// Persistent grid sizes per kernel variant: [counting][eight-wide].
 struct BlockCounts {
-  int extend = 0, extend_counting = 0, shade = 0, shade_mis = 0, shadow = 0, shadow_counting = 0;
+  int extend[2][2] = {}, shadow[2][2] = {}, shade = 0, shade_mis = 0;
 };
 
 template <int kBlock>
 const BlockCounts& block_counts() {
   static BlockCounts bc = [] {
     BlockCounts b;
-    b.extend = persistent_blocks(k_extend<kBlock, false>, kBlock);
-    b.extend_counting = persistent_blocks(k_extend<kBlock, true>, kBlock);
+    b.extend[0][0] = persistent_blocks(k_extend<kBlock, false, false>, kBlock);
+    b.extend[0][1] = persistent_blocks(k_extend<kBlock, false, true>, kBlock);
+    b.extend[1][0] = persistent_blocks(k_extend<kBlock, true, false>, kBlock);
+    b.extend[1][1] = persistent_blocks(k_extend<kBlock, true, true>, kBlock);
     b.shade = persistent_blocks(k_shade<kBlock, false>, kBlock);
     b.shade_mis = persistent_blocks(k_shade<kBlock, true>, kBlock);
-    b.shadow = persistent_blocks(k_shadow<kBlock, false>, kBlock);
-    b.shadow_counting = persistent_blocks(k_shadow<kBlock, true>, kBlock);
+    b.shadow[0][0] = persistent_blocks(k_shadow<kBlock, false, false>, kBlock);
+    b.shadow[0][1] = persistent_blocks(k_shadow<kBlock, false, true>, kBlock);
+    b.shadow[1][0] = persistent_blocks(k_shadow<kBlock, true, false>, kBlock);
+    b.shadow[1][1] = persistent_blocks(k_shadow<kBlock, true, true>, kBlock);
     return b;
   }();
   return bc;
@@ -688,6 +721,16 @@ cudaError_t launch_chained(void (*kernel)(KArgs...), int grid, int block, bool p
   return cudaLaunchKernelEx(&cfg, kernel, args...);
 }
 
+template <int kBlock, bool kCount, bool kWide8>
+cudaError_t launch_extend(int blocks, bool pdl, cudaStream_t stream, const WaveBuffers& wb, int par) {
+  return launch_chained(k_extend<kBlock, kCount, kWide8>, blocks, kBlock, pdl, stream, wb, par);
+}
+
+template <int kBlock, bool kCount, bool kWide8>
+cudaError_t launch_shadow(int blocks, bool pdl, cudaStream_t stream, const WaveBuffers& wb) {
+  return launch_chained(k_shadow<kBlock, kCount, kWide8>, blocks, kBlock, pdl, stream, wb);
+}
+
 template <int kBlock>
 cudaError_t stage_impl(Stage stage, const WaveBuffers& wb, int par, const LaunchShape& shape, bool count,
                        cudaStream_t stream) {
@@ -697,9 +740,12 @@ cudaError_t stage_impl(Stage stage, const WaveBuffers& wb, int par, const Launch
     case Stage::Plan:
       return launch_chained(k_plan, 1, kMaxGen, pdl, stream, wb, par);
     case Stage::Extend: {
-      const int blocks = shape.extend_blocks ? shape.extend_blocks : (count ? bc.extend_counting : bc.extend);
-      return count ? launch_chained(k_extend<kBlock, true>, blocks, kBlock, pdl, stream, wb, par)
-                   : launch_chained(k_extend<kBlock, false>, blocks, kBlock, pdl, stream, wb, par);
+      const bool w8 = shape.closest_tree == 8;
+      const int blocks = shape.extend_blocks ? shape.extend_blocks : bc.extend[count][w8];
+      if (count) return w8 ? launch_extend<kBlock, true, true>(blocks, pdl, stream, wb, par)
+                           : launch_extend<kBlock, true, false>(blocks, pdl, stream, wb, par);
+      return w8 ? launch_extend<kBlock, false, true>(blocks, pdl, stream, wb, par)
+                : launch_extend<kBlock, false, false>(blocks, pdl, stream, wb, par);
     }
     case Stage::Shade: {
       const int blocks = shape.shade_blocks ? shape.shade_blocks : (shape.mis ? bc.shade_mis : bc.shade);
@@ -707,9 +753,12 @@ cudaError_t stage_impl(Stage stage, const WaveBuffers& wb, int par, const Launch
                        : launch_chained(k_shade<kBlock, false>, blocks, kBlock, pdl, stream, wb, par);
     }
     case Stage::Shadow: {
-      const int blocks = shape.shadow_blocks ? shape.shadow_blocks : (count ? bc.shadow_counting : bc.shadow);
-      return count ? launch_chained(k_shadow<kBlock, true>, blocks, kBlock, pdl, stream, wb)
-                   : launch_chained(k_shadow<kBlock, false>, blocks, kBlock, pdl, stream, wb);
+      const bool w8 = shape.shadow_tree == 8;
+      const int blocks = shape.shadow_blocks ? shape.shadow_blocks : bc.shadow[count][w8];
+      if (count) return w8 ? launch_shadow<kBlock, true, true>(blocks, pdl, stream, wb)
+                           : launch_shadow<kBlock, true, false>(blocks, pdl, stream, wb);
+      return w8 ? launch_shadow<kBlock, false, true>(blocks, pdl, stream, wb)
+                : launch_shadow<kBlock, false, false>(blocks, pdl, stream, wb);
     }
   }
   return cudaErrorInvalidValue;
@@ -743,10 +792,15 @@ cudaError_t launch_accumulate(const RtgSceneDev* job_dev, std::uint64_t pixels, 
 }
 
 cudaError_t launch_direct(const RtgSceneDev* job_dev, const DevSegment& seg, float4* radiance, WaveCounters* cnt,
-                          cudaStream_t stream) {
-  static int blocks = 0;
-  if (!blocks) blocks = persistent_blocks(k_direct<128>, 128);
-  k_direct<128><<<blocks, 128, 0, stream>>>(job_dev, seg, radiance, cnt);
+                          bool wide8, cudaStream_t stream) {
+  static int blocks[2] = {0, 0};
+  if (wide8) {
+    if (!blocks[1]) blocks[1] = persistent_blocks(k_direct<128, true>, 128);
+    k_direct<128, true><<<blocks[1], 128, 0, stream>>>(job_dev, seg, radiance, cnt);
+  } else {
+    if (!blocks[0]) blocks[0] = persistent_blocks(k_direct<128, false>, 128);
+    k_direct<128, false><<<blocks[0], 128, 0, stream>>>(job_dev, seg, radiance, cnt);
+  }
   return cudaGetLastError();
 }
 
@@ -759,16 +813,16 @@ cudaError_t launch_resolve(const double* fb_sum, const std::uint32_t* fb_count, 
 }
 
 cudaError_t launch_ray_closest(const RtgSceneDev* job_dev, const float4* rays, std::uint32_t n, float4* out, int brute,
-                               cudaStream_t stream) {
+                               int tree, cudaStream_t stream) {
   if (n == 0) return cudaSuccess;
-  k_ray_closest<128><<<(n + 127) / 128, 128, 0, stream>>>(job_dev, rays, n, out, brute);
+  k_ray_closest<128><<<(n + 127) / 128, 128, 0, stream>>>(job_dev, rays, n, out, brute, tree);
   return cudaGetLastError();
 }
 
 cudaError_t launch_ray_any(const RtgSceneDev* job_dev, const float4* rays, std::uint32_t n, std::uint32_t* out, int brute,
-                           cudaStream_t stream) {
+                           int tree, cudaStream_t stream) {
   if (n == 0) return cudaSuccess;
-  k_ray_any<128><<<(n + 127) / 128, 128, 0, stream>>>(job_dev, rays, n, out, brute);
+  k_ray_any<128><<<(n + 127) / 128, 128, 0, stream>>>(job_dev, rays, n, out, brute, tree);
   return cudaGetLastError();
 }
 

@@ -41,6 +41,40 @@ struct alignas(16) DevNode4 {
   int4 pad;
 };
 constexpr std::int32_t kNoChild = INT32_MIN;
+
+// Compressed eight-child BVH node, 80 bytes (after Ylitie, Karras and Laine,
+// "Efficient Incoherent Ray Traversal on GPUs Through Compressed Wide BVHs",
+// HPG 2017), collapsed from the binary tree with the same leaves. Child boxes
+// are stored as 8-bit offsets from the node origin `p` in units of a power of two
+// per axis, rounded outward, so a decoded box always encloses the child's fp32
+// box. An unused child has lo = 255, hi = 0 on every axis (never hit).
+//  a: p.x, p.y, p.z; w bits: e_x | e_y << 8 | e_z << 16 | imask << 24, where e is a
+//     biased float exponent (scale = 2^(e - 127)) and imask bit s marks child
+//     slot s as an interior node
+//  b: x = child_base (first interior child; interior children are stored
+//     contiguously in slot order), y = prim_base (first primitive slot of the
+//     leaf children), z/w = meta bytes 0-3 / 4-7: for an interior child its index
+//     among the interior children, for a leaf child the offset of its first slot
+//     from prim_base (the leaf runs to the slot carrying kLastInLeaf)
+//  qlo_xy: x, y = lo.x bytes of children 0-3, 4-7; z, w = lo.y bytes
+//  qlo_z_hi_x: x, y = lo.z bytes; z, w = hi.x bytes
+//  qhi_yz: x, y = hi.y bytes; z, w = hi.z bytes
+// Child slots are assigned by the direction of each child's centre from the
+// node's centre (slot bit k set: positive along axis k), so a ray visiting slots
+// in the order s ^ octant meets the children roughly front to back.
+struct alignas(16) DevNode8 {
+  float4 a;
+  uint4 b;
+  uint4 qlo_xy;
+  uint4 qlo_z_hi_x;
+  uint4 qhi_yz;
+};
+static_assert(sizeof(DevNode8) == 80, "DevNode8 must be 80 bytes");
+// Leaf children of one node start within this many slots of its prim_base.
+constexpr int kWide8MaxLeafOffset = 255;
+// Traversal stack entries an eight-wide walk may need (one group per level; the
+// builder rejects deeper trees).
+constexpr int kWide8StackDepth = 64;
 // Traversal stack entries a 4-wide walk may need: 3 per level (the binary tree's
 // depth cap of 60 bounds the four-wide depth) plus the current one.
 constexpr int kWideStackDepth = 3 * 61 + 1;
@@ -123,7 +157,9 @@ struct alignas(16) RtgSceneDev {
   // 4-wide copy of the same tree (any-hit queries).
   const DevNode4* nodes4;
   std::int32_t root4;         // as root, for nodes4
-  std::int32_t pad1;
+  std::int32_t root8;         // as root, for nodes8
+  // Compressed 8-wide copy of the same tree (closest-hit queries).
+  const DevNode8* nodes8;
 };
 
 // A segment is one pass of one render: samples [pass_s0, pass_s0 + pass_spp) of every

@@ -72,16 +72,19 @@ cudaError_t scratch_address(int device, unsigned char** out) {
 constexpr int kBlock = 128;
 constexpr int kStack = 16;
 
-__global__ void __launch_bounds__(kBlock) k_ray_closest_scratch(unsigned char* scratch, std::uint32_t n, int brute) {
-  __shared__ int stack[kStack * kBlock];
+__global__ void __launch_bounds__(kBlock) k_ray_closest_scratch(unsigned char* scratch, std::uint32_t n, int brute,
+                                                                int tree) {
+  __shared__ uint2 stack[kStack * kBlock];
   const std::uint32_t i = blockIdx.x * kBlock + threadIdx.x;
   if (i >= n) return;
   const RtgSceneDev& job = *reinterpret_cast<const RtgSceneDev*>(scratch);
   const float4* rays = reinterpret_cast<const float4*>(scratch + kRaysOff);
   const float4 a = rays[2 * i], b = rays[2 * i + 1];
   TraceCount tc;
-  RayHit h = brute ? closest_brute<false>(job, f3(a), f3(b), a.w, b.w, tc)
-                   : closest_hit<kStack, kBlock, false>(job, f3(a), f3(b), a.w, b.w, stack, tc);
+  RayHit h;
+  if (brute) h = closest_brute<false>(job, f3(a), f3(b), a.w, b.w, tc);
+  else if (tree == 8) h = closest_hit8<kStack, kBlock, false>(job, f3(a), f3(b), a.w, b.w, stack, tc);
+  else h = closest_hit<kStack, kBlock, false>(job, f3(a), f3(b), a.w, b.w, reinterpret_cast<int*>(stack), tc);
   refine_hit(job, f3(a), f3(b), h);
   const bool miss = h.word == kHitMiss;
   const bool plane = !miss && (h.word & kHitPlaneBit);
@@ -97,7 +100,7 @@ __global__ void __launch_bounds__(kBlock) k_ray_closest_scratch(unsigned char* s
 }  // namespace
 
 cudaError_t noalloc_trace_closest(int device, const RtgSceneDev& job, const float* rays, std::uint64_t n, int brute,
-                                  float* t, std::int32_t* prim, std::int32_t* is_plane, float* bary,
+                                  int tree, float* t, std::int32_t* prim, std::int32_t* is_plane, float* bary,
                                   cudaStream_t stream) {
   if (n > kNoAllocMaxRays) return cudaErrorInvalidValue;
   if (n == 0) return cudaSuccess;
@@ -111,7 +114,7 @@ cudaError_t noalloc_trace_closest(int device, const RtgSceneDev& job, const floa
   if ((e = cudaMemcpyAsync(s, &job, sizeof(job), cudaMemcpyHostToDevice, stream)) != cudaSuccess) return e;
   if ((e = cudaMemcpyAsync(s + kRaysOff, rays, n * 32, cudaMemcpyHostToDevice, stream)) != cudaSuccess) return e;
   const unsigned blocks = static_cast<unsigned>((n + kBlock - 1) / kBlock);
-  k_ray_closest_scratch<<<blocks, kBlock, 0, stream>>>(s, static_cast<std::uint32_t>(n), brute);
+  k_ray_closest_scratch<<<blocks, kBlock, 0, stream>>>(s, static_cast<std::uint32_t>(n), brute, tree);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if (t && (e = cudaMemcpyAsync(t, s + kTOff, n * 4, cudaMemcpyDeviceToHost, stream)) != cudaSuccess) return e;
   if (prim && (e = cudaMemcpyAsync(prim, s + kPrimOff, n * 4, cudaMemcpyDeviceToHost, stream)) != cudaSuccess) return e;

@@ -295,6 +295,208 @@ __device__ __forceinline__ bool any_hit4(const RtgSceneDev& sc, float3 o, float3
   return false;
 }
 
+// ---------------------------------------------------------------------------
+// Compressed eight-wide tree (DevNode8; Ylitie, Karras and Laine, HPG 2017).
+//
+// A ray visits a node's children in the order of their slots XOR its direction
+// octant, which the slot assignment makes roughly front to back. The traversal
+// stack holds groups of children still to visit: the node index of the group's
+// first interior child and one word with the node's interior-slot mask (bits
+// 8-15) and the visit-order bits of the children left (bits 0-7). A node visit
+// pushes at most the rest of its group, so the stack needs one entry per level.
+// Leaf children hit at a node are tested at once, in visit order, before the
+// walk descends.
+
+struct Wide8Ray {
+  float3 o, inv;
+  std::uint32_t oct;  // bit k set: the direction is negative along axis k
+  __device__ __forceinline__ Wide8Ray(float3 origin, float3 d) : o(origin) {
+    // As SlabRay: a zero component becomes a tiny one of the same sign.
+    auto safe = [](float c) { return fabsf(c) < 1e-20f ? copysignf(1e-20f, c) : c; };
+    inv = f3(1.f / safe(d.x), 1.f / safe(d.y), 1.f / safe(d.z));
+    oct = (inv.x < 0.f ? 1u : 0u) | (inv.y < 0.f ? 2u : 0u) | (inv.z < 0.f ? 4u : 0u);
+  }
+};
+
+// Byte k (0-3) of `w` as a float, exactly: 2^23 + b built by a byte permute, then 2^23 subtracted.
+__device__ __forceinline__ float quant_byte(std::uint32_t w, int k) {
+  return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7440u | static_cast<unsigned>(k))) - 8388608.f;
+}
+
+struct Node8Hits {
+  std::uint32_t inner;  // visit-order bits of interior children hit
+  std::uint32_t leaves; // visit-order bits of leaf children hit
+  std::uint32_t imask;  // interior slots of the node
+  uint4 b;              // child_base, prim_base, meta 0-3, meta 4-7
+};
+
+// Slab tests of a node's eight children against [tmin, tmax].
+__device__ __forceinline__ Node8Hits node8_hits(const DevNode8* __restrict__ nd, const Wide8Ray& r, float tmin,
+                                                float tmax) {
+  const float4 a = __ldg(&nd->a);
+  Node8Hits h;
+  h.b = __ldg(&nd->b);
+  const uint4 q0 = __ldg(&nd->qlo_xy), q1 = __ldg(&nd->qlo_z_hi_x), q2 = __ldg(&nd->qhi_yz);
+  const std::uint32_t ew = __float_as_uint(a.w);
+  h.imask = ew >> 24;
+  // Node space: t = q * (scale / d) + (p - o) / d per axis.
+  const float ax = __uint_as_float((ew & 0xFFu) << 23) * r.inv.x;
+  const float ay = __uint_as_float(((ew >> 8) & 0xFFu) << 23) * r.inv.y;
+  const float az = __uint_as_float(((ew >> 16) & 0xFFu) << 23) * r.inv.z;
+  const float bx = (a.x - r.o.x) * r.inv.x, by = (a.y - r.o.y) * r.inv.y, bz = (a.z - r.o.z) * r.inv.z;
+  // Near and far planes per axis: lo bytes when the direction is positive.
+  const bool px = !(r.oct & 1u), py = !(r.oct & 2u), pz = !(r.oct & 4u);
+  const std::uint32_t nx0 = px ? q0.x : q1.z, nx1 = px ? q0.y : q1.w, fx0 = px ? q1.z : q0.x, fx1 = px ? q1.w : q0.y;
+  const std::uint32_t ny0 = py ? q0.z : q2.x, ny1 = py ? q0.w : q2.y, fy0 = py ? q2.x : q0.z, fy1 = py ? q2.y : q0.w;
+  const std::uint32_t nz0 = pz ? q1.x : q2.z, nz1 = pz ? q1.y : q2.w, fz0 = pz ? q2.z : q1.x, fz1 = pz ? q2.w : q1.y;
+  h.inner = h.leaves = 0u;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const int k = j & 3;
+    const float tnx = fmaf(quant_byte(j < 4 ? nx0 : nx1, k), ax, bx);
+    const float tny = fmaf(quant_byte(j < 4 ? ny0 : ny1, k), ay, by);
+    const float tnz = fmaf(quant_byte(j < 4 ? nz0 : nz1, k), az, bz);
+    const float tfx = fmaf(quant_byte(j < 4 ? fx0 : fx1, k), ax, bx);
+    const float tfy = fmaf(quant_byte(j < 4 ? fy0 : fy1, k), ay, by);
+    const float tfz = fmaf(quant_byte(j < 4 ? fz0 : fz1, k), az, bz);
+    const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
+    const float tf = fminf(fminf(tfx, tfy), fminf(tfz, tmax));
+    if (tn <= tf) {
+      const std::uint32_t bit = 1u << (static_cast<std::uint32_t>(j) ^ r.oct);
+      if ((h.imask >> j) & 1u) h.inner |= bit;
+      else h.leaves |= bit;
+    }
+  }
+  return h;
+}
+
+// First slot of the leaf child in `slot` of a node.
+__device__ __forceinline__ int leaf8_first(const uint4& b, std::uint32_t slot) {
+  return static_cast<int>(b.y + (((slot < 4 ? b.z : b.w) >> (8 * (slot & 3u))) & 0xFFu));
+}
+
+template <int kStackSmem, int kBlock>
+struct GroupStack {
+  uint2* smem;  // this thread's column: entry k at smem[k * kBlock]
+  uint2 spill[kWide8StackDepth - kStackSmem];
+  int sp = 0;
+  __device__ __forceinline__ explicit GroupStack(uint2* base) : smem(base + threadIdx.x) {}
+  __device__ __forceinline__ void push(std::uint32_t base, std::uint32_t mask) {
+    const uint2 v = make_uint2(base, mask);
+    if (sp < kStackSmem) smem[sp * kBlock] = v;
+    else spill[sp - kStackSmem] = v;
+    ++sp;
+  }
+  __device__ __forceinline__ bool pop(std::uint32_t& base, std::uint32_t& mask) {
+    if (sp == 0) return false;
+    --sp;
+    const uint2 v = sp < kStackSmem ? smem[sp * kBlock] : spill[sp - kStackSmem];
+    base = v.x;
+    mask = v.y;
+    return true;
+  }
+};
+
+// Closest hit over planes then the eight-wide tree. `stack_base` is the block's
+// shared group-stack area (kStackSmem * kBlock entries).
+template <int kStackSmem, int kBlock, bool kCount>
+__device__ __forceinline__ RayHit closest_hit8(const RtgSceneDev& sc, float3 o, float3 d, float tmin, float tmax,
+                                               uint2* stack_base, TraceCount& cnt) {
+  RayHit best{tmax, kHitMiss, 0.f, 0.f};
+  for (int i = 0; i < sc.n_planes; ++i) {
+    float t;
+    if (plane_test(sc.planes[i], o, d, tmin, best.t, t)) {
+      best.t = t;
+      best.word = kHitPlaneBit | static_cast<std::uint32_t>(i);
+    }
+  }
+  if (sc.root8 == INT32_MIN) return best;
+  if (sc.root8 < 0) {
+    for (int slot = ~sc.root8;; ++slot) {
+      const std::uint32_t id = prim_slot_test(sc.prims, slot, o, d, tmin, best);
+      if (kCount) cnt.add_prim(id);
+      if (id & kLastInLeaf) break;
+    }
+    return best;
+  }
+  const Wide8Ray r(o, d);
+  GroupStack<kStackSmem, kBlock> st(stack_base);
+  // The root as the one interior child (slot 0) of a group.
+  std::uint32_t g_base = static_cast<std::uint32_t>(sc.root8), g_mask = (1u << r.oct) | (1u << 8);
+  while (true) {
+    if ((g_mask & 0xFFu) == 0u) {
+      if (!st.pop(g_base, g_mask)) break;
+      continue;
+    }
+    const std::uint32_t pos = static_cast<std::uint32_t>(__ffs(g_mask & 0xFFu) - 1);
+    g_mask &= ~(1u << pos);
+    const std::uint32_t slot = pos ^ r.oct;
+    const std::uint32_t node = g_base + __popc((g_mask >> 8) & ((1u << slot) - 1u));
+    if (g_mask & 0xFFu) st.push(g_base, g_mask);
+    if (kCount) cnt.nodes++;
+    const Node8Hits h = node8_hits(sc.nodes8 + node, r, tmin, best.t);
+    for (std::uint32_t lh = h.leaves; lh; lh &= lh - 1u) {
+      const std::uint32_t ls = static_cast<std::uint32_t>(__ffs(lh) - 1) ^ r.oct;
+      for (int s = leaf8_first(h.b, ls);; ++s) {
+        const std::uint32_t id = prim_slot_test(sc.prims, s, o, d, tmin, best);
+        if (kCount) cnt.add_prim(id);
+        if (id & kLastInLeaf) break;
+      }
+    }
+    g_base = h.b.x;
+    g_mask = h.inner | (h.imask << 8);
+  }
+  return best;
+}
+
+// Any hit over planes then the eight-wide tree (first hit wins).
+template <int kStackSmem, int kBlock, bool kCount>
+__device__ __forceinline__ bool any_hit8(const RtgSceneDev& sc, float3 o, float3 d, float tmin, float tmax,
+                                         uint2* stack_base, TraceCount& cnt) {
+  for (int i = 0; i < sc.n_planes; ++i) {
+    float t;
+    if (plane_test(sc.planes[i], o, d, tmin, tmax, t)) return true;
+  }
+  if (sc.root8 == INT32_MIN) return false;
+  RayHit probe{tmax, kHitMiss, 0.f, 0.f};
+  if (sc.root8 < 0) {
+    for (int slot = ~sc.root8;; ++slot) {
+      const std::uint32_t id = prim_slot_test(sc.prims, slot, o, d, tmin, probe);
+      if (kCount) cnt.add_prim(id);
+      if (probe.word != kHitMiss) return true;
+      if (id & kLastInLeaf) return false;
+    }
+  }
+  const Wide8Ray r(o, d);
+  GroupStack<kStackSmem, kBlock> st(stack_base);
+  std::uint32_t g_base = static_cast<std::uint32_t>(sc.root8), g_mask = (1u << r.oct) | (1u << 8);
+  while (true) {
+    if ((g_mask & 0xFFu) == 0u) {
+      if (!st.pop(g_base, g_mask)) break;
+      continue;
+    }
+    const std::uint32_t pos = static_cast<std::uint32_t>(__ffs(g_mask & 0xFFu) - 1);
+    g_mask &= ~(1u << pos);
+    const std::uint32_t slot = pos ^ r.oct;
+    const std::uint32_t node = g_base + __popc((g_mask >> 8) & ((1u << slot) - 1u));
+    if (g_mask & 0xFFu) st.push(g_base, g_mask);
+    if (kCount) cnt.nodes++;
+    const Node8Hits h = node8_hits(sc.nodes8 + node, r, tmin, tmax);
+    for (std::uint32_t lh = h.leaves; lh; lh &= lh - 1u) {
+      const std::uint32_t ls = static_cast<std::uint32_t>(__ffs(lh) - 1) ^ r.oct;
+      for (int s = leaf8_first(h.b, ls);; ++s) {
+        const std::uint32_t id = prim_slot_test(sc.prims, s, o, d, tmin, probe);
+        if (kCount) cnt.add_prim(id);
+        if (probe.word != kHitMiss) return true;
+        if (id & kLastInLeaf) break;
+      }
+    }
+    g_base = h.b.x;
+    g_mask = h.inner | (h.imask << 8);
+  }
+  return false;
+}
+
 // Brute force over the scene's slots. Ties go to the lower primitive id, which
 // reproduces the reference's index-order loop (src/core/scene.cpp:200-215).
 template <bool kCount>

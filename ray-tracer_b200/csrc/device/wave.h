@@ -38,6 +38,8 @@ struct LaunchShape {
   int extend_block = 128;  // 64, 128 or 256
   bool chained = true;     // programmatic dependent launch between the wavefront kernels
   bool mis = false;        // a job with multiple importance sampling is open (shade kernel variant)
+  int closest_tree = 8;    // closest-hit walk: 8 the compressed eight-wide tree, 2 the binary tree
+  int shadow_tree = 4;     // any-hit walk: 4 the four-wide tree, 8 the compressed eight-wide tree
 };
 
 enum class Stage { Plan, Extend, Shade, Shadow };
@@ -58,7 +60,7 @@ cudaError_t launch_accumulate(const RtgSceneDev* job_dev, std::uint64_t pixels, 
 // Direct (Whitted) integrator over one whole segment: whole samples per thread
 // (depth-first with an explicit stack). Writes each sample's radiance slot.
 cudaError_t launch_direct(const RtgSceneDev* job_dev, const DevSegment& seg, float4* radiance, WaveCounters* cnt,
-                          cudaStream_t stream);
+                          bool wide8, cudaStream_t stream);
 
 // Framebuffer means (mean_out, 3 doubles per pixel) and/or their tone-mapped
 // sRGB encoding (rgb8, 3 bytes per pixel); either output may be null.
@@ -67,9 +69,11 @@ cudaError_t launch_resolve(const double* fb_sum, const std::uint32_t* fb_count, 
 
 // Ray queries for parity tests and the ray API. rays: 2 float4 per ray
 // (origin, tmin), (direction, tmax). closest -> float4 (t, word, b1, b2) per ray.
+// tree: 8 walks the eight-wide tree; otherwise the binary tree (closest hit) or
+// the four-wide tree (any hit).
 cudaError_t launch_ray_closest(const RtgSceneDev* job_dev, const float4* rays, std::uint32_t n, float4* out,
-                               int brute, cudaStream_t stream);
+                               int brute, int tree, cudaStream_t stream);
 cudaError_t launch_ray_any(const RtgSceneDev* job_dev, const float4* rays, std::uint32_t n, std::uint32_t* out,
-                           int brute, cudaStream_t stream);
+                           int brute, int tree, cudaStream_t stream);
 
 }  // namespace rtg

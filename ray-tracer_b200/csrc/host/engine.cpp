@@ -284,12 +284,13 @@ std::vector<int> Engine::add_scenes(const std::vector<std::shared_ptr<const Comp
 
 Engine::StagedParts Engine::staged_parts(const FlatScene& f) {
   StagedParts p{};
-  const std::size_t bytes[8] = {f.nodes.size() * sizeof(DevNode), f.nodes4.size() * sizeof(DevNode4),
-                                f.prims.size() * sizeof(float4), f.slot_material.size() * sizeof(std::uint32_t),
-                                f.slot_normals.size() * sizeof(float4), f.planes.size() * sizeof(DevPlane),
-                                f.materials.size() * sizeof(DevMaterial), f.lights.size() * sizeof(DevLight)};
+  const std::size_t bytes[kSceneParts] = {f.nodes.size() * sizeof(DevNode), f.nodes4.size() * sizeof(DevNode4),
+                                          f.prims.size() * sizeof(float4), f.slot_material.size() * sizeof(std::uint32_t),
+                                          f.slot_normals.size() * sizeof(float4), f.planes.size() * sizeof(DevPlane),
+                                          f.materials.size() * sizeof(DevMaterial), f.lights.size() * sizeof(DevLight),
+                                          f.nodes8.size() * sizeof(DevNode8)};
   p.total = 0;
-  for (int k = 0; k < 8; ++k) {
+  for (int k = 0; k < kSceneParts; ++k) {
     p.bytes[k] = bytes[k];
     p.at[k] = p.total;
     p.total += (std::max<std::size_t>(bytes[k], 1) + 255) & ~std::size_t(255);
@@ -298,9 +299,10 @@ Engine::StagedParts Engine::staged_parts(const FlatScene& f) {
 }
 
 void Engine::stage_flat(const FlatScene& f, const StagedParts& p, unsigned char* dst) {
-  const void* src[8] = {f.nodes.data(), f.nodes4.data(), f.prims.data(), f.slot_material.data(),
-                        f.slot_normals.data(), f.planes.data(), f.materials.data(), f.lights.data()};
-  for (int k = 0; k < 8; ++k)
+  const void* src[kSceneParts] = {f.nodes.data(), f.nodes4.data(), f.prims.data(), f.slot_material.data(),
+                                  f.slot_normals.data(), f.planes.data(), f.materials.data(), f.lights.data(),
+                                  f.nodes8.data()};
+  for (int k = 0; k < kSceneParts; ++k)
     if (p.bytes[k]) std::memcpy(dst + p.at[k], src[k], p.bytes[k]);
 }
 
@@ -330,6 +332,8 @@ int Engine::register_flat(std::shared_ptr<const CompiledScene> scene, FlatScene 
   gs->root4 = flat.root4;
   gs->n_interior = static_cast<std::int32_t>(flat.nodes.size());
   gs->n_wide = static_cast<std::int32_t>(flat.nodes4.size());
+  gs->root8 = flat.root8;
+  gs->n_wide8 = static_cast<std::int32_t>(flat.nodes8.size());
   void* block = nullptr;
   count_allocation();
   CK(cudaMallocFromPoolAsync(&block, p.total, pool_, stream_));
@@ -344,6 +348,7 @@ int Engine::register_flat(std::shared_ptr<const CompiledScene> scene, FlatScene 
   gs->planes = static_cast<DevPlane*>(at(5));
   gs->materials = static_cast<DevMaterial*>(at(6));
   gs->lights = static_cast<DevLight*>(at(7));
+  gs->nodes8 = static_cast<DevNode8*>(at(8));
   gs->device_bytes = p.total;
   gs->slot_prim = std::move(flat.slot_prim);
   gs->bvh = scene->info.bvh;
@@ -455,12 +460,60 @@ int Engine::add_scene_gpu_bvh(std::shared_ptr<const CompiledScene> scene) {
   GpuBvhBuilder builder(build_stream_, pool_);
   const GpuBvhCounts c = builder.build(in);
 
+  // The layout in the binary tree's leaf order, in scratch first: the
+  // eight-wide tree is built from it on the host (the same function as for a
+  // host-built scene, so the bytes agree) and sets the final slot order.
+  const std::size_t scratch_bytes[7] = {std::size_t(c.interior) * sizeof(DevNode), std::size_t(c.wide) * sizeof(DevNode4),
+                                        std::size_t(n_items) * 3 * sizeof(float4), std::size_t(n_items) * sizeof(std::uint32_t),
+                                        std::size_t(n_items) * 3 * sizeof(float4), std::size_t(n_items) * sizeof(std::uint32_t),
+                                        std::size_t(n_items) * sizeof(std::uint32_t)};
+  std::size_t sat[7], scratch_total = 0;
+  for (int k = 0; k < 7; ++k) {
+    sat[k] = scratch_total;
+    scratch_total += pad(scratch_bytes[k]);
+  }
+  void* scratch = nullptr;
+  count_allocation();
+  CK(cudaMallocFromPoolAsync(&scratch, scratch_total, pool_, build_stream_));
+  struct FreeScratch {
+    void* p;
+    cudaStream_t s;
+    ~FreeScratch() { cudaFreeAsync(p, s); }
+  } free_scratch{scratch, build_stream_};
+  auto* sb = static_cast<unsigned char*>(scratch);
+  auto* s_nodes = reinterpret_cast<DevNode*>(sb + sat[0]);
+  auto* s_nodes4 = reinterpret_cast<DevNode4*>(sb + sat[1]);
+  auto* s_prims = reinterpret_cast<float4*>(sb + sat[2]);
+  auto* s_material = reinterpret_cast<std::uint32_t*>(sb + sat[3]);
+  auto* s_normals = reinterpret_cast<float4*>(sb + sat[4]);
+  auto* s_old_of = reinterpret_cast<std::uint32_t*>(sb + sat[5]);
+  auto* s_new_of = reinterpret_cast<std::uint32_t*>(sb + sat[6]);
+  builder.emit(in, s_nodes, s_nodes4, s_prims, s_material, s_normals, order);
+  std::vector<DevNode> bin_nodes(static_cast<std::size_t>(c.interior));
+  std::vector<std::uint32_t> row0_w(n_items), prim_of_slot(n_items);
+  if (c.interior)
+    CK(cudaMemcpyAsync(bin_nodes.data(), s_nodes, scratch_bytes[0], cudaMemcpyDeviceToHost, build_stream_));
+  if (n_items) {
+    // The w word of each slot's first row: its primitive id and leaf-end mark.
+    CK(cudaMemcpy2DAsync(row0_w.data(), sizeof(std::uint32_t), reinterpret_cast<const unsigned char*>(s_prims) + 12,
+                         3 * sizeof(float4), sizeof(std::uint32_t), n_items, cudaMemcpyDeviceToHost, build_stream_));
+    CK(cudaMemcpyAsync(prim_of_slot.data(), order, n_items * sizeof(std::uint32_t), cudaMemcpyDeviceToHost,
+                       build_stream_));
+  }
+  CK(cudaStreamSynchronize(build_stream_));
+  std::vector<std::uint8_t> last(n_items);
+  for (std::size_t k = 0; k < n_items; ++k) last[k] = (row0_w[k] & kLastInLeaf) ? 1 : 0;
+  const std::int32_t bin_root = n_items ? c.root : kNoRoot;
+  Wide8 w8 = build_wide8(bin_nodes.data(), bin_nodes.size(), bin_root, last.data(), n_items);
+
   // The scene's arrays, in add_flat's order, in one allocation.
-  const std::size_t part_bytes[8] = {std::size_t(c.interior) * sizeof(DevNode), std::size_t(c.wide) * sizeof(DevNode4),
-                                     std::size_t(n_items) * 3 * sizeof(float4), std::size_t(n_items) * sizeof(std::uint32_t),
-                                     std::size_t(n_items) * 3 * sizeof(float4), in_bytes[5], in_bytes[6], in_bytes[7]};
-  std::size_t at[8], total = 0;
-  for (int k = 0; k < 8; ++k) {
+  const std::size_t part_bytes[kSceneParts] = {
+      std::size_t(c.interior) * sizeof(DevNode), std::size_t(c.wide) * sizeof(DevNode4),
+      std::size_t(n_items) * 3 * sizeof(float4), std::size_t(n_items) * sizeof(std::uint32_t),
+      std::size_t(n_items) * 3 * sizeof(float4), in_bytes[5], in_bytes[6], in_bytes[7],
+      w8.nodes.size() * sizeof(DevNode8)};
+  std::size_t at[kSceneParts], total = 0;
+  for (int k = 0; k < kSceneParts; ++k) {
     at[k] = total;
     total += pad(part_bytes[k]);
   }
@@ -486,16 +539,28 @@ int Engine::add_scene_gpu_bvh(std::shared_ptr<const CompiledScene> scene) {
   gs->planes = reinterpret_cast<DevPlane*>(dst + at[5]);
   gs->materials = reinterpret_cast<DevMaterial*>(dst + at[6]);
   gs->lights = reinterpret_cast<DevLight*>(dst + at[7]);
-  builder.emit(in, gs->nodes, gs->nodes4, gs->prims, gs->slot_material, gs->slot_normals, order);
+  gs->nodes8 = reinterpret_cast<DevNode8*>(dst + at[8]);
+  for (int k : {0, 1})
+    if (part_bytes[k])
+      CK(cudaMemcpyAsync(dst + at[k], sb + sat[k], part_bytes[k], cudaMemcpyDeviceToDevice, build_stream_));
+  if (n_items) {
+    CK(cudaMemcpyAsync(s_old_of, w8.old_of.data(), n_items * sizeof(std::uint32_t), cudaMemcpyHostToDevice, build_stream_));
+    CK(cudaMemcpyAsync(s_new_of, w8.new_of.data(), n_items * sizeof(std::uint32_t), cudaMemcpyHostToDevice, build_stream_));
+  }
+  if (part_bytes[8])
+    CK(cudaMemcpyAsync(gs->nodes8, w8.nodes.data(), part_bytes[8], cudaMemcpyHostToDevice, build_stream_));
+  CK(apply_slot_order(s_old_of, s_new_of, n_items, s_prims, s_normals, s_material, gs->prims, gs->slot_normals,
+                      gs->slot_material, gs->nodes, c.interior, gs->nodes4, c.wide, build_stream_));
   for (int k = 5; k < 8; ++k)
     if (part_bytes[k]) CK(cudaMemcpyAsync(dst + at[k], dev_in + in_at[k], part_bytes[k], cudaMemcpyDeviceToDevice, build_stream_));
   gs->slot_prim.resize(n_items);
-  if (n_items)
-    CK(cudaMemcpyAsync(gs->slot_prim.data(), order, n_items * sizeof(std::uint32_t), cudaMemcpyDeviceToHost, build_stream_));
+  for (std::size_t k = 0; k < n_items; ++k) gs->slot_prim[k] = prim_of_slot[w8.old_of[k]];
   CK(cudaStreamSynchronize(build_stream_));
 
-  gs->root = n_items ? c.root : kNoRoot;
-  gs->root4 = n_items ? c.root4 : kNoRoot;
+  gs->root = n_items ? remap_link(c.root, w8.new_of) : kNoRoot;
+  gs->root4 = n_items ? remap_link(c.root4, w8.new_of) : kNoRoot;
+  gs->root8 = w8.root;
+  gs->n_wide8 = static_cast<std::int32_t>(w8.nodes.size());
   gs->n_slots = static_cast<std::int32_t>(n_items);
   gs->n_interior = c.interior;
   gs->n_wide = c.wide;
@@ -620,6 +685,8 @@ RtgSceneDev Engine::job_descriptor(const GpuScene& sc, const RenderSettings& s, 
   d.root = sc.root;
   d.nodes4 = sc.nodes4;
   d.root4 = sc.root4;
+  d.nodes8 = sc.nodes8;
+  d.root8 = sc.root8;
   d.n_planes = sc.n_planes;
   d.n_lights = sc.n_lights;
   d.slot_begin = 0;
@@ -794,7 +861,7 @@ bool Engine::run_direct_pass(Job& j) {
   d.sample_base = at;
   const bool timed = cfg_.time_kernels;
   if (timed) CK(cudaEventRecord(W.tev[8], stream_));
-  CK(launch_direct(W.jobs_dev + j.desc_slot, d, W.wb.radiance, W.wb.cnt, stream_));
+  CK(launch_direct(W.jobs_dev + j.desc_slot, d, W.wb.radiance, W.wb.cnt, cfg_.shape.closest_tree == 8, stream_));
   if (timed) CK(cudaEventRecord(W.tev[9], stream_));
   CK(launch_accumulate(W.jobs_dev + j.desc_slot, j.pixels, d, W.wb.radiance, stream_));
   stats_.kernel_launches += 2;
@@ -1297,7 +1364,7 @@ void Engine::trace_closest(int scene_id, const float* rays, std::uint64_t n, boo
   float4* out = dev_alloc<float4>(n);
   CK(cudaMemcpyAsync(dd, &d, sizeof(d), cudaMemcpyHostToDevice, stream_));
   CK(cudaMemcpyAsync(in, rays, n * 8 * sizeof(float), cudaMemcpyHostToDevice, stream_));
-  CK(launch_ray_closest(dd, in, static_cast<std::uint32_t>(n), out, brute ? 1 : 0, stream_));
+  CK(launch_ray_closest(dd, in, static_cast<std::uint32_t>(n), out, brute ? 1 : 0, cfg_.shape.closest_tree, stream_));
   std::vector<float4> host(n);
   CK(cudaMemcpyAsync(host.data(), out, n * sizeof(float4), cudaMemcpyDeviceToHost, stream_));
   CK(cudaStreamSynchronize(stream_));
@@ -1332,7 +1399,7 @@ void Engine::trace_any(int scene_id, const float* rays, std::uint64_t n, bool br
   std::uint32_t* out = dev_alloc<std::uint32_t>(n);
   CK(cudaMemcpyAsync(dd, &d, sizeof(d), cudaMemcpyHostToDevice, stream_));
   CK(cudaMemcpyAsync(in, rays, n * 8 * sizeof(float), cudaMemcpyHostToDevice, stream_));
-  CK(launch_ray_any(dd, in, static_cast<std::uint32_t>(n), out, brute ? 1 : 0, stream_));
+  CK(launch_ray_any(dd, in, static_cast<std::uint32_t>(n), out, brute ? 1 : 0, cfg_.shape.shadow_tree, stream_));
   std::vector<std::uint32_t> host(n);
   CK(cudaMemcpyAsync(host.data(), out, n * sizeof(std::uint32_t), cudaMemcpyDeviceToHost, stream_));
   CK(cudaStreamSynchronize(stream_));

@@ -70,11 +70,13 @@ struct GpuScene {
   std::vector<std::uint32_t> slot_prim;  // slot -> primitive id (ray API)
   std::int32_t root = kNoRoot;
   std::int32_t n_slots = 0, n_planes = 0, n_lights = 0;
-  std::int32_t n_interior = 0, n_wide = 0;  // DevNode / DevNode4 records
+  std::int32_t n_interior = 0, n_wide = 0, n_wide8 = 0;  // DevNode / DevNode4 / DevNode8 records
   void* block = nullptr;       // one device allocation holding the arrays below
   DevNode* nodes = nullptr;
   DevNode4* nodes4 = nullptr;  // four-wide copy of the tree (any-hit queries)
   std::int32_t root4 = kNoRoot;
+  DevNode8* nodes8 = nullptr;  // compressed eight-wide copy (closest-hit queries)
+  std::int32_t root8 = kNoRoot;
   float4* prims = nullptr;
   std::uint32_t* slot_material = nullptr;
   float4* slot_normals = nullptr;
@@ -243,9 +245,10 @@ class Engine {
   int add_flat(std::shared_ptr<const CompiledScene> scene, FlatScene flat);
   // Byte offsets of a flattened scene's arrays in its device block (and in its
   // pinned staging copy): nodes, nodes4, prims, slot_material, slot_normals,
-  // planes, materials, lights, each 256-byte aligned.
+  // planes, materials, lights, nodes8, each 256-byte aligned.
+  static constexpr int kSceneParts = 9;
   struct StagedParts {
-    std::size_t at[8], bytes[8], total;
+    std::size_t at[kSceneParts], bytes[kSceneParts], total;
   };
   static StagedParts staged_parts(const FlatScene& f);
   static void stage_flat(const FlatScene& f, const StagedParts& p, unsigned char* dst);

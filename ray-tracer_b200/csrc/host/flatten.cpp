@@ -311,9 +311,51 @@ FlatScene flatten(const CompiledScene& s) {
   });
   if (!bvh.nodes.empty()) f.root = link_of(0);
   build_wide(bvh, fbox, f);
+  add_wide8(f);
 
   flatten_tables(s, f);
   return f;
+}
+
+void add_wide8(FlatScene& f) {
+  const std::size_t nslots = f.slot_prim.size();
+  std::vector<std::uint8_t> last(nslots);
+  for (std::size_t k = 0; k < nslots; ++k) last[k] = (bits_of(f.prims[3 * k].w) & kLastInLeaf) ? 1 : 0;
+  Wide8 w = build_wide8(f.nodes.data(), f.nodes.size(), f.root, last.data(), nslots);
+  f.nodes8 = std::move(w.nodes);
+  f.root8 = w.root;
+  bool identity = true;
+  for (std::size_t k = 0; k < nslots && identity; ++k) identity = w.old_of[k] == k;
+  if (identity) return;
+  std::vector<float4> prims(f.prims.size()), normals(f.slot_normals.size());
+  std::vector<std::uint32_t> material(nslots), prim(nslots);
+  parallel_chunks(nslots, [&](std::size_t k0, std::size_t k1) {
+    for (std::size_t k = k0; k < k1; ++k) {
+      const std::size_t o = w.old_of[k];
+      for (int r = 0; r < 3; ++r) {
+        prims[3 * k + r] = f.prims[3 * o + r];
+        normals[3 * k + r] = f.slot_normals[3 * o + r];
+      }
+      material[k] = f.slot_material[o];
+      prim[k] = f.slot_prim[o];
+    }
+  });
+  f.prims = std::move(prims);
+  f.slot_normals = std::move(normals);
+  f.slot_material = std::move(material);
+  f.slot_prim = std::move(prim);
+  for (DevNode& n : f.nodes) {
+    n.link.x = remap_link(n.link.x, w.new_of);
+    n.link.y = remap_link(n.link.y, w.new_of);
+  }
+  for (DevNode4& n : f.nodes4) {
+    n.link.x = remap_link(n.link.x, w.new_of);
+    n.link.y = remap_link(n.link.y, w.new_of);
+    n.link.z = remap_link(n.link.z, w.new_of);
+    n.link.w = remap_link(n.link.w, w.new_of);
+  }
+  f.root = remap_link(f.root, w.new_of);
+  f.root4 = remap_link(f.root4, w.new_of);
 }
 
 void describe(const CompiledScene& s, const RenderSettings& r, RtgSceneDev& d) {
@@ -338,17 +380,6 @@ void describe(const CompiledScene& s, const RenderSettings& r, RtgSceneDev& d) {
   d.bg_bottom = f3h(s.background.bottom);
   d.bg_intensity = float(s.background.intensity);
   d.bg_solid = s.background.kind == Background::Kind::Solid ? 1 : 0;
-}
-
-void rebase(FlatScene& f, std::int32_t node_offset, std::int32_t slot_offset, std::uint32_t material_offset) {
-  auto shift = [&](std::int32_t link) { return link >= 0 ? link + node_offset : ~(~link + slot_offset); };
-  for (DevNode& n : f.nodes) {
-    n.link.x = shift(n.link.x);
-    n.link.y = shift(n.link.y);
-  }
-  if (f.root != kNoRoot) f.root = shift(f.root);
-  for (std::uint32_t& m : f.slot_material) m = ((m & 0x7FFFFFFFu) + material_offset) | (m & 0x80000000u);
-  for (DevPlane& p : f.planes) p.point.w = float_of(bits_of(p.point.w) + material_offset);
 }
 
 }  // namespace rtg

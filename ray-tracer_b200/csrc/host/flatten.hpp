@@ -3,14 +3,17 @@
 //
 // The node array keeps the host tree's topology: every interior node becomes one
 // DevNode holding both children's boxes, rounded outward to fp32 so the boxes
-// still enclose what they enclosed in double. Primitive slots follow the tree's
-// leaf order so a leaf's primitives are contiguous (one streaming read per leaf);
-// the last slot of each leaf carries kLastInLeaf, so leaves need no count.
+// still enclose what they enclosed in double. A leaf's primitives occupy
+// consecutive slots (one streaming read per leaf); the last slot of each leaf
+// carries kLastInLeaf, so leaves need no count. Leaves are placed in the order the
+// compressed eight-wide tree needs (wide8.hpp): the leaf children of each of its
+// nodes side by side.
 #include <cstdint>
 #include <vector>
 
 #include "device/layout.h"
 #include "host/compiled_scene.hpp"
+#include "host/wide8.hpp"
 
 namespace rtg {
 
@@ -30,9 +33,17 @@ struct FlatScene {
   std::vector<DevNode4> nodes4;
   std::int32_t root4 = kNoRoot;
   int depth4 = 0;
+  // The same tree as compressed eight-child nodes (closest-hit queries); the
+  // slot arrays above are in the order it needs.
+  std::vector<DevNode8> nodes8;
+  std::int32_t root8 = kNoRoot;
 };
 
 FlatScene flatten(const CompiledScene& s);
+
+// Builds the eight-wide tree from f.nodes / f.root and moves every per-slot array
+// of f (and the binary and four-wide trees' leaf links) to its slot order.
+void add_wide8(FlatScene& f);
 
 // One primitive's device records, indexed by primitive rather than slot: its three
 // slot rows (id bits set, no last-in-leaf bit), its three vertex normals (zero
@@ -46,8 +57,5 @@ void flatten_tables(const CompiledScene& s, FlatScene& f);
 // Camera (set up for r's resolution), settings and background of a descriptor;
 // pointers and pass fields are filled in by the engine.
 void describe(const CompiledScene& s, const RenderSettings& r, RtgSceneDev& d);
-
-// Shift a flattened scene's indices by pool offsets (nodes, slots, materials).
-void rebase(FlatScene& f, std::int32_t node_offset, std::int32_t slot_offset, std::uint32_t material_offset);
 
 }  // namespace rtg

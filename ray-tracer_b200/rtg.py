@@ -104,7 +104,8 @@ class _Tuning(C.Structure):
         ("extend_blocks", C.c_int32), ("shade_blocks", C.c_int32), ("shadow_blocks", C.c_int32),
         ("time_kernels", C.c_int32), ("count_traversal", C.c_int32), ("backlog_pools", C.c_uint32),
         ("chained", C.c_uint32), ("serve_budget_bytes", C.c_uint64), ("serve_reserve_bytes", C.c_uint64),
-        ("refine_hits", C.c_int32), ("reserved", C.c_int32),
+        ("refine_hits", C.c_int32), ("closest_tree", C.c_int32), ("shadow_tree", C.c_int32),
+        ("reserved", C.c_int32),
     ]
 
 
@@ -133,6 +134,7 @@ _SIGNATURES = {
     "rtg_scene_upload_batch": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_void_p), C.POINTER(C.c_int32)]),
     "rtg_scene_upload_gpu_bvh": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int32)]),
     "rtg_scene_layout": (C.c_int64, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_uint64]),
+    "rtg_host_scene_layout": (C.c_int64, [C.c_void_p, C.c_int32, C.c_void_p, C.c_uint64]),
     "rtg_scene_settings": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(_Settings)]),
     "rtg_scene_get_info": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(_SceneInfo)]),
     "rtg_scene_release": (C.c_int, [C.c_void_p, C.c_int32]),
@@ -324,6 +326,17 @@ class HostScene:
             "bvh_sah_cost": v.bvh_sah_cost,
         }
 
+    def device_layout(self, part: str) -> np.ndarray:
+        """One part of the device layout this scene gets at upload, computed on
+        the host (no GPU); records as rows of raw words."""
+        code, dtype, width = LAYOUT_PARTS[part]
+        n = lib().rtg_host_scene_layout(self._h, code, None, 0)
+        if n < 0:
+            raise RtgError(int(n), f"no host layout for part {part}")
+        out = np.zeros(n // 4, dtype=dtype)
+        lib().rtg_host_scene_layout(self._h, code, out.ctypes.data_as(C.c_void_p), n)
+        return out.reshape(-1, width)
+
 
 COMPILE_DEFER_BVH = 1
 COMPILE_AUTO_BVH = 2
@@ -332,7 +345,7 @@ LAYOUT_PARTS = {
     "nodes": (0, np.float32, 16), "nodes4": (1, np.float32, 32), "prims": (2, np.float32, 12),
     "slot_material": (3, np.uint32, 1), "slot_normals": (4, np.float32, 12), "planes": (5, np.float32, 8),
     "materials": (6, np.float32, 16), "lights": (7, np.float32, 20), "slot_prim": (8, np.uint32, 1),
-    "roots": (9, np.int32, 4),
+    "roots": (9, np.int32, 5), "nodes8": (10, np.uint32, 20),
 }
 
 

@@ -21,7 +21,8 @@ import workloads
 
 pytestmark = pytest.mark.gpu
 
-PARTS = ["nodes", "nodes4", "prims", "slot_material", "slot_normals", "planes", "materials", "lights", "slot_prim"]
+PARTS = ["nodes", "nodes4", "nodes8", "prims", "slot_material", "slot_normals", "planes", "materials", "lights",
+         "slot_prim"]
 
 
 def _scene(objects, planes=()):
@@ -102,7 +103,7 @@ def _compare(ctx, host):
     try:
         ra, rb = ctx.scene_layout(a, "roots")[0], ctx.scene_layout(b, "roots")[0]
         assert ra[3] == 0 and rb[3] == 1
-        assert ra[:3].tolist() == rb[:3].tolist()
+        assert ra[:3].tolist() == rb[:3].tolist() and ra[4] == rb[4]
         for part in PARTS:
             x, y = ctx.scene_layout(a, part), ctx.scene_layout(b, part)
             assert x.shape == y.shape, (part, x.shape, y.shape)
