@@ -80,8 +80,11 @@ constexpr int kWide8StackDepth = 64;
 constexpr int kWideStackDepth = 3 * 61 + 1;
 
 // Primitive slot (leaf order): three float4.
-//  triangle: p0 = (v0, id), p1 = (e1 = v1 - v0, 0), p2 = (e2 = v2 - v0, 0)
-//  sphere:   p0 = (centre, id | kSphereBit), p1 = (radius, radius^2, 0, 0), p2 = 0
+//  triangle: p0 = (v0, id), p1 = (e1 = v1 - v0, k), p2 = (e2 = v2 - v0, 0), where
+//            k = dot(v0 - fp32(v0), e1 x e2) in double: the plane offset the
+//            rounding of v0 lost (the distance test subtracts it)
+//  sphere:   p0 = (centre, id | kSphereBit), p1 = (radius, radius^2, 0, 0),
+//            p2 = (centre - fp32(centre), 0): the rounding residual of the centre
 // `id` is the scene-local primitive id (the reference's hit id), stored as bits.
 constexpr std::uint32_t kSphereBit = 0x80000000u;
 constexpr std::uint32_t kLastInLeaf = 0x40000000u;  // set on the last primitive slot of a leaf
@@ -113,7 +116,7 @@ struct alignas(16) DevLight {
 
 struct alignas(16) DevPlane {
   float4 point;   // xyz, w = material index (bits)
-  float4 normal;  // unit xyz
+  float4 normal;  // unit xyz, w = dot(point - fp32(point), normal): the offset rounding the point lost
 };
 
 // One scene as the kernels see it. Pointers are device addresses.

@@ -236,7 +236,7 @@ __device__ __forceinline__ LightSample sample_light(const DevLight* __restrict__
     const float3 axis = oc * rsqrtf(d2);
     out.wi = Frame(axis).to_world(uniform_cone(rng, one_minus_cos));
     float t;
-    if (!sphere_test(p, out.wi, c, r, 0.f, __int_as_float(0x7f800000), t)) return out;  // grazing miss
+    if (!sphere_test(p, out.wi, c, f3(0.f, 0.f, 0.f), r, 0.f, __int_as_float(0x7f800000), t)) return out;  // grazing miss
     out.dist = t;
     out.li_over_pdf = emit * (2.f * kPiF * one_minus_cos);
     out.pdf = 1.f / (2.f * kPiF * one_minus_cos);

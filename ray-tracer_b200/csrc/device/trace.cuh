@@ -81,8 +81,12 @@ __device__ __forceinline__ void node_boxes(const DevNode* __restrict__ node, con
 constexpr float kEdgeSlack = 1e-6f;
 
 // Möller-Trumbore, two-sided (include/raytracer/geometry/shapes.hpp:110-127).
-__device__ __forceinline__ bool tri_test(float3 o, float3 d, float3 v0, float3 e1, float3 e2, float tmin, float tmax,
-                                         float& t, float& b1, float& b2) {
+// `k` is dot(r, e1 x e2) for the residual r that rounding v0 to fp32 lost: the
+// distance to the plane through the double-precision v0 is (dot(e2, qv) - k) / det.
+// For hits close to the ray origin that rounding, not the arithmetic, dominates
+// the error of t.
+__device__ __forceinline__ bool tri_test(float3 o, float3 d, float3 v0, float3 e1, float3 e2, float k, float tmin,
+                                         float tmax, float& t, float& b1, float& b2) {
   const float3 pv = cross3(d, e2);
   const float det = dot3(e1, pv);
   if (fabsf(det) < 1e-14f) return false;
@@ -93,7 +97,7 @@ __device__ __forceinline__ bool tri_test(float3 o, float3 d, float3 v0, float3 e
   const float3 qv = cross3(tv, e1);
   const float v = dot3(d, qv) * inv_det;
   if (v < -kEdgeSlack || u + v > 1.f + kEdgeSlack) return false;
-  const float tt = dot3(e2, qv) * inv_det;
+  const float tt = (dot3(e2, qv) - k) * inv_det;
   if (!(tmin < tt && tt < tmax)) return false;
   t = tt;
   b1 = u;
@@ -103,10 +107,12 @@ __device__ __forceinline__ bool tri_test(float3 o, float3 d, float3 v0, float3 e
 
 // Ray-sphere with the Haines et al. precision fixes ("Precision Improvements for
 // Ray/Sphere Intersection", Ray Tracing Gems ch. 7), as the reference's
-// Sphere::hit_t (include/raytracer/geometry/shapes.hpp:25-46).
-__device__ __forceinline__ bool sphere_test(float3 o, float3 d, float3 c, float radius, float tmin, float tmax,
-                                            float& t) {
-  const float3 oc = c - o;
+// Sphere::hit_t (include/raytracer/geometry/shapes.hpp:25-46). `rc` is what
+// rounding the centre to fp32 lost; adding it after the subtraction gives the
+// offset to the double-precision centre.
+__device__ __forceinline__ bool sphere_test(float3 o, float3 d, float3 c, float3 rc, float radius, float tmin,
+                                            float tmax, float& t) {
+  const float3 oc = (c - o) + rc;
   const float a = dot3(d, d);
   if (a == 0.f) return false;
   const float h = dot3(d, oc);
@@ -127,11 +133,12 @@ __device__ __forceinline__ bool sphere_test(float3 o, float3 d, float3 c, float 
   return true;
 }
 
+// normal.w holds the plane offset that rounding the point to fp32 lost.
 __device__ __forceinline__ bool plane_test(const DevPlane& pl, float3 o, float3 d, float tmin, float tmax, float& t) {
   const float3 n = f3(pl.normal);
   const float denom = dot3(n, d);
   if (fabsf(denom) < 1e-12f) return false;
-  const float tt = dot3(f3(pl.point) - o, n) / denom;
+  const float tt = (dot3(f3(pl.point) - o, n) + pl.normal.w) / denom;
   if (!(tmin < tt && tt < tmax)) return false;
   t = tt;
   return true;
@@ -149,9 +156,9 @@ __device__ __forceinline__ std::uint32_t prim_slot_test(const float4* __restrict
   float t, b1 = 0.f, b2 = 0.f;
   bool hit;
   if (id & kSphereBit) {
-    hit = sphere_test(o, d, f3(p0), p1.x, tmin, best.t, t);
+    hit = sphere_test(o, d, f3(p0), f3(p2), p1.x, tmin, best.t, t);
   } else {
-    hit = tri_test(o, d, f3(p0), f3(p1), f3(p2), tmin, best.t, t, b1, b2);
+    hit = tri_test(o, d, f3(p0), f3(p1), f3(p2), p1.w, tmin, best.t, t, b1, b2);
   }
   if (hit) {
     best.t = t;
@@ -523,11 +530,11 @@ __device__ __forceinline__ RayHit closest_brute(const RtgSceneDev& sc, float3 o,
     bool hit;
     // Accept t == current best too, so a lower id can take over an exact tie.
     const float limit = have ? __int_as_float(__float_as_int(tb) + 1) : tb;
+    const float4 p2 = __ldg(&sc.prims[3 * slot + 2]);
     if (id & kSphereBit) {
-      hit = sphere_test(o, d, f3(p0), p1.x, tmin, limit, t);
+      hit = sphere_test(o, d, f3(p0), f3(p2), p1.x, tmin, limit, t);
     } else {
-      const float4 p2 = __ldg(&sc.prims[3 * slot + 2]);
-      hit = tri_test(o, d, f3(p0), f3(p1), f3(p2), tmin, limit, t, b1, b2);
+      hit = tri_test(o, d, f3(p0), f3(p1), f3(p2), p1.w, tmin, limit, t, b1, b2);
     }
     if (!hit) continue;
     const std::uint32_t pid = id & kIdMask;

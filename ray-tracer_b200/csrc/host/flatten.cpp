@@ -201,15 +201,23 @@ void build_wide(const BinaryBvh& bvh, const std::vector<FBox>& fbox, FlatScene& 
 void slot_record(const Prim& p, std::uint32_t id, float4* rows, float4* normals, std::uint32_t& material) {
   std::uint32_t word = id;
   normals[0] = normals[1] = normals[2] = make_float4(0.f, 0.f, 0.f, 0.f);
+  // What rounding the position to fp32 lost, kept so the distance can be
+  // corrected where it is computed (the stored fp32 values are as before).
+  const D3 a32{double(float(p.a.x)), double(float(p.a.y)), double(float(p.a.z))};
+  const D3 residual = p.a - a32;
   if (p.kind == Prim::kSphere) {
     word |= kSphereBit;
     rows[0] = f4(p.a, float_of(word));
     rows[1] = make_float4(float(p.b.x), float(p.b.x * p.b.x), 0.f, 0.f);
-    rows[2] = make_float4(0.f, 0.f, 0.f, 0.f);
+    rows[2] = f4(residual);
   } else {
+    // The triangle's plane offset that v0's rounding lost: t gains
+    // -dot(residual, e1 x e2) / det, with the edges as stored.
+    const float4 e1 = f4(p.b - p.a), e2 = f4(p.c - p.a);
+    const D3 n = cross(D3{e1.x, e1.y, e1.z}, D3{e2.x, e2.y, e2.z});
     rows[0] = f4(p.a, float_of(word));
-    rows[1] = f4(p.b - p.a);
-    rows[2] = f4(p.c - p.a);
+    rows[1] = make_float4(e1.x, e1.y, e1.z, float(dot(residual, n)));
+    rows[2] = e2;
     if (p.smooth) {
       normals[0] = f4(p.n0);
       normals[1] = f4(p.n1);
@@ -227,6 +235,9 @@ void flatten_tables(const CompiledScene& s, FlatScene& f) {
     DevPlane dp;
     dp.point = f4(pl.point, float_of(pl.material));
     dp.normal = f4(pl.normal);
+    // The plane offset its point's rounding lost, along the stored normal.
+    const D3 p32{double(float(pl.point.x)), double(float(pl.point.y)), double(float(pl.point.z))};
+    dp.normal.w = float(dot(pl.point - p32, D3{dp.normal.x, dp.normal.y, dp.normal.z}));
     f.planes.push_back(dp);
   }
   for (const Material& m : s.materials) f.materials.push_back(material_record(m));

@@ -21,12 +21,12 @@ CONFIGS = {"cornell": workloads.cornell, "spheres": workloads.sphere_field, "mes
 # primitive's t in double; "fp32" reports the traversal's own t, the value the
 # renderer's closest-hit stage hands to shading.
 MODES = ["refined", "fp32"]
-# Share of hits whose fp32 t is within 1e-5 of the reference's double t. With
-# world coordinates stored in fp32, a hit at distance t from an origin at |o|
-# carries an error of about 2^-24 |o| / t, so short hits far from the world
-# origin miss 1e-5: the random-origin sets of the 555-unit Cornell room and the
-# sphere field keep about 99.8%. The mesh scene's 1M-ray set meets 99.99%.
-FP32_T_SHARE = {"cornell": 0.997, "spheres": 0.997, "mesh": 0.9999}
+# Share of hits whose fp32 t is within 1e-5 of the reference's double t. Each
+# primitive slot carries the residual its fp32 position lost (triangle plane
+# offset, sphere centre, plane point), which the distance test adds back, so the
+# remaining error is the fp32 arithmetic. In the 555-unit Cornell room that still
+# leaves a few short hits just above 1e-5.
+FP32_T_SHARE = {"cornell": 0.999, "spheres": 0.9999, "mesh": 0.9999}
 
 
 @pytest.fixture
