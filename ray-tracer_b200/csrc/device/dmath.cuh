@@ -94,13 +94,6 @@ struct Pcg {
     const std::uint64_t h = mix64(seed ^ mix64(pixel ^ mix64(sample)));
     return seeded(h, mix64(h));
   }
-  // The increment of for_sample's stream alone (it never changes as the stream
-  // advances), so a path's state can be stored without it.
-  __device__ static __forceinline__ std::uint64_t stream_inc(std::uint64_t seed, std::uint64_t pixel,
-                                                             std::uint64_t sample) {
-    const std::uint64_t h = mix64(seed ^ mix64(pixel ^ mix64(sample)));
-    return (mix64(h) << 1u) | 1u;
-  }
 };
 
 // ---------------------------------------------------------------------------

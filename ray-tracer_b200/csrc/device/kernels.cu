@@ -248,7 +248,8 @@ __global__ void __launch_bounds__(kBlock) k_extend(WaveBuffers wb, int par) {
       // Camera rays count as a specular bounce (no NEE double-count guard).
       __stcs(&B[i], make_float4(d.x, d.y, d.z, __uint_as_float(kFlagSpecular | (job << kMetaSceneShift))));
       __stcs(&wb.st_c[par][i], make_float4(1.f, 1.f, 1.f, __uint_as_float(seg)));
-      __stcs(&wb.st_d[par][i], make_uint2(static_cast<std::uint32_t>(cs.rng.state), static_cast<std::uint32_t>(cs.rng.state >> 32)));
+      __stcs(&wb.st_d[par][i], make_uint4(static_cast<std::uint32_t>(cs.rng.state), static_cast<std::uint32_t>(cs.rng.state >> 32),
+                                   static_cast<std::uint32_t>(cs.rng.inc), static_cast<std::uint32_t>(cs.rng.inc >> 32)));
       wb.radiance[cs.sample] = make_float4(0.f, 0.f, 0.f, 0.f);
     } else {
       const float4 a = __ldcs(&A[i]);
@@ -286,7 +287,7 @@ __global__ void __launch_bounds__(kBlock, 1024 / kBlock) k_shade(WaveBuffers wb,
   const float4* const A = wb.st_a[par];
   const float4* const B = wb.st_b[par];
   const float4* const Cc = wb.st_c[par];
-  const uint2* const D = wb.st_d[par];
+  const uint4* const D = wb.st_d[par];
   std::uint64_t rr_killed = 0;
   // Uniform work per path: blocks stride over the hits in order (no fetch atomics).
   for (std::uint32_t base = blockIdx.x * kBlock; base < n; base += gridDim.x * kBlock) {
@@ -299,7 +300,7 @@ __global__ void __launch_bounds__(kBlock, 1024 / kBlock) k_shade(WaveBuffers wb,
     Pcg rng{0, 0};
     if (i < n) {
       const float4 a = __ldcs(&A[i]), b = __ldcs(&B[i]), c = __ldcs(&Cc[i]), hv = __ldcs(&wb.hits[i]);
-      const uint2 r = __ldcs(&D[i]);
+      const uint4 r = __ldcs(&D[i]);
       const float3 o = f3(a), d = f3(b);
       sample = __float_as_uint(a.w);
       const std::uint32_t meta = __float_as_uint(b.w);
@@ -308,16 +309,9 @@ __global__ void __launch_bounds__(kBlock, 1024 / kBlock) k_shade(WaveBuffers wb,
       job = meta >> kMetaSceneShift;
       seg = __float_as_uint(c.w);
       beta = f3(c);
-      const RtgSceneDev& J = wb.jobs[job];
       rng.state = ld_u64(r.x, r.y);
-      {
-        // The stream's increment from (seed, pixel, sample): the radiance slot is
-        // sample_base + pixel * pass_spp + (s - pass_s0) within the segment.
-        const DevSegment& S = wb.segs[seg];
-        const std::uint32_t local = sample - static_cast<std::uint32_t>(S.sample_base);
-        const std::uint32_t pixel = local / S.pass_spp;
-        rng.inc = Pcg::stream_inc(J.seed, pixel, S.pass_s0 + (local - pixel * S.pass_spp));
-      }
+      rng.inc = ld_u64(r.z, r.w);
+      const RtgSceneDev& J = wb.jobs[job];
       const RayHit h{hv.x, __float_as_uint(hv.y), hv.z, hv.w};
       float4* const slot = &wb.radiance[sample];
       if (J.integrator == 2) {
@@ -424,7 +418,8 @@ __global__ void __launch_bounds__(kBlock, 1024 / kBlock) k_shade(WaveBuffers wb,
       __stcs(&wb.st_a[par ^ 1][cpos], make_float4(o_next.x, o_next.y, o_next.z, __uint_as_float(sample)));
       __stcs(&wb.st_b[par ^ 1][cpos], make_float4(d_next.x, d_next.y, d_next.z, __uint_as_float(meta_next)));
       __stcs(&wb.st_c[par ^ 1][cpos], make_float4(beta.x, beta.y, beta.z, __uint_as_float(seg)));
-      __stcs(&wb.st_d[par ^ 1][cpos], make_uint2(static_cast<std::uint32_t>(rng.state), static_cast<std::uint32_t>(rng.state >> 32)));
+      __stcs(&wb.st_d[par ^ 1][cpos], make_uint4(static_cast<std::uint32_t>(rng.state), static_cast<std::uint32_t>(rng.state >> 32),
+                                          static_cast<std::uint32_t>(rng.inc), static_cast<std::uint32_t>(rng.inc >> 32)));
       if (kMis && pdf_next >= 0.f) __stcs(&wb.st_e[par ^ 1][cpos], pdf_next);
     }
     if (shadow) {

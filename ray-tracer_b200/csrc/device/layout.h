@@ -209,10 +209,9 @@ struct alignas(16) GenPlan {
   std::uint64_t start[kMaxGen];
 };
 
-// Path-state stream record, three float4 and one uint2 (SoA): one element per live path.
+// Path-state stream record, four float4 (SoA): one element per live path.
 //  a = (origin, sample id bits)         b = (direction, meta bits)
-//  c = (throughput, segment slot bits)  d = PCG32 state (lo, hi); the stream's
-//  increment is a function of (seed, pixel, sample) and is recomputed, not stored
+//  c = (throughput, segment slot bits)  d = PCG32 state (lo, hi) and increment (lo, hi)
 // meta: depth (bits 0-11) | flags (bits 12-15) | job (bits 16-31)
 constexpr std::uint32_t kFlagSpecular = 1u << 12;
 constexpr std::uint32_t kMetaDepthMask = 0xFFFu;

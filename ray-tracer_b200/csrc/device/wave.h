@@ -15,7 +15,7 @@ struct WaveBuffers {
   float4* st_a[2];
   float4* st_b[2];
   float4* st_c[2];
-  uint2* st_d[2];  // PCG32 state (its increment is recomputed from the sample)
+  uint4* st_d[2];
   float* st_e[2];  // pdf of the direction a diffuse bounce sampled (read only by MIS jobs)
   float4* hits;
   float4* sh_a;

@@ -607,7 +607,7 @@ void Engine::ensure_wave() {
     b.st_a[i] = dev_alloc<float4>(P);
     b.st_b[i] = dev_alloc<float4>(P);
     b.st_c[i] = dev_alloc<float4>(P);
-    b.st_d[i] = dev_alloc<uint2>(P);
+    b.st_d[i] = dev_alloc<uint4>(P);
     b.st_e[i] = dev_alloc<float>(P);
   }
   b.hits = dev_alloc<float4>(P);
