@@ -306,7 +306,7 @@ typedef struct rtg_tuning {
   int32_t refine_hits;       /* ray queries report t recomputed in double for the winning primitive
                               * (default 1); 0: the fp32 traversal's own t, the value the renderer's
                               * closest-hit stage hands to shading */
-  int32_t closest_tree;      /* closest-hit walk: 8 the compressed eight-wide tree (default), 2 the binary tree */
+  int32_t closest_tree;      /* closest-hit walk: 2 the binary tree (default), 8 the compressed eight-wide tree */
   int32_t shadow_tree;       /* any-hit walk: 4 the four-wide tree (default), 8 the compressed eight-wide tree */
   int32_t reserved;
 } rtg_tuning;

@@ -38,7 +38,7 @@ struct LaunchShape {
   int extend_block = 128;  // 64, 128 or 256
   bool chained = true;     // programmatic dependent launch between the wavefront kernels
   bool mis = false;        // a job with multiple importance sampling is open (shade kernel variant)
-  int closest_tree = 8;    // closest-hit walk: 8 the compressed eight-wide tree, 2 the binary tree
+  int closest_tree = 2;    // closest-hit walk: 2 the binary tree, 8 the compressed eight-wide tree
   int shadow_tree = 4;     // any-hit walk: 4 the four-wide tree, 8 the compressed eight-wide tree
 };
 

@@ -344,3 +344,20 @@ def test_invalid_samples_are_counted_and_recorded_black(ctx, kind, integ):
     # The same scene with a finite emission: no invalid sample, every pixel lit.
     prog, s, q, n, stats = render(ctx, _invalid_scene(kind, 1e30))
     assert stats["invalid_samples"] == 0 and np.isfinite(s).all() and (s[..., 0] > 0).all()
+
+
+def test_eight_wide_walk_renders_the_same_samples(ctx):
+    """The wavefront with the compressed eight-wide tree for closest and any hit
+    gives the default walk's samples: the walks differ only in which of two
+    primitives at exactly the same distance they report."""
+    scene = workloads.mesh_stress(width=32, height=32, spp=1)
+    opts = rtg.RenderOptions(progressive=False)
+    _, s2, _, _, st2 = render(ctx, scene, opts)
+    ctx.set_tuning(closest_tree=8, shadow_tree=8)
+    try:
+        _, s8, _, _, st8 = render(ctx, scene, opts)
+    finally:
+        ctx.set_tuning(closest_tree=2, shadow_tree=4)
+    err = np.abs(s8 - s2).max(-1) / np.maximum(1.0, np.abs(s2).max(-1))
+    assert np.mean(err <= 1e-4) >= 0.999, np.mean(err <= 1e-4)
+    assert st8["invalid_samples"] == 0 and abs(st8["rays"] - st2["rays"]) <= 0.001 * st2["rays"]
