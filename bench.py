@@ -82,6 +82,8 @@ def args(argv=None):
     p.add_argument("--no-autotune", action="store_true", help="keep the default pool and block size")
     p.add_argument("--pool", type=int, default=0, help="path slots (implies --no-autotune)")
     p.add_argument("--block", type=int, default=0, help="threads per block: 64, 128, 256 (implies --no-autotune)")
+    p.add_argument("--no-probe", action="store_true",
+                   help="skip the bandwidth probes (the roofline then uses the HBM figure alone)")
     p.add_argument("--closest-tree", type=int, choices=[2, 8], default=0,
                    help="closest-hit walk: 8 compressed eight-wide tree, 2 binary tree (default: the library's)")
     p.add_argument("--shadow-tree", type=int, choices=[4, 8], default=0,
@@ -369,7 +371,7 @@ def run_reference(a, dist, scenes, desc):
 # ---------------------------------------------------------------------------
 # GPU side: peaks and rooflines
 
-def measured_peaks(ctx):
+def measured_peaks(ctx, probe=True):
     """HBM copy peak (driver-measured file, else the pool's fallback), plus the
     read bandwidths this GPU shows for an L2-resident buffer, an L1-resident one
     and an HBM-sized one (rtg_probe_read_bandwidth)."""
@@ -378,6 +380,8 @@ def measured_peaks(ctx):
         hbm, src = float(json.load(open(p))["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs, STREAM-style copy)"
     else:
         hbm, src = 6650.0, "fallback 6.65 TB/s (MEASURED_PEAKS.json absent)"
+    if not probe:
+        return {"hbm": hbm, "hbm_source": src, "l2": float("inf"), "l1": float("inf"), "probe": "skipped"}
     return {"hbm": hbm, "hbm_source": src,
             "l2": ctx.probe_read_bandwidth(32 << 20, reps=40),
             "l1": ctx.probe_read_bandwidth(64 << 10, reps=200, l1=True),
@@ -576,7 +580,7 @@ def run_rtg(a, dist, scenes, desc):
     if a.closest_tree or a.shadow_tree:
         ctx.set_tuning(**({"closest_tree": a.closest_tree} if a.closest_tree else {}),
                        **({"shadow_tree": a.shadow_tree} if a.shadow_tree else {}))
-    peaks = measured_peaks(ctx)
+    peaks = measured_peaks(ctx, probe=not a.no_probe)
     opts = rtg.RenderOptions(progressive=not a.single_pass, max_pass_spp=32)
     hosts = [rtg.parse_scene(json.dumps(s)) for s in scenes]
     sids = [ctx.upload(h) for h in hosts]
