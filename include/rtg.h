@@ -210,8 +210,9 @@ enum {
 };
 int64_t rtg_scene_layout(rtg_context* ctx, rtg_scene_id scene, int32_t part, void* out, uint64_t cap);
 /* No counterpart in the reference. The device layout a host-compiled scene gets
- * at upload, computed on the host without a GPU (tests and tools): the same parts
- * and record formats as rtg_scene_layout (the built-on-GPU flag of ROOTS is 0).
+ * at upload with an eight-wide walk selected (so with the eight-wide tree and its
+ * slot order), computed on the host without a GPU (tests and tools): the same
+ * parts and record formats as rtg_scene_layout (the built-on-GPU flag of ROOTS is 0).
  * Copies min(cap, size) bytes to out (out may be NULL) and returns the part's full
  * size in bytes; RTG_ERR_INVALID for an unknown part or a scene compiled without
  * its BVH. */
@@ -307,7 +308,10 @@ typedef struct rtg_tuning {
                               * (default 1); 0: the fp32 traversal's own t, the value the renderer's
                               * closest-hit stage hands to shading */
   int32_t closest_tree;      /* closest-hit walk: 2 the binary tree (default), 8 the compressed eight-wide tree */
-  int32_t shadow_tree;       /* any-hit walk: 4 the four-wide tree (default), 8 the compressed eight-wide tree */
+  int32_t shadow_tree;       /* any-hit walk: 4 the four-wide tree (default), 8 the compressed eight-wide tree.
+                              * Scenes get the eight-wide tree (and its slot order) when they are uploaded
+                              * while either walk is 8; rendering or querying a scene without it with an
+                              * eight-wide walk selected returns RTG_ERR_INVALID. */
   int32_t reserved;
 } rtg_tuning;
 int rtg_get_tuning(rtg_context* ctx, rtg_tuning* out);

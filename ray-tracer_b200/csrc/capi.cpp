@@ -293,7 +293,7 @@ int64_t rtg_host_scene_layout(const rtg_host_scene* hs, int32_t part, void* out,
   if (!hs) return RTG_ERR_INVALID;
   try {
     if (!hs->scene->bvh_built) return RTG_ERR_INVALID;
-    const rtg::FlatScene f = rtg::flatten(*hs->scene);
+    const rtg::FlatScene f = rtg::flatten(*hs->scene, true);
     const std::int32_t roots[5] = {f.root, f.root4, static_cast<std::int32_t>(f.slot_prim.size()), 0, f.root8};
     const void* src = nullptr;
     std::size_t bytes = 0;

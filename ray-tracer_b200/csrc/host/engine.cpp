@@ -214,10 +214,10 @@ int Engine::add_scene(std::shared_ptr<const CompiledScene> scene) {
     built->bvh.build(boxes, 4);
     built->info.bvh = built->bvh.stats;
     built->bvh_built = true;
-    FlatScene flat = flatten(*built);
+    FlatScene flat = flatten(*built, wants_wide8());
     return add_flat(std::move(built), std::move(flat));
   }
-  FlatScene flat = flatten(*scene);
+  FlatScene flat = flatten(*scene, wants_wide8());
   return add_flat(std::move(scene), std::move(flat));
 }
 
@@ -232,13 +232,14 @@ std::vector<int> Engine::add_scenes(const std::vector<std::shared_ptr<const Comp
       return ids;
     }
   std::vector<FlatScene> flats(scenes.size());
+  const bool wide8 = wants_wide8();
   std::atomic<std::size_t> next{0};
   std::exception_ptr failed;
   std::mutex failed_lock;
   auto work = [&] {
     for (std::size_t k; (k = next.fetch_add(1)) < scenes.size();) {
       try {
-        flats[k] = flatten(*scenes[k]);
+        flats[k] = flatten(*scenes[k], wide8);
       } catch (...) {
         std::lock_guard<std::mutex> g(failed_lock);
         if (!failed) failed = std::current_exception();
@@ -334,6 +335,7 @@ int Engine::register_flat(std::shared_ptr<const CompiledScene> scene, FlatScene 
   gs->n_wide = static_cast<std::int32_t>(flat.nodes4.size());
   gs->root8 = flat.root8;
   gs->n_wide8 = static_cast<std::int32_t>(flat.nodes8.size());
+  gs->has_wide8 = wants_wide8();
   void* block = nullptr;
   count_allocation();
   CK(cudaMallocFromPoolAsync(&block, p.total, pool_, stream_));
@@ -489,22 +491,35 @@ int Engine::add_scene_gpu_bvh(std::shared_ptr<const CompiledScene> scene) {
   auto* s_old_of = reinterpret_cast<std::uint32_t*>(sb + sat[5]);
   auto* s_new_of = reinterpret_cast<std::uint32_t*>(sb + sat[6]);
   builder.emit(in, s_nodes, s_nodes4, s_prims, s_material, s_normals, order);
-  std::vector<DevNode> bin_nodes(static_cast<std::size_t>(c.interior));
-  std::vector<std::uint32_t> row0_w(n_items), prim_of_slot(n_items);
-  if (c.interior)
-    CK(cudaMemcpyAsync(bin_nodes.data(), s_nodes, scratch_bytes[0], cudaMemcpyDeviceToHost, build_stream_));
-  if (n_items) {
-    // The w word of each slot's first row: its primitive id and leaf-end mark.
-    CK(cudaMemcpy2DAsync(row0_w.data(), sizeof(std::uint32_t), reinterpret_cast<const unsigned char*>(s_prims) + 12,
-                         3 * sizeof(float4), sizeof(std::uint32_t), n_items, cudaMemcpyDeviceToHost, build_stream_));
+  const bool want8 = wants_wide8();
+  std::vector<DevNode> bin_nodes;
+  std::vector<std::uint32_t> row0_w, prim_of_slot(n_items);
+  if (n_items)
     CK(cudaMemcpyAsync(prim_of_slot.data(), order, n_items * sizeof(std::uint32_t), cudaMemcpyDeviceToHost,
                        build_stream_));
+  if (want8) {
+    bin_nodes.resize(static_cast<std::size_t>(c.interior));
+    row0_w.resize(n_items);
+    if (c.interior)
+      CK(cudaMemcpyAsync(bin_nodes.data(), s_nodes, scratch_bytes[0], cudaMemcpyDeviceToHost, build_stream_));
+    if (n_items)  // the w word of each slot's first row: its primitive id and leaf-end mark
+      CK(cudaMemcpy2DAsync(row0_w.data(), sizeof(std::uint32_t), reinterpret_cast<const unsigned char*>(s_prims) + 12,
+                           3 * sizeof(float4), sizeof(std::uint32_t), n_items, cudaMemcpyDeviceToHost, build_stream_));
+    CK(cudaStreamSynchronize(build_stream_));
   }
-  CK(cudaStreamSynchronize(build_stream_));
-  std::vector<std::uint8_t> last(n_items);
-  for (std::size_t k = 0; k < n_items; ++k) last[k] = (row0_w[k] & kLastInLeaf) ? 1 : 0;
-  const std::int32_t bin_root = n_items ? c.root : kNoRoot;
-  Wide8 w8 = build_wide8(bin_nodes.data(), bin_nodes.size(), bin_root, last.data(), n_items);
+  Wide8 w8;
+  if (want8) {
+    std::vector<std::uint8_t> last(n_items);
+    for (std::size_t k = 0; k < n_items; ++k) last[k] = (row0_w[k] & kLastInLeaf) ? 1 : 0;
+    const std::int32_t bin_root = n_items ? c.root : kNoRoot;
+    w8 = build_wide8(bin_nodes.data(), bin_nodes.size(), bin_root, last.data(), n_items);
+  } else {
+    // The binary tree's own slot order, no eight-wide tree.
+    w8.old_of.resize(n_items);
+    for (std::size_t k = 0; k < n_items; ++k) w8.old_of[k] = static_cast<std::uint32_t>(k);
+    w8.new_of = w8.old_of;
+    w8.root = kNoRoot;
+  }
 
   // The scene's arrays, in add_flat's order, in one allocation.
   const std::size_t part_bytes[kSceneParts] = {
@@ -543,24 +558,32 @@ int Engine::add_scene_gpu_bvh(std::shared_ptr<const CompiledScene> scene) {
   for (int k : {0, 1})
     if (part_bytes[k])
       CK(cudaMemcpyAsync(dst + at[k], sb + sat[k], part_bytes[k], cudaMemcpyDeviceToDevice, build_stream_));
-  if (n_items) {
-    CK(cudaMemcpyAsync(s_old_of, w8.old_of.data(), n_items * sizeof(std::uint32_t), cudaMemcpyHostToDevice, build_stream_));
-    CK(cudaMemcpyAsync(s_new_of, w8.new_of.data(), n_items * sizeof(std::uint32_t), cudaMemcpyHostToDevice, build_stream_));
+  if (want8) {
+    if (n_items) {
+      CK(cudaMemcpyAsync(s_old_of, w8.old_of.data(), n_items * sizeof(std::uint32_t), cudaMemcpyHostToDevice, build_stream_));
+      CK(cudaMemcpyAsync(s_new_of, w8.new_of.data(), n_items * sizeof(std::uint32_t), cudaMemcpyHostToDevice, build_stream_));
+    }
+    if (part_bytes[8])
+      CK(cudaMemcpyAsync(gs->nodes8, w8.nodes.data(), part_bytes[8], cudaMemcpyHostToDevice, build_stream_));
+    CK(apply_slot_order(s_old_of, s_new_of, n_items, s_prims, s_normals, s_material, gs->prims, gs->slot_normals,
+                        gs->slot_material, gs->nodes, c.interior, gs->nodes4, c.wide, build_stream_));
+  } else {
+    // The slots stay in the binary tree's order.
+    for (int k : {2, 3, 4})
+      if (part_bytes[k])
+        CK(cudaMemcpyAsync(dst + at[k], sb + sat[k], part_bytes[k], cudaMemcpyDeviceToDevice, build_stream_));
   }
-  if (part_bytes[8])
-    CK(cudaMemcpyAsync(gs->nodes8, w8.nodes.data(), part_bytes[8], cudaMemcpyHostToDevice, build_stream_));
-  CK(apply_slot_order(s_old_of, s_new_of, n_items, s_prims, s_normals, s_material, gs->prims, gs->slot_normals,
-                      gs->slot_material, gs->nodes, c.interior, gs->nodes4, c.wide, build_stream_));
   for (int k = 5; k < 8; ++k)
     if (part_bytes[k]) CK(cudaMemcpyAsync(dst + at[k], dev_in + in_at[k], part_bytes[k], cudaMemcpyDeviceToDevice, build_stream_));
+  CK(cudaStreamSynchronize(build_stream_));
   gs->slot_prim.resize(n_items);
   for (std::size_t k = 0; k < n_items; ++k) gs->slot_prim[k] = prim_of_slot[w8.old_of[k]];
-  CK(cudaStreamSynchronize(build_stream_));
 
   gs->root = n_items ? remap_link(c.root, w8.new_of) : kNoRoot;
   gs->root4 = n_items ? remap_link(c.root4, w8.new_of) : kNoRoot;
   gs->root8 = w8.root;
   gs->n_wide8 = static_cast<std::int32_t>(w8.nodes.size());
+  gs->has_wide8 = want8;
   gs->n_slots = static_cast<std::int32_t>(n_items);
   gs->n_interior = c.interior;
   gs->n_wide = c.wide;
@@ -673,6 +696,9 @@ void Engine::free_frame(GpuFrame& f) {
 }
 
 RtgSceneDev Engine::job_descriptor(const GpuScene& sc, const RenderSettings& s, const GpuFrame& f) const {
+  if (wants_wide8() && !sc.has_wide8)
+    throw std::invalid_argument("scene was uploaded without the eight-wide tree: select the eight-wide walk "
+                                "(rtg_tuning closest_tree / shadow_tree = 8) before uploading it");
   RtgSceneDev d{};
   describe(*sc.host, s, d);
   d.nodes = sc.nodes;

@@ -75,8 +75,9 @@ struct GpuScene {
   DevNode* nodes = nullptr;
   DevNode4* nodes4 = nullptr;  // four-wide copy of the tree (any-hit queries)
   std::int32_t root4 = kNoRoot;
-  DevNode8* nodes8 = nullptr;  // compressed eight-wide copy (closest-hit queries)
+  DevNode8* nodes8 = nullptr;  // compressed eight-wide copy (built when an eight-wide walk is selected)
   std::int32_t root8 = kNoRoot;
+  bool has_wide8 = false;      // uploaded with the eight-wide tree (and its slot order)
   float4* prims = nullptr;
   std::uint32_t* slot_material = nullptr;
   float4* slot_normals = nullptr;
@@ -137,6 +138,8 @@ class Engine {
   void reset_wave();
   cudaStream_t stream() const { return stream_; }
   EngineConfig& config() { return cfg_; }
+  // Scenes uploaded now get the eight-wide tree: an eight-wide walk is selected.
+  bool wants_wide8() const { return cfg_.shape.closest_tree == 8 || cfg_.shape.shadow_tree == 8; }
 
   // Host-built scenes are flattened on the host. Scenes compiled without a BVH
   // (BvhBuild::Defer / Auto) get it built on the GPU (add_scene_gpu_bvh) from

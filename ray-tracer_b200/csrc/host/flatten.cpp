@@ -269,7 +269,7 @@ void flatten_tables(const CompiledScene& s, FlatScene& f) {
   }
 }
 
-FlatScene flatten(const CompiledScene& s) {
+FlatScene flatten(const CompiledScene& s, bool wide8) {
   FlatScene f;
   const BinaryBvh& bvh = s.bvh;
 
@@ -322,7 +322,7 @@ FlatScene flatten(const CompiledScene& s) {
   });
   if (!bvh.nodes.empty()) f.root = link_of(0);
   build_wide(bvh, fbox, f);
-  add_wide8(f);
+  if (wide8) add_wide8(f);
 
   flatten_tables(s, f);
   return f;

@@ -39,7 +39,9 @@ struct FlatScene {
   std::int32_t root8 = kNoRoot;
 };
 
-FlatScene flatten(const CompiledScene& s);
+// wide8: also build the compressed eight-wide tree and move the slots to its
+// order (add_wide8); without it nodes8 stays empty and root8 kNoRoot.
+FlatScene flatten(const CompiledScene& s, bool wide8);
 
 // Builds the eight-wide tree from f.nodes / f.root and moves every per-slot array
 // of f (and the binary and four-wide trees' leaf links) to its slot order.

@@ -194,3 +194,16 @@ def test_ray_queries_on_a_gpu_built_scene(ctx):
     finally:
         ctx.release(a)
         ctx.release(b)
+
+
+@pytest.mark.parametrize("name", ["mesh", "spheres", "depth_cap_level_pass", "emitters_and_planes"])
+def test_eight_wide_layout_matches_host_build(ctx, name):
+    """With an eight-wide walk selected, both builds also make the eight-wide tree
+    and move the slots to its order: still byte-identical, eight-wide nodes included."""
+    scene = {"mesh": workloads.mesh_stress, "spheres": workloads.sphere_field}.get(name)
+    host = rtg.parse_scene(json.dumps(scene() if scene else EDGE[name]))
+    ctx.set_tuning(closest_tree=8, shadow_tree=8)
+    try:
+        ia, _ = _compare(ctx, host)
+    finally:
+        ctx.set_tuning(closest_tree=2, shadow_tree=4)

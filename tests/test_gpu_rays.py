@@ -198,8 +198,13 @@ def tree(ctx, request):
 def test_eight_wide_tree_finds_the_hits_of_the_binary_tree(ctx, scenes, cfg, tree):
     """The compressed eight-wide walk (selectable with closest_tree / shadow_tree)
     against the oracle, like the default walk: ids identical or exact ties, t within
-    1e-5 after refinement; any-hit answers equal the binary closest hit's verdict."""
-    _, view, sid = scenes[cfg]
+    1e-5 after refinement; any-hit answers equal the closest hit's verdict. The
+    scene is uploaded with the eight-wide walk selected, so it gets that tree; a
+    scene uploaded before is refused rather than walked without it."""
+    host, view, old_sid = scenes[cfg]
+    with pytest.raises(rtg.RtgError):
+        ctx.trace_closest(old_sid, workloads.random_rays(view, 16, seed=1))
+    sid = ctx.upload(host)
     n = 1_000_000 if cfg == "mesh" else 200_000
     rays = workloads.random_rays(view, n, seed=404)
     t, prim, plane, _ = ctx.trace_closest(sid, rays)
@@ -214,3 +219,4 @@ def test_eight_wide_tree_finds_the_hits_of_the_binary_tree(ctx, scenes, cfg, tre
     near = np.abs(t - tmax) <= 1e-5 * tmax
     expect = (prim >= 0) & (t < tmax)
     assert np.array_equal(occ[~near].astype(bool), expect[~near])
+    ctx.release(sid)
