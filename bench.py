@@ -390,13 +390,13 @@ def measured_peaks(ctx, probe=True):
                      "x200; HBM read = 4 GiB, x1; best of 5 launches"}
 
 
-def ncu_profile(kernel: str, pool_paths: int):
+def ncu_profile(kernel: str, pool_paths: int, tree: int = 2):
     """Per-ray counters of `kernel` from the committed ncu capture of the mix
-    (profiles/<kernel>_mix_*.json) at this pool size, or None."""
+    (profiles/<kernel>_mix_*.json) at this pool size and closest-hit tree, or None."""
     for fname in sorted(os.listdir(os.path.join(ROOT, "profiles"))):
         if fname.startswith(kernel + "_mix") and fname.endswith(".json"):
             d = json.load(open(os.path.join(ROOT, "profiles", fname)))
-            if int(d.get("pool_paths", 0)) != int(pool_paths):
+            if int(d.get("pool_paths", 0)) != int(pool_paths) or int(d.get("closest_tree", 2)) != int(tree):
                 continue
             if "dram_bytes_per_ray" not in d and d.get("rays_per_launch"):
                 d["dram_bytes_per_ray"] = d["dram_bytes_per_launch"] / d["rays_per_launch"]
@@ -433,7 +433,7 @@ def rooflines(ctx, step, peaks, profile=True):
     hbm_b = (cont * 32 + rays * 16 + new_paths * (64 + 16)) / launches
     onchip_b = (c_st["node_visits"] * node_bytes + c_st["prim_tests"] * PRIM_BYTES) / launches
     levels = {"hbm": {"bytes": hbm_b, "peak": peaks["hbm"]}, "l1": {"bytes": onchip_b, "peak": peaks["l1"]}}
-    prof = ncu_profile("k_extend", ctx.tuning()["pool_paths"]) if profile else None
+    prof = ncu_profile("k_extend", ctx.tuning()["pool_paths"], ctx.tuning().get("closest_tree", 2)) if profile else None
     rays_pl = rays / launches
     if prof and prof.get("l2_bytes_per_ray"):
         levels["l2"] = {"bytes": prof["l2_bytes_per_ray"] * rays_pl, "peak": peaks["l2"]}
