@@ -746,6 +746,10 @@ int rtg_set_tuning(rtg_context* ctx, const rtg_tuning* in) {
     if (in->pool_paths < 1024 || in->pool_paths > (1u << 23)) throw std::invalid_argument("pool_paths must be in [1024, 2^23]");
     if (in->max_pass_samples < 1 || in->max_pass_samples > (1ull << 31)) throw std::invalid_argument("max_pass_samples must be in [1, 2^31]");
     if (in->backlog_pools < 1 || in->backlog_pools > 64) throw std::invalid_argument("backlog_pools must be in [1, 64]");
+    if (in->closest_tree != 2 && in->closest_tree != 8) throw std::invalid_argument("closest_tree must be 2 or 8");
+    if (in->shadow_tree != 4 && in->shadow_tree != 8) throw std::invalid_argument("shadow_tree must be 4 or 8");
+    if (in->serve_reserve_bytes > (in->serve_budget_bytes ? in->serve_budget_bytes : ctx->serve_budget))
+      throw std::invalid_argument("serve_reserve_bytes exceeds the budget");
     rtg::EngineConfig& c = ctx->engine->config();
     const bool realloc = c.pool_paths != in->pool_paths || c.max_pass_samples != in->max_pass_samples;
     if (realloc && ctx->engine->open_requests() > 0) {
@@ -763,12 +767,9 @@ int rtg_set_tuning(rtg_context* ctx, const rtg_tuning* in) {
     c.backlog_pools = in->backlog_pools;
     c.shape.chained = in->chained != 0;
     c.refine_hits = in->refine_hits != 0;
-    if (in->closest_tree != 2 && in->closest_tree != 8) throw std::invalid_argument("closest_tree must be 2 or 8");
-    if (in->shadow_tree != 4 && in->shadow_tree != 8) throw std::invalid_argument("shadow_tree must be 4 or 8");
     c.shape.closest_tree = in->closest_tree;
     c.shape.shadow_tree = in->shadow_tree;
     if (in->serve_budget_bytes) ctx->serve_budget = in->serve_budget_bytes;
-    if (in->serve_reserve_bytes > ctx->serve_budget) throw std::invalid_argument("serve_reserve_bytes exceeds the budget");
     ctx->serve_reserve = in->serve_reserve_bytes;
     if (realloc) ctx->engine->reset_wave();
     return RTG_OK;

@@ -24,10 +24,13 @@ MODES = ["refined", "fp32"]
 # Share of hits whose fp32 t is within 1e-5 of the reference's double t. Each
 # primitive slot carries the residual its fp32 position lost (triangle plane
 # offset, sphere centre, plane point), which the distance test adds back, so the
-# remaining error is the fp32 arithmetic: the mesh's 1M-ray set meets 1e-5 on
-# 99.99% of hits; the random-origin sets of the sphere field (99.988% measured)
-# and the 555-unit Cornell room keep a few short or grazing hits just above it.
-FP32_T_SHARE = {"cornell": 0.999, "spheres": 0.9998, "mesh": 0.9999}
+# remaining error is the fp32 arithmetic. Measured on the seeded sets: mesh 1M
+# rays 99.9991%, Cornell 200k rays 99.9908%, and every hit of the reference's
+# own fixtures. The sphere field's 200k random-origin rays reach 99.988%: a few
+# hits within a few percent of a radius of the ray origin (origins next to or
+# inside a sphere) keep an fp32 root error that is a larger share of their short
+# t, so its bar is below 99.99%.
+FP32_T_SHARE = {"cornell": 0.9999, "spheres": 0.9998, "mesh": 0.9999}
 
 
 @pytest.fixture
