@@ -390,6 +390,16 @@ def measured_peaks(ctx, probe=True):
                      "x200; HBM read = 4 GiB, x1; best of 5 launches"}
 
 
+def sm_count(dev: int):
+    """Streaming multiprocessors of GPU `dev` (None when it cannot be read)."""
+    try:
+        import torch
+
+        return torch.cuda.get_device_properties(dev).multi_processor_count
+    except Exception:
+        return None
+
+
 def ncu_profile(kernel: str, pool_paths: int, tree: int = 2):
     """Per-ray counters of `kernel` from the committed ncu capture of the mix
     (profiles/<kernel>_mix_*.json) at this pool size and closest-hit tree, or None."""
@@ -416,7 +426,10 @@ def rooflines(ctx, step, peaks, profile=True):
            init per new camera path) / HBM peak;
       L1:  the traversal's fetches (node bytes per visit, 48 B per primitive
            test, from device counters) / aggregate L1 read peak;
-      L2:  the L2 bytes an ncu capture of the same kernel measured / L2 peak.
+      L2:  the L2 bytes an ncu capture of the same kernel measured / L2 peak;
+      issue: the warp instructions per ray that capture counted / the SM's
+           peak issue rate (4 schedulers per SM, one instruction per clock each,
+           at the SM clock sampled during the timed steps).
     The binding level is the `bound`; frac = that level's lower bound on the
     launch time / the measured launch time."""
     ctx.set_tuning(time_kernels=1, count_traversal=0)
@@ -432,11 +445,15 @@ def rooflines(ctx, step, peaks, profile=True):
     cont = rays - new_paths
     hbm_b = (cont * 32 + rays * 16 + new_paths * (64 + 16)) / launches
     onchip_b = (c_st["node_visits"] * node_bytes + c_st["prim_tests"] * PRIM_BYTES) / launches
-    levels = {"hbm": {"bytes": hbm_b, "peak": peaks["hbm"]}, "l1": {"bytes": onchip_b, "peak": peaks["l1"]}}
+    levels = {"hbm": {"bytes": hbm_b, "peak": peaks["hbm"], "unit": "GB/s"},
+              "l1": {"bytes": onchip_b, "peak": peaks["l1"], "unit": "GB/s"}}
     prof = ncu_profile("k_extend", ctx.tuning()["pool_paths"], ctx.tuning().get("closest_tree", 2)) if profile else None
     rays_pl = rays / launches
     if prof and prof.get("l2_bytes_per_ray"):
-        levels["l2"] = {"bytes": prof["l2_bytes_per_ray"] * rays_pl, "peak": peaks["l2"]}
+        levels["l2"] = {"bytes": prof["l2_bytes_per_ray"] * rays_pl, "peak": peaks["l2"], "unit": "GB/s"}
+    if prof and prof.get("warp_inst_per_ray") and peaks.get("sms") and peaks.get("sm_mhz"):
+        levels["issue"] = {"bytes": prof["warp_inst_per_ray"] * rays_pl,
+                           "peak": 4 * peaks["sms"] * peaks["sm_mhz"] / 1e3, "unit": "G warp instructions/s"}
     for v in levels.values():
         v["achieved"] = v["bytes"] / avg_s / 1e9
         v["frac"] = v["achieved"] / v["peak"]
@@ -445,9 +462,10 @@ def rooflines(ctx, step, peaks, profile=True):
     kernel_total = sum(t_st[k] for k in ("extend_ms", "shade_ms", "shadow_ms", "accumulate_ms", "plan_ms"))
     ext = {
         "kernel": "k_extend (closest-hit BVH traversal + camera-path generation)",
-        "bound": bound, "achieved": levels[bound]["achieved"], "peak": levels[bound]["peak"], "unit": "GB/s",
-        "frac": levels[bound]["frac"], "traffic": traffic,
-        "levels": {k: {"achieved": v["achieved"], "peak": v["peak"], "frac": v["frac"]} for k, v in levels.items()},
+        "bound": bound, "achieved": levels[bound]["achieved"], "peak": levels[bound]["peak"],
+        "unit": levels[bound]["unit"], "frac": levels[bound]["frac"], "traffic": traffic,
+        "levels": {k: {"achieved": v["achieved"], "peak": v["peak"], "unit": v["unit"], "frac": v["frac"]}
+                   for k, v in levels.items()},
         "dram_frac": traffic / avg_s / 1e9 / peaks["hbm"] if traffic else None,
         "avg_launch_ms": avg_s * 1e3, "launches": launches, "rays_per_launch": rays_pl,
         "share_of_kernel_time": t_st["extend_ms"] / kernel_total if kernel_total else None,
@@ -455,12 +473,15 @@ def rooflines(ctx, step, peaks, profile=True):
                     "node_bytes": node_bytes},
     }
     if prof:
-        ext["ncu"] = {k: prof[k] for k in ("lanes_active", "issue_active", "l1_hit_rate", "l2_hit_rate")
-                      if k in prof}
+        ext["ncu"] = {k: prof[k] for k in ("lanes_active", "issue_active", "l1_hit_rate", "l2_hit_rate",
+                                           "warp_inst_per_ray", "thread_inst_per_ray") if k in prof}
+        if prof.get("warp_inst_per_ray") and prof.get("thread_inst_per_ray"):
+            # Useful share of the issue slots: lanes doing work in each issued instruction.
+            ext["lane_efficiency"] = prof["thread_inst_per_ray"] / (32 * prof["warp_inst_per_ray"])
         ext["ncu"]["file"] = prof["file"]
-    # k_shade streams path state: read 56 B state + 16 B hit per path, write 56 B
+    # k_shade streams path state: read 64 B state + 16 B hit per path, write 64 B
     # per continuing path and 48 B per shadow ray (materials and lights stay cached).
-    shade_b = (rays * (56 + 16) + cont * 56 + c_st["shadow_rays"] * 48) / max(1, launches)
+    shade_b = (rays * (64 + 16) + cont * 64 + c_st["shadow_rays"] * 48) / max(1, launches)
     shade_s = t_st["shade_ms"] / max(1, launches) / 1e3
     shade = {"kernel": "k_shade", "bound": "hbm", "achieved": shade_b / shade_s / 1e9 if shade_s else None,
              "peak": peaks["hbm"], "unit": "GB/s",
@@ -657,6 +678,8 @@ def run_rtg(a, dist, scenes, desc):
                  "target_batched_over_plain": 2.0,
                  "rmse": "identical images (bit-identical framebuffers), so matched RMSE by construction"}
 
+    peaks["sm_mhz"] = t["clocks"].get("sm_mhz") or t["clocks"].get("sm_max_mhz")
+    peaks["sms"] = sm_count(dev)
     ext, shade, kernel_ms, c_st = rooflines(ctx, step, peaks)
 
     # Serving: Poisson arrivals of previews and finals over 32 resident scenes.
@@ -743,7 +766,8 @@ def run_rtg(a, dist, scenes, desc):
                    "k_extend": {"bound": ext["bound"], "frac": ext["frac"], "dram_frac": ext["dram_frac"],
                                 "levels": {k: v["frac"] for k, v in ext["levels"].items()},
                                 **({"lanes_active": ext["ncu"].get("lanes_active"),
-                                    "issue_active": ext["ncu"].get("issue_active")} if "ncu" in ext else {})},
+                                    "issue_active": ext["ncu"].get("issue_active"),
+                                    "lane_efficiency": ext.get("lane_efficiency")} if "ncu" in ext else {})},
                    "k_shade_hbm_frac": shade["frac"]}
         if per_config:
             for tag, e in per_config.items():

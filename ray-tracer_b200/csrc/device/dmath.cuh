@@ -29,11 +29,30 @@ __device__ __forceinline__ float3 cross3(float3 a, float3 b) {
 __device__ __forceinline__ float max3(float3 a) { return fmaxf(a.x, fmaxf(a.y, a.z)); }
 __device__ __forceinline__ bool is_zero3(float3 a) { return a.x == 0.f && a.y == 0.f && a.z == 0.f; }
 
-// Normalise, or return `fallback` for (near-)zero or non-finite input.
+// Pinned rounding, for the code that decides hits: the hit tests, the slab
+// set-up and the camera ray. Every product and sum is an explicit fmaf or an
+// __fmul_rn / __fadd_rn / __fsub_rn, which the compiler never fuses, so the bits
+// do not depend on the kernel the code is inlined into. (Left to contract freely,
+// the counting and non-counting instances of the closest-hit kernel rounded a few
+// hits differently.)
+__device__ __forceinline__ float3 sub3p(float3 a, float3 b) {
+  return f3(__fsub_rn(a.x, b.x), __fsub_rn(a.y, b.y), __fsub_rn(a.z, b.z));
+}
+__device__ __forceinline__ float3 add3p(float3 a, float3 b) {
+  return f3(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y), __fadd_rn(a.z, b.z));
+}
+__device__ __forceinline__ float dot3p(float3 a, float3 b) { return fmaf(a.z, b.z, fmaf(a.y, b.y, __fmul_rn(a.x, b.x))); }
+__device__ __forceinline__ float3 cross3p(float3 a, float3 b) {
+  return f3(fmaf(a.y, b.z, -__fmul_rn(a.z, b.y)), fmaf(a.z, b.x, -__fmul_rn(a.x, b.z)),
+            fmaf(a.x, b.y, -__fmul_rn(a.y, b.x)));
+}
+
+// Normalise (pinned rounding), or return `fallback` for (near-)zero or non-finite input.
 __device__ __forceinline__ float3 unit_or(float3 v, float3 fallback) {
-  const float l2 = dot3(v, v);
+  const float l2 = dot3p(v, v);
   if (!(l2 > 1e-30f) || !isfinite(l2)) return fallback;
-  return v * rsqrtf(l2);
+  const float s = rsqrtf(l2);
+  return f3(__fmul_rn(v.x, s), __fmul_rn(v.y, s), __fmul_rn(v.z, s));
 }
 
 __device__ __forceinline__ float3 reflect3(float3 v, float3 n) { return v - (2.f * dot3(v, n)) * n; }
@@ -103,7 +122,7 @@ __device__ __forceinline__ float2 unit_disk(Pcg& rng) {
   const float r = sqrtf(rng.uniform());
   float s, c;
   sincospif(2.f * rng.uniform(), &s, &c);
-  return make_float2(r * c, r * s);
+  return make_float2(__fmul_rn(r, c), __fmul_rn(r, s));
 }
 
 __device__ __forceinline__ float3 unit_vector(Pcg& rng) {

@@ -44,7 +44,7 @@ struct SlabRay {
     // the slab on that axis then spans everything or nothing, as it should.
     auto safe = [](float c) { return fabsf(c) < 1e-20f ? copysignf(1e-20f, c) : c; };
     inv = f3(1.f / safe(d.x), 1.f / safe(d.y), 1.f / safe(d.z));
-    ooi = f3(o.x * inv.x, o.y * inv.y, o.z * inv.z);
+    ooi = f3(__fmul_rn(o.x, inv.x), __fmul_rn(o.y, inv.y), __fmul_rn(o.z, inv.z));
     neg[0] = d.x < 0.f;
     neg[1] = d.y < 0.f;
     neg[2] = d.z < 0.f;
@@ -84,20 +84,20 @@ constexpr float kEdgeSlack = 1e-6f;
 // `k` is dot(r, e1 x e2) for the residual r that rounding v0 to fp32 lost: the
 // distance to the plane through the double-precision v0 is (dot(e2, qv) - k) / det.
 // For hits close to the ray origin that rounding, not the arithmetic, dominates
-// the error of t.
+// the error of t. Rounding is pinned (dmath.cuh) so every kernel gets the same hit.
 __device__ __forceinline__ bool tri_test(float3 o, float3 d, float3 v0, float3 e1, float3 e2, float k, float tmin,
                                          float tmax, float& t, float& b1, float& b2) {
-  const float3 pv = cross3(d, e2);
-  const float det = dot3(e1, pv);
+  const float3 pv = cross3p(d, e2);
+  const float det = dot3p(e1, pv);
   if (fabsf(det) < 1e-14f) return false;
   const float inv_det = 1.f / det;
-  const float3 tv = o - v0;
-  const float u = dot3(tv, pv) * inv_det;
+  const float3 tv = sub3p(o, v0);
+  const float u = __fmul_rn(dot3p(tv, pv), inv_det);
   if (u < -kEdgeSlack || u > 1.f + kEdgeSlack) return false;
-  const float3 qv = cross3(tv, e1);
-  const float v = dot3(d, qv) * inv_det;
-  if (v < -kEdgeSlack || u + v > 1.f + kEdgeSlack) return false;
-  const float tt = (dot3(e2, qv) - k) * inv_det;
+  const float3 qv = cross3p(tv, e1);
+  const float v = __fmul_rn(dot3p(d, qv), inv_det);
+  if (v < -kEdgeSlack || __fadd_rn(u, v) > 1.f + kEdgeSlack) return false;
+  const float tt = __fmul_rn(__fsub_rn(dot3p(e2, qv), k), inv_det);
   if (!(tmin < tt && tt < tmax)) return false;
   t = tt;
   b1 = u;
@@ -109,18 +109,19 @@ __device__ __forceinline__ bool tri_test(float3 o, float3 d, float3 v0, float3 e
 // Ray/Sphere Intersection", Ray Tracing Gems ch. 7), as the reference's
 // Sphere::hit_t (include/raytracer/geometry/shapes.hpp:25-46). `rc` is what
 // rounding the centre to fp32 lost; adding it after the subtraction gives the
-// offset to the double-precision centre.
+// offset to the double-precision centre. Rounding is pinned (dmath.cuh).
 __device__ __forceinline__ bool sphere_test(float3 o, float3 d, float3 c, float3 rc, float radius, float tmin,
                                             float tmax, float& t) {
-  const float3 oc = (c - o) + rc;
-  const float a = dot3(d, d);
+  const float3 oc = add3p(sub3p(c, o), rc);
+  const float a = dot3p(d, d);
   if (a == 0.f) return false;
-  const float h = dot3(d, oc);
-  const float cc = dot3(oc, oc) - radius * radius;
-  const float3 perp = oc - (h / a) * d;
-  const float disc = a * (radius * radius - dot3(perp, perp));
+  const float h = dot3p(d, oc);
+  const float cc = fmaf(-radius, radius, dot3p(oc, oc));
+  const float s = h / a;
+  const float3 perp = f3(fmaf(-s, d.x, oc.x), fmaf(-s, d.y, oc.y), fmaf(-s, d.z, oc.z));
+  const float disc = __fmul_rn(a, fmaf(radius, radius, -dot3p(perp, perp)));
   if (disc < 0.f) return false;
-  const float q = h + copysignf(sqrtf(disc), h);
+  const float q = __fadd_rn(h, copysignf(sqrtf(disc), h));
   float t0 = cc / q, t1 = q / a;
   if (q == 0.f) t0 = t1 = h / a;
   if (t0 > t1) { const float s = t0; t0 = t1; t1 = s; }
@@ -133,12 +134,13 @@ __device__ __forceinline__ bool sphere_test(float3 o, float3 d, float3 c, float3
   return true;
 }
 
-// normal.w holds the plane offset that rounding the point to fp32 lost.
+// normal.w holds the plane offset that rounding the point to fp32 lost. Rounding
+// is pinned (dmath.cuh).
 __device__ __forceinline__ bool plane_test(const DevPlane& pl, float3 o, float3 d, float tmin, float tmax, float& t) {
   const float3 n = f3(pl.normal);
-  const float denom = dot3(n, d);
+  const float denom = dot3p(n, d);
   if (fabsf(denom) < 1e-12f) return false;
-  const float tt = (dot3(f3(pl.point) - o, n) + pl.normal.w) / denom;
+  const float tt = __fadd_rn(dot3p(sub3p(f3(pl.point), o), n), pl.normal.w) / denom;
   if (!(tmin < tt && tt < tmax)) return false;
   t = tt;
   return true;
@@ -347,10 +349,11 @@ __device__ __forceinline__ Node8Hits node8_hits(const DevNode8* __restrict__ nd,
   const std::uint32_t ew = __float_as_uint(a.w);
   h.imask = ew >> 24;
   // Node space: t = q * (scale / d) + (p - o) / d per axis.
-  const float ax = __uint_as_float((ew & 0xFFu) << 23) * r.inv.x;
-  const float ay = __uint_as_float(((ew >> 8) & 0xFFu) << 23) * r.inv.y;
-  const float az = __uint_as_float(((ew >> 16) & 0xFFu) << 23) * r.inv.z;
-  const float bx = (a.x - r.o.x) * r.inv.x, by = (a.y - r.o.y) * r.inv.y, bz = (a.z - r.o.z) * r.inv.z;
+  const float ax = __fmul_rn(__uint_as_float((ew & 0xFFu) << 23), r.inv.x);
+  const float ay = __fmul_rn(__uint_as_float(((ew >> 8) & 0xFFu) << 23), r.inv.y);
+  const float az = __fmul_rn(__uint_as_float(((ew >> 16) & 0xFFu) << 23), r.inv.z);
+  const float bx = __fmul_rn(__fsub_rn(a.x, r.o.x), r.inv.x), by = __fmul_rn(__fsub_rn(a.y, r.o.y), r.inv.y);
+  const float bz = __fmul_rn(__fsub_rn(a.z, r.o.z), r.inv.z);
   // Near and far planes per axis: lo bytes when the direction is positive.
   const bool px = !(r.oct & 1u), py = !(r.oct & 2u), pz = !(r.oct & 4u);
   const std::uint32_t nx0 = px ? q0.x : q1.z, nx1 = px ? q0.y : q1.w, fx0 = px ? q1.z : q0.x, fx1 = px ? q1.w : q0.y;

@@ -361,3 +361,36 @@ def test_eight_wide_walk_renders_the_same_samples(ctx):
     err = np.abs(s8 - s2).max(-1) / np.maximum(1.0, np.abs(s2).max(-1))
     assert np.mean(err <= 1e-4) >= 0.999, np.mean(err <= 1e-4)
     assert st8["invalid_samples"] == 0 and abs(st8["rays"] - st2["rays"]) <= 0.001 * st2["rays"]
+
+
+def test_counting_instances_render_identical_images(ctx):
+    """count_traversal switches the wavefront to kernel instances that also count
+    node visits and primitive tests. The hit tests, slab set-up and camera ray have
+    their rounding pinned in the source (explicit FMAs, unfused products), so those
+    instances find the same hits to the bit: framebuffers identical with counting on
+    and off. The batch mixes BVH scenes with a brute-force job (use_bvh false)."""
+    brute = workloads.sphere_field(width=24, height=24, spp=5)
+    brute["render"]["use_bvh"] = False
+    scenes = [workloads.cornell(width=40, height=32, spp=6), workloads.mesh_stress(width=24, height=20, spp=4),
+              brute, workloads.mix_scene(4)]
+    scenes[3]["render"].update(width=20, height=20, spp=3)
+    sids = [ctx.load_json(json.dumps(s)) for s in scenes]
+    settings = [ctx.scene_settings(i) for i in sids]
+
+    def run(count):
+        ctx.set_tuning(count_traversal=count)
+        try:
+            progs = ctx.render_batch(sids, settings)
+        finally:
+            ctx.set_tuning(count_traversal=0)
+        assert all(p.finished for p in progs)
+        return ctx.stats(), [ctx.framebuffer_moments(j, s.width, s.height) for j, s in enumerate(settings)]
+
+    st0, fb0 = run(0)
+    st1, fb1 = run(1)
+    for j, (a, b) in enumerate(zip(fb0, fb1)):
+        assert a[0].tobytes() == b[0].tobytes() and a[1].tobytes() == b[1].tobytes(), j
+    assert st0["rays"] == st1["rays"] and st0["shadow_rays"] == st1["shadow_rays"]
+    assert st1["node_visits"] > 0 and st1["prim_tests"] > 0
+    for sid in sids:
+        ctx.release(sid)
