@@ -651,8 +651,10 @@ def run_rtg(a, dist, scenes, desc):
             ctx.render(ids[0], settings[0], opts)
         e2e_samples += ctx.stats()["camera_samples"]
         c2 = time.perf_counter()
-        for j, s in enumerate(settings):
-            ctx.image(j if batched else -1, s.width, s.height)
+        if batched:
+            ctx.images(range(len(settings)), [(s.width, s.height) for s in settings])
+        else:
+            ctx.image(-1, settings[0].width, settings[0].height)
         c3 = time.perf_counter()
         for i in ids:
             ctx.release(i)

@@ -244,6 +244,12 @@ int rtg_framebuffer_moments(rtg_context* ctx, int32_t job, double* sum, double* 
 /* Renderer::image (src/rendering/renderer.cpp:107-110): tone-mapped sRGB8, w*h*3.
  * tone_map < 0 uses the render's settings (normals: clamp, exposure 1). */
 int rtg_image_rgb8(rtg_context* ctx, int32_t job, int32_t tone_map, double exposure, uint8_t* rgb);
+/* rtg_image_rgb8 for n jobs at once (no reference counterpart; Renderer::image
+ * per job): image of jobs[k] into rgb[k]. All images are resolved on the device,
+ * copied to the host in one transfer with one synchronisation, then copied out on
+ * the host cores. tone_map and exposure as rtg_image_rgb8, for every job. */
+int rtg_images_rgb8(rtg_context* ctx, int32_t n, const int32_t* jobs, int32_t tone_map, double exposure,
+                    uint8_t* const* rgb);
 int rtg_render_stats(rtg_context* ctx, rtg_stats* out);
 
 /* ---- ray queries (Scene::intersect / intersect_brute / occluded,

@@ -603,28 +603,55 @@ int rtg_framebuffer_moments(rtg_context* ctx, int32_t job, double* sum, double* 
   });
 }
 
+namespace {
+
+// The tone map and exposure an image of `job` uses: the render's settings when
+// tone_map < 0 (normals: clamp, exposure 1, as Renderer::image), else the given ones.
+void image_op(const rtg_context* ctx, int32_t job, int32_t tone_map, double exposure, rtg::ToneMap& op, double& ex) {
+  op = rtg::ToneMap::Clamp;
+  ex = exposure;
+  if (tone_map < 0) {
+    const std::size_t j = job < 0 ? 0 : static_cast<std::size_t>(job);
+    if (j >= ctx->last_settings.size()) throw std::invalid_argument("no render for job");
+    const rtg::RenderSettings& s = ctx->last_settings[j];
+    if (s.integrator == rtg::Integrator::Normals) {
+      ex = 1.0;
+    } else {
+      op = s.tone_map;
+      ex = s.exposure;
+    }
+  } else {
+    if (tone_map > 2) throw std::invalid_argument("tone_map must be 0, 1 or 2");
+    op = static_cast<rtg::ToneMap>(tone_map);
+  }
+}
+
+}  // namespace
+
 int rtg_image_rgb8(rtg_context* ctx, int32_t job, int32_t tone_map, double exposure, uint8_t* rgb) {
   return guarded(ctx, [&]() {
     if (!rgb) throw std::invalid_argument("null argument");
-    rtg::ToneMap op = rtg::ToneMap::Clamp;
-    double ex = exposure;
-    if (tone_map < 0) {
-      const std::size_t j = job < 0 ? 0 : static_cast<std::size_t>(job);
-      if (j >= ctx->last_settings.size()) throw std::invalid_argument("no render for job");
-      const rtg::RenderSettings& s = ctx->last_settings[j];
-      // Renderer::image(): the normals view is shown unmapped.
-      if (s.integrator == rtg::Integrator::Normals) {
-        op = rtg::ToneMap::Clamp;
-        ex = 1.0;
-      } else {
-        op = s.tone_map;
-        ex = s.exposure;
-      }
-    } else {
-      if (tone_map > 2) throw std::invalid_argument("tone_map must be 0, 1 or 2");
-      op = static_cast<rtg::ToneMap>(tone_map);
-    }
+    rtg::ToneMap op;
+    double ex;
+    image_op(ctx, job, tone_map, exposure, op, ex);
     ctx->engine->read_image(job, op, ex, rgb);
+    return RTG_OK;
+  });
+}
+
+int rtg_images_rgb8(rtg_context* ctx, int32_t n, const int32_t* jobs, int32_t tone_map, double exposure,
+                    uint8_t* const* rgb) {
+  return guarded(ctx, [&]() {
+    if (n < 0 || (n > 0 && (!jobs || !rgb))) throw std::invalid_argument("null argument");
+    std::vector<rtg::ToneMap> ops(static_cast<std::size_t>(n));
+    std::vector<double> exs(static_cast<std::size_t>(n));
+    std::vector<int> js(static_cast<std::size_t>(n));
+    for (int32_t k = 0; k < n; ++k) {
+      if (!rgb[k]) throw std::invalid_argument("null argument");
+      image_op(ctx, jobs[k], tone_map, exposure, ops[k], exs[k]);
+      js[k] = jobs[k];
+    }
+    ctx->engine->read_images(n, js.data(), ops.data(), exs.data(), rgb);
     return RTG_OK;
   });
 }

@@ -73,6 +73,7 @@ void free_scene_arrays(GpuScene& s, cudaStream_t stream) {
 constexpr int kRing = 8;   // snapshot / staging slots (iterations in flight at most)
 constexpr int kLag = 2;    // iterations queued ahead of the snapshot being read
 constexpr std::size_t kStageBytes = std::size_t(1) << 20;  // host->device staging per iteration
+constexpr std::size_t kStagePiece = std::size_t(1) << 20;  // batch upload: bytes per host copy task
 constexpr int kJobSlots = 4096;  // job descriptors resident at once
 
 }  // namespace
@@ -178,6 +179,7 @@ Engine::~Engine() {
     cudaEventDestroy(upload_ev_[b]);
     if (upload_host_[b]) cudaFreeHost(upload_host_[b]);
   }
+  if (readback_host_) cudaFreeHost(readback_host_);
   cudaStreamSynchronize(build_stream_);
   cudaStreamDestroy(build_stream_);
   cudaStreamDestroy(stream_);
@@ -233,11 +235,18 @@ std::vector<int> Engine::add_scenes(const std::vector<std::shared_ptr<const Comp
     }
   std::vector<FlatScene> flats(scenes.size());
   const bool wide8 = wants_wide8();
+  // Largest scenes first, so none of them starts last and sets the finish.
+  std::vector<std::size_t> by_size(scenes.size());
+  for (std::size_t k = 0; k < scenes.size(); ++k) by_size[k] = k;
+  std::stable_sort(by_size.begin(), by_size.end(), [&](std::size_t a, std::size_t b) {
+    return scenes[a]->prims.size() > scenes[b]->prims.size();
+  });
   std::atomic<std::size_t> next{0};
   std::exception_ptr failed;
   std::mutex failed_lock;
   auto work = [&] {
-    for (std::size_t k; (k = next.fetch_add(1)) < scenes.size();) {
+    for (std::size_t i; (i = next.fetch_add(1)) < scenes.size();) {
+      const std::size_t k = by_size[i];
       try {
         flats[k] = flatten(*scenes[k], wide8);
       } catch (...) {
@@ -266,9 +275,25 @@ std::vector<int> Engine::add_scenes(const std::vector<std::shared_ptr<const Comp
   }
   int b = 0;
   unsigned char* host = upload_staging(std::max<std::size_t>(total, 1), b, 0);
+  // The copy into pinned memory in pieces of at most 1 MiB over all scenes' parts,
+  // so one large scene is not copied by one thread.
+  struct Piece {
+    unsigned char* dst;
+    const unsigned char* src;
+    std::size_t bytes;
+  };
+  std::vector<Piece> pieces;
+  for (std::size_t k = 0; k < scenes.size(); ++k) {
+    const void* src[kSceneParts];
+    flat_sources(flats[k], src);
+    for (int q = 0; q < kSceneParts; ++q)
+      for (std::size_t o = 0; o < parts[k].bytes[q]; o += kStagePiece)
+        pieces.push_back({host + offset[k] + parts[k].at[q] + o, static_cast<const unsigned char*>(src[q]) + o,
+                          std::min(kStagePiece, parts[k].bytes[q] - o)});
+  }
   next = 0;
   auto copy = [&] {
-    for (std::size_t k; (k = next.fetch_add(1)) < scenes.size();) stage_flat(flats[k], parts[k], host + offset[k]);
+    for (std::size_t k; (k = next.fetch_add(1)) < pieces.size();) std::memcpy(pieces[k].dst, pieces[k].src, pieces[k].bytes);
   };
   pool.clear();
   for (std::size_t w = 1; w < workers; ++w) pool.emplace_back(copy);
@@ -299,10 +324,16 @@ Engine::StagedParts Engine::staged_parts(const FlatScene& f) {
   return p;
 }
 
+void Engine::flat_sources(const FlatScene& f, const void** src) {
+  const void* s[kSceneParts] = {f.nodes.data(), f.nodes4.data(), f.prims.data(), f.slot_material.data(),
+                                f.slot_normals.data(), f.planes.data(), f.materials.data(), f.lights.data(),
+                                f.nodes8.data()};
+  for (int k = 0; k < kSceneParts; ++k) src[k] = s[k];
+}
+
 void Engine::stage_flat(const FlatScene& f, const StagedParts& p, unsigned char* dst) {
-  const void* src[kSceneParts] = {f.nodes.data(), f.nodes4.data(), f.prims.data(), f.slot_material.data(),
-                                  f.slot_normals.data(), f.planes.data(), f.materials.data(), f.lights.data(),
-                                  f.nodes8.data()};
+  const void* src[kSceneParts];
+  flat_sources(f, src);
   for (int k = 0; k < kSceneParts; ++k)
     if (p.bytes[k]) std::memcpy(dst + p.at[k], src[k], p.bytes[k]);
 }
@@ -1349,6 +1380,46 @@ void Engine::read_image_frame(const GpuFrame& f, ToneMap op, double exposure, st
   CK(cudaMemcpyAsync(rgb, tmp, px * 3, cudaMemcpyDeviceToHost, stream_));
   CK(cudaFreeAsync(tmp, stream_));
   CK(cudaStreamSynchronize(stream_));
+}
+
+void Engine::read_images(int n, const int* jobs, const ToneMap* ops, const double* exposures, std::uint8_t* const* rgb) {
+  CK(cudaSetDevice(device_));
+  if (n <= 0) return;
+  std::vector<const GpuFrame*> fr(static_cast<std::size_t>(n));
+  std::vector<std::size_t> at(static_cast<std::size_t>(n) + 1, 0), bytes(static_cast<std::size_t>(n));
+  for (int k = 0; k < n; ++k) {
+    fr[k] = &frame(jobs[k]);
+    bytes[k] = std::uint64_t(fr[k]->width) * fr[k]->height * 3;
+    at[k + 1] = at[k] + ((bytes[k] + 255) & ~std::size_t(255));
+  }
+  const std::size_t total = at[n];
+  if (total == 0) return;
+  std::uint8_t* dev = dev_alloc_async<std::uint8_t>(total, pool_, stream_);
+  for (int k = 0; k < n; ++k)
+    CK(launch_resolve(fr[k]->sum, fr[k]->count, std::uint64_t(fr[k]->width) * fr[k]->height, static_cast<int>(ops[k]),
+                      exposures[k], dev + at[k], nullptr, stream_));
+  if (readback_cap_ < total) {
+    CK(cudaStreamSynchronize(stream_));
+    if (readback_host_) CK(cudaFreeHost(readback_host_));
+    readback_host_ = nullptr;
+    readback_cap_ = 0;
+    count_allocation();
+    CK(cudaMallocHost(reinterpret_cast<void**>(&readback_host_), total));
+    readback_cap_ = total;
+  }
+  CK(cudaMemcpyAsync(readback_host_, dev, total, cudaMemcpyDeviceToHost, stream_));
+  CK(cudaFreeAsync(dev, stream_));
+  CK(cudaStreamSynchronize(stream_));
+  // Out of pinned memory into the caller's buffers, one image per task.
+  std::atomic<int> next{0};
+  auto copy = [&] {
+    for (int k; (k = next.fetch_add(1)) < n;) std::memcpy(rgb[k], readback_host_ + at[k], bytes[k]);
+  };
+  const int workers = std::min(n, static_cast<int>(std::min(16u, std::max(1u, std::thread::hardware_concurrency()))));
+  std::vector<std::thread> pool;
+  for (int w = 1; w < workers; ++w) pool.emplace_back(copy);
+  copy();
+  for (auto& t : pool) t.join();
 }
 
 // ---------------------------------------------------------------------------

@@ -172,6 +172,9 @@ class Engine {
   void read_mean(int job, double* rgb) const;
   void read_moments(int job, double* sum, double* sumsq, std::uint32_t* count) const;
   void read_image(int job, ToneMap op, double exposure, std::uint8_t* rgb) const;
+  // Several jobs' images: every resolve, then one device-to-host copy into pinned
+  // memory and one synchronisation, then copies out to rgb[k] on the host cores.
+  void read_images(int n, const int* jobs, const ToneMap* ops, const double* exposures, std::uint8_t* const* rgb);
   void read_mean_frame(const GpuFrame& f, double* rgb) const;
   void read_image_frame(const GpuFrame& f, ToneMap op, double exposure, std::uint8_t* rgb) const;
   const RenderStats& stats() const { return stats_; }
@@ -255,6 +258,7 @@ class Engine {
   };
   static StagedParts staged_parts(const FlatScene& f);
   static void stage_flat(const FlatScene& f, const StagedParts& p, unsigned char* dst);
+  static void flat_sources(const FlatScene& f, const void** src);  // kSceneParts pointers, in staged order
   // Allocates the scene's device block, queues its copy from `staged` (pinned,
   // laid out by `p`) and registers the scene.
   int register_flat(std::shared_ptr<const CompiledScene> scene, FlatScene flat, const StagedParts& p,
@@ -300,6 +304,9 @@ class Engine {
   std::size_t upload_cap_[2] = {0, 0};
   cudaEvent_t upload_ev_[2] = {nullptr, nullptr};
   bool upload_pending_[2] = {false, false};
+  // Pinned read-back buffer of read_images (grown on demand).
+  unsigned char* readback_host_ = nullptr;
+  std::size_t readback_cap_ = 0;
   int upload_next_ = 0;
   std::size_t pool_reserved_ = 0;
   bool bvh_preloaded_ = false;

@@ -118,16 +118,14 @@ void build_wide(const BinaryBvh& bvh, const std::vector<FBox>& fbox, FlatScene& 
     f.root4 = ~static_cast<std::int32_t>(bvh.nodes[0].first);
     return;
   }
-  // Topology first (serial, indices only), then the boxes in parallel.
+  // Topology first (serial, indices only), then the boxes in parallel. A
+  // four-wide node's children are recorded under the binary node it starts from,
+  // so numbering the starts in binary (depth-first) order needs no sort.
   struct Kids {
     std::uint32_t bin[4];
-    int n;
+    int n;  // 0: this binary node starts no four-wide node
   };
-  struct Root {
-    std::uint32_t bin;  // the binary interior node this four-wide node starts from
-    Kids kids;
-  };
-  std::vector<Root> roots;
+  std::vector<Kids> kids_of(bvh.nodes.size());
   std::vector<std::pair<std::uint32_t, int>> work{{0u, 1}};
   while (!work.empty()) {
     const auto [bin, depth] = work.back();
@@ -155,15 +153,19 @@ void build_wide(const BinaryBvh& bvh, const std::vector<FBox>& fbox, FlatScene& 
     }
     for (int q = 0; q < k.n; ++q)
       if (!bvh.nodes[k.bin[q]].leaf()) work.push_back({k.bin[q], depth + 1});
-    roots.push_back({bin, k});
+    kids_of[bin] = k;
   }
-  std::sort(roots.begin(), roots.end(), [](const Root& x, const Root& y) { return x.bin < y.bin; });
   std::vector<std::int32_t> wide_index(bvh.nodes.size(), -1);
-  for (std::size_t i = 0; i < roots.size(); ++i) wide_index[roots[i].bin] = static_cast<std::int32_t>(i);
-  f.nodes4.resize(roots.size());
-  parallel_chunks(roots.size(), [&](std::size_t i0, std::size_t i1) {
+  std::vector<std::uint32_t> start;  // four-wide node i starts from binary node start[i]
+  for (std::size_t b = 0; b < bvh.nodes.size(); ++b)
+    if (kids_of[b].n) {
+      wide_index[b] = static_cast<std::int32_t>(start.size());
+      start.push_back(static_cast<std::uint32_t>(b));
+    }
+  f.nodes4.resize(start.size());
+  parallel_chunks(start.size(), [&](std::size_t i0, std::size_t i1) {
     for (std::size_t i = i0; i < i1; ++i) {
-      const Kids& k = roots[i].kids;
+      const Kids& k = kids_of[start[i]];
       float lo[3][4], hi[3][4];
       std::int32_t link[4];
       for (int q = 0; q < 4; ++q) {

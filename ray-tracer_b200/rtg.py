@@ -20,7 +20,7 @@ import ctypes as C
 import dataclasses
 import os
 import threading
-from typing import Callable, Optional
+from typing import Callable, Optional, Sequence
 
 import numpy as np
 
@@ -146,6 +146,8 @@ _SIGNATURES = {
     "rtg_framebuffer_moments": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                           C.POINTER(C.c_uint32)]),
     "rtg_image_rgb8": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_double, C.POINTER(C.c_uint8)]),
+    "rtg_images_rgb8": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.c_int32, C.c_double,
+                                  C.POINTER(C.POINTER(C.c_uint8))]),
     "rtg_render_stats": (C.c_int, [C.c_void_p, C.POINTER(_Stats)]),
     "rtg_trace_closest": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_float), C.c_uint64, C.c_int32,
                                     C.POINTER(C.c_float), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
@@ -527,6 +529,18 @@ class Context:
         op = -1 if tone_map is None else TONE_MAPS[tone_map]
         self._check(lib().rtg_image_rgb8(self._h, job, op, exposure, _ptr(out, C.c_uint8)))
         return out
+
+    def images(self, jobs: Sequence[int], sizes: Sequence[tuple], tone_map: Optional[str] = None,
+               exposure: float = 1.0) -> list:
+        """image() of several jobs at once (one device-to-host transfer): sizes[k] is
+        (width, height) of jobs[k]."""
+        outs = [np.zeros((h, w, 3), dtype=np.uint8) for w, h in sizes]
+        n = len(outs)
+        js = (C.c_int32 * n)(*[int(j) for j in jobs])
+        ptrs = (C.POINTER(C.c_uint8) * n)(*[_ptr(o, C.c_uint8) for o in outs])
+        op = -1 if tone_map is None else TONE_MAPS[tone_map]
+        self._check(lib().rtg_images_rgb8(self._h, n, js, op, exposure, ptrs))
+        return outs
 
     def stats(self) -> dict:
         s = _Stats()

@@ -394,3 +394,29 @@ def test_counting_instances_render_identical_images(ctx):
     assert st1["node_visits"] > 0 and st1["prim_tests"] > 0
     for sid in sids:
         ctx.release(sid)
+
+
+def test_images_of_a_batch_equal_the_single_image_reads(ctx):
+    """rtg_images_rgb8 (one transfer for several jobs) gives each job exactly the
+    bytes rtg_image_rgb8 gives it: with every job's own tone map and exposure
+    (a normals job included, shown unmapped), with an explicit operator, and for a
+    subset of the jobs in another order."""
+    scenes = [workloads.cornell(width=40, height=32, spp=4), workloads.sphere_field(width=24, height=20, spp=3),
+              workloads.mesh_stress(width=16, height=16, spp=2)]
+    scenes[1]["render"].update(tone_map="reinhard", exposure=1.5)
+    scenes[2]["render"]["integrator"] = "normals"
+    sids = [ctx.load_json(json.dumps(s)) for s in scenes]
+    settings = [ctx.scene_settings(i) for i in sids]
+    ctx.render_batch(sids, settings)
+    sizes = [(s.width, s.height) for s in settings]
+    for tm, ex in ((None, 1.0), ("aces", 0.7)):
+        single = [ctx.image(j, w, h, tone_map=tm, exposure=ex) for j, (w, h) in enumerate(sizes)]
+        many = ctx.images(range(3), sizes, tone_map=tm, exposure=ex)
+        for a, b in zip(single, many):
+            assert a.tobytes() == b.tobytes()
+    sub = ctx.images([2, 0], [sizes[2], sizes[0]])
+    assert sub[0].tobytes() == ctx.image(2, *sizes[2]).tobytes()
+    assert sub[1].tobytes() == ctx.image(0, *sizes[0]).tobytes()
+    assert ctx.images([], []) == []
+    for sid in sids:
+        ctx.release(sid)
