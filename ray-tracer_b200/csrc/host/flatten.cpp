@@ -1,9 +1,11 @@
 #include "host/flatten.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <mutex>
 #include <stdexcept>
 #include <thread>
 
@@ -54,7 +56,7 @@ float up(double v) {
 template <class F>
 void parallel_chunks(std::size_t n, F&& body) {
   const std::size_t hw = std::max(1u, std::thread::hardware_concurrency());
-  const std::size_t workers = std::min<std::size_t>({hw, 16, (n + 32767) / 32768});
+  const std::size_t workers = std::min<std::size_t>({hw, 16, (n + 8191) / 8192});
   if (workers <= 1) {
     body(std::size_t(0), n);
     return;
@@ -107,7 +109,7 @@ DevMaterial material_record(const Material& m) {
 // keep their slot ranges. Four-wide nodes are numbered in the depth-first order
 // of the binary nodes they start from, which the device build computes with a
 // scan instead of a serial walk.
-void build_wide(const BinaryBvh& bvh, const std::vector<FBox>& fbox, FlatScene& f) {
+void build_wide(const BinaryBvh& bvh, const RecordVector<FBox>& fbox, FlatScene& f) {
   f.nodes4.clear();
   f.depth4 = 0;
   if (bvh.nodes.empty()) {
@@ -118,19 +120,18 @@ void build_wide(const BinaryBvh& bvh, const std::vector<FBox>& fbox, FlatScene& 
     f.root4 = ~static_cast<std::int32_t>(bvh.nodes[0].first);
     return;
   }
-  // Topology first (serial, indices only), then the boxes in parallel. A
-  // four-wide node's children are recorded under the binary node it starts from,
-  // so numbering the starts in binary (depth-first) order needs no sort.
+  // Topology first (indices only), then the boxes. A four-wide node's children
+  // are recorded under the binary node it starts from, so numbering the starts
+  // in binary (depth-first) order needs no sort, and disjoint subtrees can be
+  // collapsed on different threads.
   struct Kids {
     std::uint32_t bin[4];
     int n;  // 0: this binary node starts no four-wide node
   };
   std::vector<Kids> kids_of(bvh.nodes.size());
-  std::vector<std::pair<std::uint32_t, int>> work{{0u, 1}};
-  while (!work.empty()) {
-    const auto [bin, depth] = work.back();
-    work.pop_back();
-    f.depth4 = std::max(f.depth4, depth);
+  // The four-wide node starting at binary node `bin`; push(c) gets each interior
+  // child, which starts a four-wide node of its own.
+  auto expand = [&](std::uint32_t bin, auto&& push) {
     Kids k{};
     k.bin[k.n++] = bin + 1;
     k.bin[k.n++] = bvh.nodes[bin].first;
@@ -152,9 +153,44 @@ void build_wide(const BinaryBvh& bvh, const std::vector<FBox>& fbox, FlatScene& 
       k.bin[k.n++] = bvh.nodes[b].first;
     }
     for (int q = 0; q < k.n; ++q)
-      if (!bvh.nodes[k.bin[q]].leaf()) work.push_back({k.bin[q], depth + 1});
+      if (!bvh.nodes[k.bin[q]].leaf()) push(k.bin[q]);
     kids_of[bin] = k;
+  };
+  // Breadth first from the root until about 256 subtrees are open, then each of
+  // those depth first as its own task.
+  std::vector<std::pair<std::uint32_t, int>> open{{0u, 1}};
+  std::size_t head = 0;
+  int depth4 = 0;
+  while (head < open.size() && open.size() - head < 256) {
+    const auto [bin, depth] = open[head++];
+    depth4 = std::max(depth4, depth);
+    expand(bin, [&, depth = depth](std::uint32_t c) { open.push_back({c, depth + 1}); });
   }
+  std::atomic<std::size_t> next_task{head};
+  std::mutex depth_lock;
+  auto subtrees = [&] {
+    int deepest = 0;
+    std::vector<std::pair<std::uint32_t, int>> work;
+    for (std::size_t t; (t = next_task.fetch_add(1)) < open.size();) {
+      work.assign(1, open[t]);
+      while (!work.empty()) {
+        const auto [bin, depth] = work.back();
+        work.pop_back();
+        deepest = std::max(deepest, depth);
+        expand(bin, [&, depth = depth](std::uint32_t c) { work.push_back({c, depth + 1}); });
+      }
+    }
+    std::lock_guard<std::mutex> g(depth_lock);
+    depth4 = std::max(depth4, deepest);
+  };
+  const std::size_t tasks = open.size() - head;
+  const std::size_t workers =
+      std::min<std::size_t>({std::max(1u, std::thread::hardware_concurrency()), 16, (tasks + 15) / 16});
+  std::vector<std::thread> pool;
+  for (std::size_t w = 1; w < workers; ++w) pool.emplace_back(subtrees);
+  subtrees();
+  for (auto& t : pool) t.join();
+  f.depth4 = depth4;
   std::vector<std::int32_t> wide_index(bvh.nodes.size(), -1);
   std::vector<std::uint32_t> start;  // four-wide node i starts from binary node start[i]
   for (std::size_t b = 0; b < bvh.nodes.size(); ++b)
@@ -281,9 +317,9 @@ FlatScene flatten(const CompiledScene& s, bool wide8) {
   std::vector<std::uint8_t> last(nslots, 0);
   for (const BinaryNode& n : bvh.nodes)
     if (n.leaf()) last[n.first + n.count - 1] = 1;
-  f.prims.resize(nslots * 3);
+  f.prims.resize(nslots * 3);  // every slot_record writes all three rows and normals
   f.slot_material.resize(nslots);
-  f.slot_normals.resize(nslots * 3, make_float4(0.f, 0.f, 0.f, 0.f));
+  f.slot_normals.resize(nslots * 3);
   f.slot_prim.resize(nslots);
   parallel_chunks(nslots, [&](std::size_t k0, std::size_t k1) {
     for (std::size_t k = k0; k < k1; ++k) {
@@ -304,7 +340,7 @@ FlatScene flatten(const CompiledScene& s, bool wide8) {
     return c.leaf() ? ~static_cast<std::int32_t>(c.first) : dev_index[child];
   };
   // Every node's box rounded outward once; both device trees copy from here.
-  std::vector<FBox> fbox(bvh.nodes.size());
+  RecordVector<FBox> fbox(bvh.nodes.size());  // every entry written below
   parallel_chunks(bvh.nodes.size(), [&](std::size_t i0, std::size_t i1) {
     for (std::size_t i = i0; i < i1; ++i) fbox[i] = outward(bvh.nodes[i].box);
   });
@@ -340,7 +376,7 @@ void add_wide8(FlatScene& f) {
   bool identity = true;
   for (std::size_t k = 0; k < nslots && identity; ++k) identity = w.old_of[k] == k;
   if (identity) return;
-  std::vector<float4> prims(f.prims.size()), normals(f.slot_normals.size());
+  RecordVector<float4> prims(f.prims.size()), normals(f.slot_normals.size());
   std::vector<std::uint32_t> material(nslots), prim(nslots);
   parallel_chunks(nslots, [&](std::size_t k0, std::size_t k1) {
     for (std::size_t k = k0; k < k1; ++k) {

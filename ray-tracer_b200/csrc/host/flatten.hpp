@@ -9,6 +9,9 @@
 // compressed eight-wide tree needs (wide8.hpp): the leaf children of each of its
 // nodes side by side.
 #include <cstdint>
+#include <memory>
+#include <new>
+#include <utility>
 #include <vector>
 
 #include "device/layout.h"
@@ -19,11 +22,35 @@ namespace rtg {
 
 constexpr std::int32_t kNoRoot = INT32_MIN;
 
+// Allocator whose resize leaves new elements uninitialised: the large record
+// arrays below are written in full by flatten's parallel loops, so filling them
+// with zeros first only adds a serial pass over fresh pages.
+template <class T>
+struct Uninit : std::allocator<T> {
+  template <class U>
+  struct rebind {
+    using other = Uninit<U>;
+  };
+  Uninit() = default;
+  template <class U>
+  Uninit(const Uninit<U>&) noexcept {}
+  template <class U>
+  void construct(U* p) noexcept {
+    ::new (static_cast<void*>(p)) U;
+  }
+  template <class U, class... A>
+  void construct(U* p, A&&... a) {
+    ::new (static_cast<void*>(p)) U(std::forward<A>(a)...);
+  }
+};
+template <class T>
+using RecordVector = std::vector<T, Uninit<T>>;
+
 struct FlatScene {
-  std::vector<DevNode> nodes;
-  std::vector<float4> prims;                // 3 per slot
+  RecordVector<DevNode> nodes;
+  RecordVector<float4> prims;               // 3 per slot
   std::vector<std::uint32_t> slot_material; // material | smooth << 31 (scene-local material index)
-  std::vector<float4> slot_normals;         // 3 per slot
+  RecordVector<float4> slot_normals;        // 3 per slot
   std::vector<std::uint32_t> slot_prim;     // slot -> primitive id
   std::vector<DevPlane> planes;             // material scene-local
   std::vector<DevMaterial> materials;
