@@ -276,7 +276,7 @@ __device__ __forceinline__ float light_pdf_of_hit(const RtgSceneDev& sc, float3 
   const float4 p1 = __ldg(&sc.prims[3 * slot + 1]);
   const float cos_l = fabsf(dot3(s.gn, d));
   if (__float_as_uint(p0.w) & kSphereBit) {
-    const float r = p1.x, r2 = p1.y;
+    const float r2 = p1.y;  // radius squared (p1.x holds the radius)
     const float3 oc = f3(p0) - o;
     const float d2 = dot3(oc, oc);
     if (d2 <= r2) return cos_l > 0.f ? h.t * h.t / (cos_l * 4.f * kPiF * r2) : 0.f;

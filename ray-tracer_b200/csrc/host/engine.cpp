@@ -275,30 +275,10 @@ std::vector<int> Engine::add_scenes(const std::vector<std::shared_ptr<const Comp
   }
   int b = 0;
   unsigned char* host = upload_staging(std::max<std::size_t>(total, 1), b, 0);
-  // The copy into pinned memory in pieces of at most 1 MiB over all scenes' parts,
-  // so one large scene is not copied by one thread.
-  struct Piece {
-    unsigned char* dst;
-    const unsigned char* src;
-    std::size_t bytes;
-  };
-  std::vector<Piece> pieces;
-  for (std::size_t k = 0; k < scenes.size(); ++k) {
-    const void* src[kSceneParts];
-    flat_sources(flats[k], src);
-    for (int q = 0; q < kSceneParts; ++q)
-      for (std::size_t o = 0; o < parts[k].bytes[q]; o += kStagePiece)
-        pieces.push_back({host + offset[k] + parts[k].at[q] + o, static_cast<const unsigned char*>(src[q]) + o,
-                          std::min(kStagePiece, parts[k].bytes[q] - o)});
-  }
-  next = 0;
-  auto copy = [&] {
-    for (std::size_t k; (k = next.fetch_add(1)) < pieces.size();) std::memcpy(pieces[k].dst, pieces[k].src, pieces[k].bytes);
-  };
-  pool.clear();
-  for (std::size_t w = 1; w < workers; ++w) pool.emplace_back(copy);
-  copy();
-  for (auto& t : pool) t.join();
+  // The copy into pinned memory, in pieces over all scenes' parts.
+  std::vector<StagePiece> pieces;
+  for (std::size_t k = 0; k < scenes.size(); ++k) stage_pieces(flats[k], parts[k], host + offset[k], pieces);
+  copy_pieces(pieces);
   std::vector<int> ids;
   ids.reserve(scenes.size());
   for (std::size_t k = 0; k < scenes.size(); ++k)
@@ -324,18 +304,34 @@ Engine::StagedParts Engine::staged_parts(const FlatScene& f) {
   return p;
 }
 
-void Engine::flat_sources(const FlatScene& f, const void** src) {
-  const void* s[kSceneParts] = {f.nodes.data(), f.nodes4.data(), f.prims.data(), f.slot_material.data(),
-                                f.slot_normals.data(), f.planes.data(), f.materials.data(), f.lights.data(),
-                                f.nodes8.data()};
-  for (int k = 0; k < kSceneParts; ++k) src[k] = s[k];
+void Engine::stage_pieces(const FlatScene& f, const StagedParts& p, unsigned char* dst, std::vector<StagePiece>& out) {
+  const void* src[kSceneParts] = {f.nodes.data(), f.nodes4.data(), f.prims.data(), f.slot_material.data(),
+                                  f.slot_normals.data(), f.planes.data(), f.materials.data(), f.lights.data(),
+                                  f.nodes8.data()};
+  for (int q = 0; q < kSceneParts; ++q)
+    for (std::size_t o = 0; o < p.bytes[q]; o += kStagePiece)
+      out.push_back({dst + p.at[q] + o, static_cast<const unsigned char*>(src[q]) + o,
+                     std::min(kStagePiece, p.bytes[q] - o)});
+}
+
+void Engine::copy_pieces(const std::vector<StagePiece>& pieces) {
+  std::atomic<std::size_t> next{0};
+  auto copy = [&] {
+    for (std::size_t k; (k = next.fetch_add(1)) < pieces.size();) std::memcpy(pieces[k].dst, pieces[k].src, pieces[k].bytes);
+  };
+  // A thread per 4 pieces at most: small scenes are copied inline.
+  const std::size_t workers =
+      std::min<std::size_t>({std::max(1u, std::thread::hardware_concurrency()), 16, (pieces.size() + 3) / 4});
+  std::vector<std::thread> pool;
+  for (std::size_t w = 1; w < workers; ++w) pool.emplace_back(copy);
+  copy();
+  for (auto& t : pool) t.join();
 }
 
 void Engine::stage_flat(const FlatScene& f, const StagedParts& p, unsigned char* dst) {
-  const void* src[kSceneParts];
-  flat_sources(f, src);
-  for (int k = 0; k < kSceneParts; ++k)
-    if (p.bytes[k]) std::memcpy(dst + p.at[k], src[k], p.bytes[k]);
+  std::vector<StagePiece> pieces;
+  stage_pieces(f, p, dst, pieces);
+  copy_pieces(pieces);
 }
 
 int Engine::add_flat(std::shared_ptr<const CompiledScene> scene, FlatScene flat) {

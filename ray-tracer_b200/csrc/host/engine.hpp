@@ -257,8 +257,16 @@ class Engine {
     std::size_t at[kSceneParts], bytes[kSceneParts], total;
   };
   static StagedParts staged_parts(const FlatScene& f);
+  // The host copy into pinned staging, as pieces of at most 1 MiB so that one
+  // large scene is copied by many threads.
+  struct StagePiece {
+    unsigned char* dst;
+    const unsigned char* src;
+    std::size_t bytes;
+  };
+  static void stage_pieces(const FlatScene& f, const StagedParts& p, unsigned char* dst, std::vector<StagePiece>& out);
+  static void copy_pieces(const std::vector<StagePiece>& pieces);  // on the host cores
   static void stage_flat(const FlatScene& f, const StagedParts& p, unsigned char* dst);
-  static void flat_sources(const FlatScene& f, const void** src);  // kSceneParts pointers, in staged order
   // Allocates the scene's device block, queues its copy from `staged` (pinned,
   // laid out by `p`) and registers the scene.
   int register_flat(std::shared_ptr<const CompiledScene> scene, FlatScene flat, const StagedParts& p,
