@@ -248,7 +248,10 @@ std::vector<int> Engine::add_scenes(const std::vector<std::shared_ptr<const Comp
     for (std::size_t i; (i = next.fetch_add(1)) < scenes.size();) {
       const std::size_t k = by_size[i];
       try {
-        flats[k] = flatten(*scenes[k], wide8);
+        // The workers already use every core: only the largest scenes, which
+        // start first and set the finish, split their own loops.
+        const std::size_t np = scenes[k]->prims.size();
+        flats[k] = flatten(*scenes[k], wide8, np >= 100000 ? 4u : np >= 32768 ? 2u : 1u);
       } catch (...) {
         std::lock_guard<std::mutex> g(failed_lock);
         if (!failed) failed = std::current_exception();

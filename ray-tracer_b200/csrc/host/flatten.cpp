@@ -50,13 +50,19 @@ float up(double v) {
   return step_up(f);
 }
 
-// Runs body(begin, end) over [0, n) in contiguous chunks on up to 16 threads
-// (one chunk inline when n is small). Used for the per-slot and per-node loops,
-// whose iterations write disjoint records.
+// Threads one flatten call may use (its max_threads argument; set for the call).
+thread_local std::size_t t_flatten_threads = 16;
+
+std::size_t flatten_threads() {
+  return std::min<std::size_t>({std::max(1u, std::thread::hardware_concurrency()), 16, t_flatten_threads});
+}
+
+// Runs body(begin, end) over [0, n) in contiguous chunks on up to
+// flatten_threads() threads (one chunk inline when n is small). Used for the
+// per-slot and per-node loops, whose iterations write disjoint records.
 template <class F>
 void parallel_chunks(std::size_t n, F&& body) {
-  const std::size_t hw = std::max(1u, std::thread::hardware_concurrency());
-  const std::size_t workers = std::min<std::size_t>({hw, 16, (n + 8191) / 8192});
+  const std::size_t workers = std::min<std::size_t>(flatten_threads(), (n + 8191) / 8192);
   if (workers <= 1) {
     body(std::size_t(0), n);
     return;
@@ -184,8 +190,7 @@ void build_wide(const BinaryBvh& bvh, const RecordVector<FBox>& fbox, FlatScene&
     depth4 = std::max(depth4, deepest);
   };
   const std::size_t tasks = open.size() - head;
-  const std::size_t workers =
-      std::min<std::size_t>({std::max(1u, std::thread::hardware_concurrency()), 16, (tasks + 15) / 16});
+  const std::size_t workers = std::min<std::size_t>(flatten_threads(), (tasks + 15) / 16);
   std::vector<std::thread> pool;
   for (std::size_t w = 1; w < workers; ++w) pool.emplace_back(subtrees);
   subtrees();
@@ -307,7 +312,12 @@ void flatten_tables(const CompiledScene& s, FlatScene& f) {
   }
 }
 
-FlatScene flatten(const CompiledScene& s, bool wide8) {
+FlatScene flatten(const CompiledScene& s, bool wide8, unsigned max_threads) {
+  struct Cap {
+    std::size_t old = t_flatten_threads;
+    explicit Cap(unsigned n) { t_flatten_threads = n ? n : 16; }
+    ~Cap() { t_flatten_threads = old; }
+  } cap(max_threads);
   FlatScene f;
   const BinaryBvh& bvh = s.bvh;
 

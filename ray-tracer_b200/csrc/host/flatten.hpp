@@ -68,7 +68,9 @@ struct FlatScene {
 
 // wide8: also build the compressed eight-wide tree and move the slots to its
 // order (add_wide8); without it nodes8 stays empty and root8 kNoRoot.
-FlatScene flatten(const CompiledScene& s, bool wide8);
+// max_threads bounds the threads this call uses (0: up to 16, or the core
+// count); callers flattening many scenes at once give each a small share.
+FlatScene flatten(const CompiledScene& s, bool wide8, unsigned max_threads = 0);
 
 // Builds the eight-wide tree from f.nodes / f.root and moves every per-slot array
 // of f (and the binary and four-wide trees' leaf links) to its slot order.
