@@ -286,8 +286,12 @@ __global__ void __launch_bounds__(kBlock) k_extend(WaveBuffers wb, int par) {
 template <int kBlock, bool kMis>
 __global__ void __launch_bounds__(kBlock, 1024 / kBlock) k_shade(WaveBuffers wb, int par) {
   constexpr int kWarps = kBlock / 32;
-  __shared__ std::uint32_t s_cnt[2][kWarps];
-  __shared__ std::uint32_t s_base[2];
+  // Per-round queue counts and bases, double-buffered by round parity: a round
+  // writes one buffer while the other may still be read, so no barrier is needed
+  // at the end of a round.
+  __shared__ std::uint32_t s_cnt[2][2][kWarps];
+  __shared__ std::uint32_t s_base[2][2];
+  int rb = 0;
   chain_to_previous_grid();
   WaveCounters* C = wb.cnt;
   const std::uint32_t n = C->n_extend;
@@ -398,24 +402,26 @@ __global__ void __launch_bounds__(kBlock, 1024 / kBlock) k_shade(WaveBuffers wb,
     // Appends aggregated per block: one atomic per queue per 256 paths.
     const unsigned mc = __ballot_sync(kFull, cont), ms = __ballot_sync(kFull, shadow);
     if (lane == 0) {
-      s_cnt[0][warp] = __popc(mc);
-      s_cnt[1][warp] = __popc(ms);
+      s_cnt[rb][0][warp] = __popc(mc);
+      s_cnt[rb][1][warp] = __popc(ms);
     }
     __syncthreads();
     if (threadIdx.x < 2) {
       std::uint32_t total = 0;
       for (int w = 0; w < kWarps; ++w) {
-        const std::uint32_t c = s_cnt[threadIdx.x][w];
-        s_cnt[threadIdx.x][w] = total;
+        const std::uint32_t c = s_cnt[rb][threadIdx.x][w];
+        s_cnt[rb][threadIdx.x][w] = total;
         total += c;
       }
-      s_base[threadIdx.x] = total ? atomicAdd(threadIdx.x == 0 ? &C->live[par ^ 1] : &C->n_shadow, total) : 0u;
+      s_base[rb][threadIdx.x] = total ? atomicAdd(threadIdx.x == 0 ? &C->live[par ^ 1] : &C->n_shadow, total) : 0u;
     }
     __syncthreads();
     const unsigned below = (1u << lane) - 1u;
-    const std::uint32_t cpos = s_base[0] + s_cnt[0][warp] + __popc(mc & below);
-    const std::uint32_t spos = s_base[1] + s_cnt[1][warp] + __popc(ms & below);
-    __syncthreads();  // s_cnt / s_base are rewritten next round
+    const std::uint32_t cpos = s_base[rb][0] + s_cnt[rb][0][warp] + __popc(mc & below);
+    const std::uint32_t spos = s_base[rb][1] + s_cnt[rb][1][warp] + __popc(ms & below);
+    // The next round writes the other buffer; the one after writes this one again
+    // only after its first barrier, which every thread reaches after these reads.
+    rb ^= 1;
     // A path that ends here is done once this iteration's shadow stage has run:
     // count it in its segment (one atomic per segment present in the warp).
     const bool fin = i < n && !cont;
