@@ -291,14 +291,22 @@ def test_workloads_render_with_no_invalid_samples(ctx, make):
 
 
 def test_batch_upload_renders_like_single_uploads(ctx):
+    """rtg_scene_upload_batch flattens its scenes concurrently (the largest first, each
+    with its own share of threads) and stages them in pieces: every part of every
+    scene's device layout is byte-identical to a single upload's, and so are renders.
+    The scenes span the thread shares: 174k primitives, 82k and small ones."""
     scenes = [workloads.cornell(width=24, height=24, spp=3), workloads.mesh_stress(width=16, height=16, spp=2),
-              workloads.mix_scene(5)]
-    scenes[2]["render"].update(width=16, height=16, spp=2)
+              workloads.mix_scene(5), workloads.mix_scene(1)]
+    for k in (2, 3):
+        scenes[k]["render"].update(width=16, height=16, spp=2)
     hosts = [rtg.parse_scene(json.dumps(s)) for s in scenes]
     single = [ctx.upload(h) for h in hosts]
     many = ctx.upload_many(hosts)
-    assert len(set(single + many)) == 6
+    assert len(set(single + many)) == 8
+    assert ctx.scene_info(single[3])["primitives"] > 32768
     for a, b in zip(single, many):
+        for part in rtg.LAYOUT_PARTS:
+            assert ctx.scene_layout(a, part).tobytes() == ctx.scene_layout(b, part).tobytes(), part
         st = ctx.scene_settings(a)
         assert ctx.scene_info(a)["primitives"] == ctx.scene_info(b)["primitives"]
         ctx.render(a, st)
