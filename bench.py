@@ -513,14 +513,15 @@ class _NoDist:
 
 def render_config(ctx, name, a, peaks):
     """One configuration rendered alone (plain renderer): device-time Msamples/s,
-    Mrays/s, end to end through the public API, roofline, reference CPU."""
+    Mrays/s, end to end through the public API, roofline, reference CPU. One pass
+    of all samples, as the reference CLI's --single-pass run it is compared with."""
     import rtg
 
     scene = config_scene(name)
     host = rtg.parse_scene(json.dumps(scene))
     sid = ctx.upload(host)
     st = ctx.scene_settings(sid)
-    opts = rtg.RenderOptions(progressive=not a.single_pass, max_pass_spp=32)
+    opts = rtg.RenderOptions(progressive=False)
 
     def step():
         ctx.render(sid, st, opts)
@@ -545,7 +546,8 @@ def render_config(ctx, name, a, peaks):
         ctx.image(-1, st.width, st.height)
         ctx.release(i)
     e2e = e2e_samples / (time.perf_counter() - t0) / 1e6
-    return {"workload": config_desc(name), "value": value, "unit": "Msamples/s",
+    return {"workload": config_desc(name), "passes": "single pass (as the CPU arm's --single-pass)",
+            "value": value, "unit": "Msamples/s",
             "ms_per_render": t["t_max_ms"] / steps, "mrays_per_s": t["rays"] / (t["t_max_ms"] / 1e3) / 1e6,
             "e2e": {"value": e2e, "unit": "Msamples/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": st.width * st.height * 3},
