@@ -426,5 +426,11 @@ def test_images_of_a_batch_equal_the_single_image_reads(ctx):
     assert sub[0].tobytes() == ctx.image(2, *sizes[2]).tobytes()
     assert sub[1].tobytes() == ctx.image(0, *sizes[0]).tobytes()
     assert ctx.images([], []) == []
+    # A job index past the batch is an error, with either tone-map source, and the
+    # context stays usable.
+    for tm in (None, "clamp"):
+        with pytest.raises(rtg.RtgError):
+            ctx.images([0, 7], [sizes[0], (4, 4)], tone_map=tm)
+    assert ctx.images([1], [sizes[1]])[0].tobytes() == ctx.image(1, *sizes[1]).tobytes()
     for sid in sids:
         ctx.release(sid)
